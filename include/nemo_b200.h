@@ -1,0 +1,60 @@
+#ifndef NEMO_B200_H
+#define NEMO_B200_H
+
+/* Extensions of the NeMo C ABI provided by libnemo_b200.so. None of these
+ * has a counterpart in the reference C ABI (src/nemo.h); they expose the
+ * device-resident forms of the step path. Errors follow the include/nemo.h
+ * model (status code + nemo_strerror). */
+
+#include <stddef.h>
+#include <stdint.h>
+#include <nemo.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Run `cycles` cycles (<= 1024 per call) without stimulus, entirely on the
+ * device as one CUDA graph (gather, neuron update with scatter, STDP
+ * accumulation per cycle). Equivalent to `cycles` calls of nemo_step with
+ * empty stimulus. fired_counts[k] / events[k] (each may be NULL) receive the
+ * number of neurons fired in cycle k and the synaptic events those firings
+ * generate (fired neurons x out-degree, the throughput unit of the
+ * reference benchmark, src/examples/common.cpp:93-98). */
+nemo_status_t nemo_b200_run(nemo_simulation_t sim, unsigned cycles,
+		uint32_t fired_counts[], uint64_t events[]);
+
+/* Fired neurons of an earlier cycle (one of the last 1024 simulated), in the
+ * same order and ownership as nemo_step's output. `cycle` counts from the
+ * creation of the simulation. */
+nemo_status_t nemo_b200_fired_at(nemo_simulation_t sim, uint64_t cycle,
+		unsigned* fired[], size_t* fired_count);
+
+/* Number of cycles simulated since the simulation was created. */
+nemo_status_t nemo_b200_cycle(nemo_simulation_t sim, uint64_t* cycle);
+
+/* Wait for all device work of the simulation. */
+nemo_status_t nemo_b200_synchronize(nemo_simulation_t sim);
+
+/* Diagnostics: the device noise transform of two RNG words per sample,
+ * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the
+ * Izhikevich kernel (glibc-matching), for n samples. */
+nemo_status_t nemo_b200_nrand_probe(nemo_simulation_t sim, const uint32_t u1[], const uint32_t u2[],
+		float out[], size_t n);
+
+/* Diagnostics: evaluate the device sinf/logf of the noise generator on all
+ * 83886081 inputs the RNG can produce and count results that differ from the
+ * host glibc (0 when the device reproduces the reference bit for bit). */
+nemo_status_t nemo_b200_libm_check(nemo_simulation_t sim, uint64_t* mismatches);
+
+/* Path of the glibc correction-table cache file used by this process. */
+const char* nemo_b200_libm_cache_path(void);
+
+/* Build the glibc correction tables now (and write the cache file). */
+nemo_status_t nemo_b200_prepare_libm_tables(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

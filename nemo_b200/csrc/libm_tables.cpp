@@ -1,0 +1,183 @@
+/* Correction tables that let the device reproduce the host glibc sinf/logf
+ * results of the reference's thalamic-noise generator bit for bit (see
+ * libm_match.cuh for the method). Built once per process on the host with all
+ * available cores and cached on disk, keyed by the glibc version.
+ *
+ * This is calibration data, not a CPU path: the tables record, for each of
+ * the 83886081 inputs the RNG can produce, how glibc's rounding differs from
+ * the device candidate. The noise itself is computed by the kernels. */
+
+#include "libm_tables.hpp"
+
+#include <gnu/libc-version.h>
+#include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "common.hpp"
+#include "libm_match.cuh"
+
+namespace nemo_b200 {
+
+using namespace libm;
+
+static const uint32_t FILE_MAGIC = 0x4e4d4c54u; /* "NMLT" */
+static const uint32_t FILE_VERSION = 1u;
+
+static uint32_t
+codeFor(float glibc, float cand)
+{
+	uint32_t g = f2u(glibc), c = f2u(cand);
+	if(g == c) return 0u;
+	if(g == c + 1u) return 1u;
+	if(g == c - 1u) return 2u;
+	return 3u;
+}
+
+static void
+buildRange(uint32_t w0, uint32_t w1, uint32_t* sinT, uint32_t* logT, unsigned long* bad)
+{
+	unsigned long nbad = 0;
+	for(uint32_t w = w0; w < w1; ++w) {
+		uint32_t ws = 0, wl = 0;
+		for(uint32_t k = 0; k < 16; ++k) {
+			uint32_t idx = w * 16 + k;
+			if(idx >= TABLE_ENTRIES) break;
+			float fu = libm_value(idx);
+			float a = sin_argument(fu);
+			float y = log_argument(fu);
+			volatile float gs = sinf(a);
+			volatile float gl = logf(y);
+			uint32_t cs = codeFor(gs, sin_candidate(a));
+			uint32_t cl = codeFor(gl, log_candidate(y));
+			if(cs == 3u || cl == 3u) nbad++;
+			ws |= (cs & 3u) << (2 * k);
+			wl |= (cl & 3u) << (2 * k);
+		}
+		sinT[w] = ws;
+		logT[w] = wl;
+	}
+	*bad = nbad;
+}
+
+static std::string
+cachePath()
+{
+	std::string dir;
+	if(const char* env = getenv("NEMO_B200_CACHE_DIR")) {
+		dir = env;
+	} else {
+		Dl_info info;
+		if(dladdr((void*) &cachePath, &info) && info.dli_fname) {
+			std::string lib = info.dli_fname;
+			size_t slash = lib.rfind('/');
+			dir = (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/data";
+		} else {
+			dir = "data";
+		}
+	}
+	return dir + "/libm_tables_v1_glibc-" + gnu_get_libc_version() + ".bin";
+}
+
+static bool
+loadCache(const std::string& path, LibmTables& t)
+{
+	FILE* f = fopen(path.c_str(), "rb");
+	if(!f) return false;
+	uint32_t hdr[3] = {0, 0, 0};
+	char ver[32] = {0};
+	bool ok = fread(hdr, sizeof(hdr), 1, f) == 1 && fread(ver, sizeof(ver), 1, f) == 1
+		&& hdr[0] == FILE_MAGIC && hdr[1] == FILE_VERSION && hdr[2] == TABLE_WORDS
+		&& strncmp(ver, gnu_get_libc_version(), sizeof(ver)) == 0;
+	if(ok) {
+		t.sinCodes.resize(TABLE_WORDS);
+		t.logCodes.resize(TABLE_WORDS);
+		ok = fread(t.sinCodes.data(), 4, TABLE_WORDS, f) == TABLE_WORDS
+			&& fread(t.logCodes.data(), 4, TABLE_WORDS, f) == TABLE_WORDS;
+	}
+	fclose(f);
+	return ok;
+}
+
+static void
+saveCache(const std::string& path, const LibmTables& t)
+{
+	size_t slash = path.rfind('/');
+	if(slash != std::string::npos) {
+		mkdir(path.substr(0, slash).c_str(), 0755);
+	}
+	std::string tmp = path + ".tmp." + std::to_string(getpid());
+	FILE* f = fopen(tmp.c_str(), "wb");
+	if(!f) return; /* read-only location: keep the in-memory tables */
+	uint32_t hdr[3] = {FILE_MAGIC, FILE_VERSION, TABLE_WORDS};
+	char ver[32] = {0};
+	strncpy(ver, gnu_get_libc_version(), sizeof(ver) - 1);
+	bool ok = fwrite(hdr, sizeof(hdr), 1, f) == 1 && fwrite(ver, sizeof(ver), 1, f) == 1
+		&& fwrite(t.sinCodes.data(), 4, TABLE_WORDS, f) == TABLE_WORDS
+		&& fwrite(t.logCodes.data(), 4, TABLE_WORDS, f) == TABLE_WORDS;
+	ok = (fclose(f) == 0) && ok;
+	if(ok) {
+		rename(tmp.c_str(), path.c_str());
+	} else {
+		remove(tmp.c_str());
+	}
+}
+
+LibmTables
+buildLibmTables()
+{
+	LibmTables t;
+	t.sinCodes.assign(TABLE_WORDS, 0);
+	t.logCodes.assign(TABLE_WORDS, 0);
+	unsigned nthreads = std::max(1u, std::thread::hardware_concurrency());
+	std::vector<std::thread> pool;
+	std::vector<unsigned long> bad(nthreads, 0);
+	uint32_t per = (TABLE_WORDS + nthreads - 1) / nthreads;
+	for(unsigned i = 0; i < nthreads; ++i) {
+		uint32_t w0 = std::min<uint32_t>(TABLE_WORDS, i * per);
+		uint32_t w1 = std::min<uint32_t>(TABLE_WORDS, w0 + per);
+		pool.emplace_back(buildRange, w0, w1, t.sinCodes.data(), t.logCodes.data(), &bad[i]);
+	}
+	for(auto& th : pool) th.join();
+	unsigned long nbad = 0;
+	for(unsigned long b : bad) nbad += b;
+	if(nbad) {
+		fail(NEMO_LOGIC_ERROR, "libm correction tables: " + std::to_string(nbad)
+				+ " inputs differ from glibc by more than one unit in the last place");
+	}
+	return t;
+}
+
+const LibmTables&
+libmTables()
+{
+	static std::mutex lock;
+	static LibmTables tables;
+	static bool ready = false;
+	std::lock_guard<std::mutex> guard(lock);
+	if(!ready) {
+		std::string path = cachePath();
+		if(!loadCache(path, tables)) {
+			tables = buildLibmTables();
+			saveCache(path, tables);
+		}
+		ready = true;
+	}
+	return tables;
+}
+
+std::string
+libmCachePath()
+{
+	return cachePath();
+}
+
+} // namespace nemo_b200

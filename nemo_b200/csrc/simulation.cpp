@@ -1,0 +1,841 @@
+/* Host orchestration of the B200 backend (see simulation.hpp).
+ *
+ * Construction compiles the network into the device layout of kernels.hpp
+ * with linear-time counting sorts; error precedence follows the reference
+ * (src/nemo/nemo.cpp:110-134, cpu/Simulation.cpp:36-82,
+ * ConnectivityMatrix.cpp:65-93): empty network, STDP window vs. max delay,
+ * max delay > 64, duplicate neurons, STDP constants, then the first invalid
+ * synapse in synapse-iteration order (ascending source, then id). */
+
+#include "simulation.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <sstream>
+#include <thread>
+
+#include "libm_match.cuh"
+#include "libm_tables.hpp"
+
+namespace nemo_b200 {
+
+static inline uint64_t shl64(uint64_t x, unsigned n) { return x << (n & 63); }
+
+static inline cudaStream_t STREAM(void* s) { return static_cast<cudaStream_t>(s); }
+
+/* src/nemo/fixedpoint.cpp:17-29 */
+static int32_t
+toFix(float f, unsigned fbits)
+{
+	if(std::abs(int(f)) >= 1 << (31 - fbits)) {
+		std::ostringstream msg;
+		msg << "Fixed-point overflow. Value " << f << " does not fit into fixed-point format Q"
+			<< 31 - fbits << "." << fbits;
+		throw std::runtime_error(msg.str());
+	}
+	return static_cast<int32_t>(f * (1 << fbits));
+}
+
+static bool
+fitsFix(float f, unsigned fbits)
+{
+	return !(std::abs(int(f)) >= 1 << (31 - fbits));
+}
+
+static float
+fixToFloat(int32_t v, unsigned fbits)
+{
+	return float(v) / float(1 << fbits);
+}
+
+void*
+Simulation::alloc(size_t bytes)
+{
+	void* p = nullptr;
+	if(bytes == 0) bytes = 16;
+	NEMO_CUDA(cudaMalloc(&p, bytes));
+	m_allocs.push_back(p);
+	NEMO_CUDA(cudaMemsetAsync(p, 0, bytes, STREAM(m_stream)));
+	return p;
+}
+
+Simulation::Simulation(const Network& net, const Configuration& conf) :
+	m_nNeurons(net.neuronCount()),
+	m_nDev(0),
+	m_maxDelay(net.maxDelay()),
+	m_fbits(conf.fractionalBits),
+	m_nsyn(net.synapseCount()),
+	m_nrcm(0),
+	m_stdpOn(conf.hasStdp),
+	m_stdpFn(conf.stdp),
+	m_ring(1024),
+	m_writeOnly(conf.writeOnlySynapses),
+	m_fcmHostValid(false),
+	m_cycle(0),
+	m_counter(0),
+	m_timerBase(0),
+	m_stateDirty(false),
+	m_stream(nullptr),
+	m_dCounter(nullptr),
+	m_hWords(nullptr),
+	m_hStim(nullptr),
+	m_hCur(nullptr),
+	m_dStim(nullptr),
+	m_dCur(nullptr),
+	m_stimCap(0),
+	m_graphExec(nullptr),
+	m_graphCycles(0)
+{
+	std::memset(&m_net, 0, sizeof(m_net));
+	std::memset(&m_rule, 0, sizeof(m_rule));
+
+	if(m_nNeurons == 0) {
+		fail(NEMO_INVALID_INPUT, "Cannot create simulation from empty network");
+	}
+	if(m_stdpOn) {
+		m_stdpFn.verifyDynamicWindowLength(net.maxDelay());
+	}
+	if(m_maxDelay > 64) {
+		fail(NEMO_INVALID_INPUT, "The network has synapses with delay " + std::to_string(m_maxDelay)
+				+ "ms. The B200 backend supports a maximum of 64 ms");
+	}
+
+	/* ---- neurons: simulation order = type registration order ---- */
+	uint32_t local = 0, devPos = 0;
+	std::vector<const std::vector<uint32_t>*> groupGidx;
+	for(const NeuronGroup& ng : net.groups) {
+		uint32_t n = uint32_t(ng.gidx.size());
+		if(n == 0) continue;
+		if(ng.type.kind == MODEL_COUNT || ng.type.kind == MODEL_HH) {
+			fail(NEMO_API_UNSUPPORTED, "The B200 backend has no kernel for neuron model " + ng.type.name);
+		}
+		Group g;
+		g.type = ng.type;
+		g.localBase = local;
+		g.devBase = devPos;
+		g.count = n;
+		g.param.resize(size_t(ng.type.nParam) * n);
+		g.state.resize(size_t(ng.type.nState) * n);
+		for(unsigned p = 0; p < ng.type.nParam; ++p)
+			std::copy(ng.param[p].begin(), ng.param[p].end(), g.param.begin() + size_t(p) * n);
+		for(unsigned s = 0; s < ng.type.nState; ++s)
+			std::copy(ng.state[s].begin(), ng.state[s].end(), g.state.begin() + size_t(s) * n);
+		for(uint32_t i = 0; i < n; ++i) {
+			if(!m_g2d.emplace(ng.gidx[i], devPos + i).second) {
+				fail(NEMO_INVALID_INPUT, "Duplicate neuron index " + std::to_string(ng.gidx[i]));
+			}
+		}
+		m_groups.push_back(std::move(g));
+		groupGidx.push_back(&ng.gidx);
+		local += n;
+		devPos = uint32_t(roundUp(uint64_t(devPos) + n, 32));
+	}
+	m_nDev = std::max<uint32_t>(devPos, 32);
+	if(uint64_t(m_nDev) >= (uint64_t(1) << 26)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^26 neurons per simulation");
+	}
+	m_d2g.assign(m_nDev, ~0u);
+	m_d2group.assign(m_nDev, -1);
+	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
+		const Group& g = m_groups[gi];
+		for(uint32_t i = 0; i < g.count; ++i) {
+			m_d2g[g.devBase + i] = (*groupGidx[gi])[i];
+			m_d2group[g.devBase + i] = int32_t(gi);
+		}
+	}
+	/* dense user -> device table when the user indices are compact */
+	uint32_t lo = ~0u, hi = 0;
+	for(const auto& kv : m_g2d) { lo = std::min(lo, kv.first); hi = std::max(hi, kv.first); }
+	bool dense = uint64_t(hi) - lo + 1 <= std::max<uint64_t>(uint64_t(m_nNeurons) * 4, 1u << 20);
+	std::vector<uint32_t> denseMap;
+	if(dense) {
+		denseMap.assign(size_t(hi) - lo + 1, ~0u);
+		for(const auto& kv : m_g2d) denseMap[kv.first - lo] = kv.second;
+	}
+	auto map = [&](uint32_t gidx) -> uint32_t {
+		if(dense) {
+			return (gidx >= lo && gidx <= hi) ? denseMap[gidx - lo] : ~0u;
+		}
+		auto it = m_g2d.find(gidx);
+		return it == m_g2d.end() ? ~0u : it->second;
+	};
+
+	/* ---- STDP constants (src/nemo/StdpProcess.cpp:20-46) ---- */
+	if(m_stdpOn) {
+		m_rule.minE = toFix(m_stdpFn.minE, m_fbits);
+		m_rule.maxE = toFix(m_stdpFn.maxE, m_fbits);
+		m_rule.minI = toFix(m_stdpFn.minI, m_fbits);
+		m_rule.maxI = toFix(m_stdpFn.maxI, m_fbits);
+		for(size_t i = 0; i < m_stdpFn.prefire.size(); ++i) m_rule.fnPre[i] = toFix(m_stdpFn.prefire[i], m_fbits);
+		for(size_t i = 0; i < m_stdpFn.postfire.size(); ++i) m_rule.fnPost[i] = toFix(m_stdpFn.postfire[i], m_fbits);
+		unsigned nPre = unsigned(m_stdpFn.prefire.size());
+		unsigned nPost = unsigned(m_stdpFn.postfire.size());
+		m_rule.potentiation = m_stdpFn.potentiationBits();
+		m_rule.depression = m_stdpFn.depressionBits();
+		m_rule.prePostBits = shl64(~shl64(~uint64_t(0), nPre), nPost);
+		m_rule.postPreBits = ~shl64(~uint64_t(0), nPost);
+		m_rule.postPreWindow = nPost;
+	}
+
+	/* ---- synapse validation: first failure in iteration order ---- */
+	const size_t S = m_nsyn;
+	{
+		size_t bad = S;
+		int badKind = 0;
+		for(size_t s = 0; s < S; ++s) {
+			int kind = 0;
+			if(map(net.src[s]) == ~0u) kind = 1;
+			else if(map(net.tgt[s]) == ~0u) kind = 2;
+			else if(!fitsFix(net.wgt[s], m_fbits)) kind = 3;
+			if(kind && (bad == S || net.src[s] < net.src[bad]
+						|| (net.src[s] == net.src[bad] && net.sid[s] < net.sid[bad]))) {
+				bad = s;
+				badKind = kind;
+			}
+		}
+		if(bad != S) {
+			if(badKind == 1) fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(net.src[bad]));
+			if(badKind == 2) fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(net.tgt[bad]));
+			toFix(net.wgt[bad], m_fbits); /* throws the overflow error */
+		}
+	}
+	if(S >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 synapses per simulation");
+	}
+
+	/* ---- forward matrix: rows (source, delay), insertion order within a row ---- */
+	const uint32_t Ds = std::max<uint32_t>(m_maxDelay, 1);
+	const size_t nrows = size_t(m_nDev) * Ds;
+	std::vector<uint64_t> rowStart(nrows + 1, 0);
+	std::vector<uint32_t> dsrc(S), dtgt(S);
+	for(size_t s = 0; s < S; ++s) {
+		dsrc[s] = map(net.src[s]);
+		dtgt[s] = map(net.tgt[s]);
+		rowStart[size_t(dsrc[s]) * Ds + net.dly[s] - 1 + 1]++;
+	}
+	for(size_t r = 0; r < nrows; ++r) rowStart[r + 1] += rowStart[r];
+	std::vector<uint2> fcm(S);
+	std::vector<uint32_t> fcmPos(S);
+	std::vector<uint64_t> delayBits(m_nDev, 0);
+	std::vector<uint32_t> outDegree(m_nDev, 0);
+	{
+		std::vector<uint64_t> fill(rowStart.begin(), rowStart.end() - 1);
+		for(size_t s = 0; s < S; ++s) {
+			size_t r = size_t(dsrc[s]) * Ds + net.dly[s] - 1;
+			uint64_t pos = fill[r]++;
+			fcm[pos] = make_uint2(dtgt[s], uint32_t(toFix(net.wgt[s], m_fbits)));
+			fcmPos[s] = uint32_t(pos);
+			delayBits[dsrc[s]] |= uint64_t(1) << (net.dly[s] - 1);
+			outDegree[dsrc[s]]++;
+		}
+	}
+	/* deliverable delays: the reference masks the history with
+	 * ~(~0 << maxDelay), a shift evaluated modulo 64 on x86-64
+	 * (src/nemo/cpu/Simulation.cpp:264) */
+	uint64_t validSpikes = ~shl64(~uint64_t(0), m_maxDelay);
+	uint64_t qCap = 0;
+	for(uint32_t n = 0; n < m_nDev; ++n) {
+		delayBits[n] &= validSpikes;
+		qCap += __builtin_popcountll(delayBits[n]);
+	}
+	uint32_t slots = 2;
+	while(slots <= m_maxDelay) slots *= 2;
+
+	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
+	std::vector<uint64_t> rcmStart;
+	std::vector<uint32_t> rcmSrcDelay, rcmForward;
+	if(m_stdpOn) {
+		rcmStart.assign(size_t(m_nDev) + 1, 0);
+		for(size_t s = 0; s < S; ++s) if(net.plastic[s]) rcmStart[dtgt[s] + 1]++;
+		for(uint32_t n = 0; n < m_nDev; ++n) rcmStart[n + 1] += rcmStart[n];
+		m_nrcm = rcmStart[m_nDev];
+		rcmSrcDelay.resize(m_nrcm);
+		rcmForward.resize(m_nrcm);
+		std::vector<uint64_t> fill(rcmStart.begin(), rcmStart.end() - 1);
+		for(size_t s = 0; s < S; ++s) {
+			if(!net.plastic[s]) continue;
+			uint64_t j = fill[dtgt[s]]++;
+			rcmSrcDelay[j] = (dsrc[s] << 6) | (net.dly[s] - 1);
+			rcmForward[j] = fcmPos[s];
+		}
+	}
+
+	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
+	if(!m_writeOnly) {
+		net.indexBySource();
+		m_auxRange = net.m_srcRange;
+		m_aux.resize(S);
+		for(size_t k = 0; k < S; ++k) {
+			size_t s = net.m_bySource[k];
+			m_aux[k] = Aux{fcmPos[s], net.tgt[s], uint8_t(net.dly[s]), net.plastic[s]};
+		}
+	}
+
+	/* ---- device ---- */
+	if(conf.cudaDevice >= 0) {
+		NEMO_CUDA(cudaSetDevice(conf.cudaDevice));
+	}
+	cudaStream_t stream;
+	NEMO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+	m_stream = stream;
+
+	auto put = [&](const void* host, size_t bytes) -> void* {
+		void* d = alloc(bytes);
+		if(bytes) NEMO_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream));
+		return d;
+	};
+
+	m_net.nDev = m_nDev;
+	m_net.nWords = m_nDev / 32;
+	m_net.rowStride = Ds;
+	m_net.qMask = slots - 1;
+	m_net.qCap = std::max<uint64_t>(qCap, 1);
+	m_net.ringMask = m_ring - 1;
+	m_net.fbits = m_fbits;
+	m_dCounter = (uint32_t*) alloc(sizeof(uint32_t));
+	m_net.cycleBase = m_dCounter;
+	m_net.rowStart = (const uint64_t*) put(rowStart.data(), rowStart.size() * 8);
+	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
+	m_net.delayBits = (const uint64_t*) put(delayBits.data(), delayBits.size() * 8);
+	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
+	m_net.queue = (uint32_t*) alloc(size_t(slots) * m_net.qCap * 4);
+	m_net.queueFill = (uint32_t*) alloc(size_t(slots) * 4);
+	m_net.acc = (long long*) alloc(size_t(m_nDev) * 16);
+	m_net.recentFiring = (uint64_t*) alloc(size_t(m_nDev) * 8);
+	m_net.firedRing = (uint32_t*) alloc(size_t(m_ring) * m_net.nWords * 4);
+	m_net.eventsRing = (unsigned long long*) alloc(size_t(m_ring) * 8);
+	m_net.firedCountRing = (uint32_t*) alloc(size_t(m_ring) * 4);
+	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
+	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
+	m_net.stdp = m_stdpOn ? 1 : 0;
+	if(m_stdpOn) {
+		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
+		m_net.postList = (uint32_t*) alloc(size_t(m_nDev) * 2 * 4);
+		m_net.postCount = (uint32_t*) alloc(2 * 4);
+		m_net.rcmStart = (const uint64_t*) put(rcmStart.data(), rcmStart.size() * 8);
+		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
+		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
+		m_net.rcmAcc = (int32_t*) alloc(size_t(m_nrcm) * 4);
+	}
+
+	/* per-neuron RNG seeds by simulation index (src/nemo/RNG.cpp:39-62):
+	 * outputs 4i..4i+3 of a default-seeded mt19937, reduced to [0, 2^31) by
+	 * Boost's uniform_int (bucket size 2, i.e. >> 1) */
+	std::mt19937 mt;
+	bool needTables = false;
+	for(Group& g : m_groups) {
+		g.dParam = (float*) put(g.param.data(), g.param.size() * 4);
+		g.dState = (float*) put(g.state.data(), g.state.size() * 4);
+		std::vector<uint4> seeds(g.count);
+		for(uint32_t i = 0; i < g.count; ++i) {
+			uint32_t a = mt() >> 1, b = mt() >> 1, c = mt() >> 1, d = mt() >> 1;
+			seeds[i] = make_uint4(a, b, c, d);
+		}
+		g.dRng = (uint4*) put(seeds.data(), seeds.size() * 16);
+		needTables = needTables || g.type.kind == MODEL_IZHIKEVICH;
+	}
+	if(needTables) {
+		const LibmTables& t = libmTables();
+		m_net.sinTab = (const uint32_t*) put(t.sinCodes.data(), t.sinCodes.size() * 4);
+		m_net.logTab = (const uint32_t*) put(t.logCodes.data(), t.logCodes.size() * 4);
+	}
+
+	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords) * 4));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	m_wallStart = std::chrono::steady_clock::now();
+}
+
+Simulation::~Simulation()
+{
+	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
+	if(m_graphExec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
+	for(void* p : m_allocs) cudaFree(p);
+	if(m_hWords) cudaFreeHost(m_hWords);
+	if(m_hStim) cudaFreeHost(m_hStim);
+	if(m_hCur) cudaFreeHost(m_hCur);
+	if(m_dStim) cudaFree(m_dStim);
+	if(m_dCur) cudaFree(m_dCur);
+	if(m_stream) cudaStreamDestroy(STREAM(m_stream));
+}
+
+uint32_t
+Simulation::devIndex(unsigned gidx) const
+{
+	auto it = m_g2d.find(gidx);
+	if(it == m_g2d.end()) {
+		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(gidx));
+	}
+	return it->second;
+}
+
+Simulation::Group&
+Simulation::groupOfDev(uint32_t dev, uint32_t* i)
+{
+	Group& g = m_groups.at(size_t(m_d2group.at(dev)));
+	*i = dev - g.devBase;
+	return g;
+}
+
+const Simulation::Group&
+Simulation::groupOfDev(uint32_t dev, uint32_t* i) const
+{
+	const Group& g = m_groups.at(size_t(m_d2group.at(dev)));
+	*i = dev - g.devBase;
+	return g;
+}
+
+void
+Simulation::launchCycle(uint32_t offset)
+{
+	launchGather(m_net, offset, m_stream);
+	bool first = true;
+	for(const Group& g : m_groups) {
+		GroupDev gd;
+		gd.devBase = g.devBase;
+		gd.count = g.count;
+		gd.timerBase = uint32_t(m_timerBase);
+		gd.param = g.dParam;
+		gd.state = g.dState;
+		gd.rng = g.dRng;
+		launchUpdate(int(g.type.kind), m_net, gd, offset, first, m_stream);
+		first = false;
+	}
+	if(m_stdpOn) {
+		launchStdp(m_net, m_rule, offset, m_stream);
+	}
+}
+
+void
+Simulation::decodeFired(const uint32_t* words, std::vector<unsigned>& out) const
+{
+	out.clear();
+	for(uint32_t w = 0; w < m_net.nWords; ++w) {
+		uint32_t bits = words[w];
+		while(bits) {
+			uint32_t b = uint32_t(__builtin_ctz(bits));
+			bits &= bits - 1;
+			out.push_back(m_d2g[w * 32 + b]);
+		}
+	}
+}
+
+/* src/nemo/nemo_c.cpp:439-461 and cpu/Simulation.cpp:140-163: firing
+ * stimulus, then current stimulus; an invalid index raises after the entries
+ * before it have been applied. */
+const std::vector<unsigned>&
+Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
+{
+	cudaStream_t stream = STREAM(m_stream);
+	size_t need = nf + ni;
+	if(need > m_stimCap) {
+		if(m_hStim) cudaFreeHost(m_hStim);
+		if(m_hCur) cudaFreeHost(m_hCur);
+		if(m_dStim) cudaFree(m_dStim);
+		if(m_dCur) cudaFree(m_dCur);
+		m_stimCap = std::max<size_t>(need, 1024);
+		NEMO_CUDA(cudaMallocHost((void**) &m_hStim, m_stimCap * 4));
+		NEMO_CUDA(cudaMallocHost((void**) &m_hCur, m_stimCap * 4));
+		NEMO_CUDA(cudaMalloc((void**) &m_dStim, m_stimCap * 4));
+		NEMO_CUDA(cudaMalloc((void**) &m_dCur, m_stimCap * 4));
+	}
+	uint32_t nfOk = 0, niOk = 0;
+	int err = 0;
+	unsigned badIdx = 0;
+	for(size_t k = 0; k < nf; ++k) {
+		auto it = m_g2d.find(fstim[k]);
+		if(it == m_g2d.end()) { err = 1; badIdx = fstim[k]; break; }
+		m_hStim[nfOk++] = it->second;
+	}
+	if(!err && ni) {
+		/* last write wins for repeated neurons */
+		std::unordered_map<uint32_t, uint32_t> seen;
+		uint32_t* idx = m_hStim + nfOk;
+		for(size_t k = 0; k < ni; ++k) {
+			auto it = m_g2d.find(inidx[k]);
+			if(it == m_g2d.end()) { err = 1; badIdx = inidx[k]; break; }
+			auto s = seen.find(it->second);
+			if(s != seen.end()) {
+				m_hCur[s->second] = icur[k];
+			} else {
+				seen.emplace(it->second, niOk);
+				idx[niOk] = it->second;
+				m_hCur[niOk] = icur[k];
+				niOk++;
+			}
+		}
+	}
+	if(nfOk + niOk) {
+		NEMO_CUDA(cudaMemcpyAsync(m_dStim, m_hStim, size_t(nfOk + niOk) * 4, cudaMemcpyHostToDevice, stream));
+		if(niOk) NEMO_CUDA(cudaMemcpyAsync(m_dCur, m_hCur, size_t(niOk) * 4, cudaMemcpyHostToDevice, stream));
+		StimDev sd{m_dStim, nfOk, m_dStim + nfOk, m_dCur, niOk};
+		launchStimulus(m_net, sd, m_stream);
+	}
+	if(err) {
+		NEMO_CUDA(cudaStreamSynchronize(stream));
+		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
+	}
+
+	launchCycle(uint32_t(m_cycle - m_counter));
+	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
+				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	NEMO_CUDA(cudaGetLastError());
+	m_cycle++;
+	m_stateDirty = true;
+	decodeFired(m_hWords, m_fired);
+	return m_fired;
+}
+
+void
+Simulation::buildGraph(unsigned cycles)
+{
+	cudaStream_t stream = STREAM(m_stream);
+	if(m_graphExec) {
+		cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
+		m_graphExec = nullptr;
+	}
+	cudaGraph_t graph;
+	NEMO_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+	for(unsigned k = 0; k < cycles; ++k) {
+		launchCycle(k);
+	}
+	launchAdvanceCycle(m_dCounter, cycles, m_stream);
+	NEMO_CUDA(cudaStreamEndCapture(stream, &graph));
+	cudaGraphExec_t exec;
+	NEMO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+	cudaGraphDestroy(graph);
+	m_graphExec = exec;
+	m_graphCycles = cycles;
+}
+
+void
+Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
+{
+	if(cycles == 0) return;
+	if(cycles > m_ring) {
+		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
+	}
+	cudaStream_t stream = STREAM(m_stream);
+	if(m_counter != m_cycle) {
+		uint32_t c = uint32_t(m_cycle);
+		NEMO_CUDA(cudaMemcpyAsync(m_dCounter, &c, 4, cudaMemcpyHostToDevice, stream));
+		NEMO_CUDA(cudaStreamSynchronize(stream));
+		m_counter = m_cycle;
+	}
+	if(!m_graphExec || m_graphCycles != cycles) {
+		buildGraph(cycles);
+	}
+	NEMO_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(m_graphExec), stream));
+	uint64_t first = m_cycle;
+	m_cycle += cycles;
+	m_counter += cycles;
+	m_stateDirty = true;
+	if(firedCounts || events) {
+		std::vector<uint32_t> fc(m_ring);
+		std::vector<uint64_t> ev(m_ring);
+		NEMO_CUDA(cudaMemcpyAsync(fc.data(), m_net.firedCountRing, m_ring * 4, cudaMemcpyDeviceToHost, stream));
+		NEMO_CUDA(cudaMemcpyAsync(ev.data(), m_net.eventsRing, m_ring * 8, cudaMemcpyDeviceToHost, stream));
+		NEMO_CUDA(cudaStreamSynchronize(stream));
+		for(unsigned k = 0; k < cycles; ++k) {
+			uint32_t slot = uint32_t(first + k) & m_net.ringMask;
+			if(firedCounts) firedCounts[k] = fc[slot];
+			if(events) events[k] = ev[slot];
+		}
+	}
+}
+
+void
+Simulation::synchronize()
+{
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+	NEMO_CUDA(cudaGetLastError());
+}
+
+const std::vector<unsigned>&
+Simulation::firedAt(uint64_t cycle)
+{
+	if(cycle >= m_cycle || m_cycle - cycle > m_ring) {
+		fail(NEMO_INVALID_INPUT, "firing of cycle " + std::to_string(cycle) + " is no longer (or not yet) available");
+	}
+	uint32_t slot = uint32_t(cycle) & m_net.ringMask;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
+				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, STREAM(m_stream)));
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+	decodeFired(m_hWords, m_fired);
+	return m_fired;
+}
+
+/* src/nemo/ConnectivityMatrix.cpp:272-325 */
+void
+Simulation::applyStdp(float reward)
+{
+	if(!m_stdpOn) {
+		fail(NEMO_LOGIC_ERROR, "applyStdp called, but no STDP model specified");
+	}
+	int32_t fx = toFix(reward, m_fbits);
+	if(fx == 0 && reward != 0) {
+		std::ostringstream msg;
+		msg << "STDP reward rounded down to zero. The smallest valid reward is " << fixToFloat(1, m_fbits);
+		fail(NEMO_INVALID_INPUT, msg.str());
+	}
+	if(m_nrcm) {
+		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
+	}
+	m_fcmHostValid = false;
+}
+
+void
+Simulation::syncStateToHost()
+{
+	if(!m_stateDirty) return;
+	cudaStream_t stream = STREAM(m_stream);
+	for(Group& g : m_groups) {
+		if(!g.state.empty()) {
+			NEMO_CUDA(cudaMemcpyAsync(g.state.data(), g.dState, g.state.size() * 4, cudaMemcpyDeviceToHost, stream));
+		}
+	}
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	m_stateDirty = false;
+}
+
+static void
+checkVar(unsigned i, unsigned n, const char* what)
+{
+	if(i >= n) {
+		fail(NEMO_INVALID_INPUT, std::string("Invalid ") + what + " index " + std::to_string(i));
+	}
+}
+
+float
+Simulation::getNeuronState(unsigned gidx, unsigned var)
+{
+	uint32_t i;
+	Group& g = groupOfDev(devIndex(gidx), &i);
+	checkVar(var, g.type.nState, "state variable");
+	syncStateToHost();
+	return g.state[size_t(var) * g.count + i];
+}
+
+float
+Simulation::getNeuronParameter(unsigned gidx, unsigned param) const
+{
+	uint32_t i;
+	const Group& g = groupOfDev(devIndex(gidx), &i);
+	checkVar(param, g.type.nParam, "parameter");
+	return g.param[size_t(param) * g.count + i];
+}
+
+float
+Simulation::getMembranePotential(unsigned gidx)
+{
+	uint32_t i;
+	Group& g = groupOfDev(devIndex(gidx), &i);
+	return getNeuronState(gidx, g.type.membranePotential);
+}
+
+void
+Simulation::setNeuron(unsigned gidx, unsigned nargs, const float* args)
+{
+	uint32_t i;
+	Group& g = groupOfDev(devIndex(gidx), &i);
+	if(nargs != g.type.nParam + g.type.nState) {
+		std::ostringstream msg;
+		msg << "Unexpected number of parameters/state variables when modifying neuron. Expected "
+			<< g.type.nParam + g.type.nState << ", found " << nargs;
+		fail(NEMO_INVALID_INPUT, msg.str());
+	}
+	syncStateToHost();
+	cudaStream_t stream = STREAM(m_stream);
+	for(unsigned p = 0; p < g.type.nParam; ++p) {
+		float* h = &g.param[size_t(p) * g.count + i];
+		*h = args[p];
+		NEMO_CUDA(cudaMemcpyAsync(g.dParam + size_t(p) * g.count + i, h, 4, cudaMemcpyHostToDevice, stream));
+	}
+	for(unsigned s = 0; s < g.type.nState; ++s) {
+		float* h = &g.state[size_t(s) * g.count + i];
+		*h = args[g.type.nParam + s];
+		NEMO_CUDA(cudaMemcpyAsync(g.dState + size_t(s) * g.count + i, h, 4, cudaMemcpyHostToDevice, stream));
+	}
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+}
+
+void
+Simulation::setNeuronState(unsigned gidx, unsigned var, float val)
+{
+	uint32_t i;
+	Group& g = groupOfDev(devIndex(gidx), &i);
+	checkVar(var, g.type.nState, "state variable");
+	syncStateToHost();
+	float* h = &g.state[size_t(var) * g.count + i];
+	*h = val;
+	NEMO_CUDA(cudaMemcpyAsync(g.dState + size_t(var) * g.count + i, h, 4, cudaMemcpyHostToDevice, STREAM(m_stream)));
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+}
+
+void
+Simulation::setNeuronParameter(unsigned gidx, unsigned param, float val)
+{
+	uint32_t i;
+	Group& g = groupOfDev(devIndex(gidx), &i);
+	checkVar(param, g.type.nParam, "parameter");
+	float* h = &g.param[size_t(param) * g.count + i];
+	*h = val;
+	NEMO_CUDA(cudaMemcpyAsync(g.dParam + size_t(param) * g.count + i, h, 4, cudaMemcpyHostToDevice, STREAM(m_stream)));
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+}
+
+/* src/nemo/ConnectivityMatrix.cpp:329-362 */
+const std::vector<synapse_id>&
+Simulation::getSynapsesFrom(unsigned source)
+{
+	if(m_writeOnly) {
+		fail(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
+	}
+	uint32_t n = 0;
+	auto it = m_auxRange.find(source);
+	if(it == m_auxRange.end()) {
+		if(m_g2d.find(source) == m_g2d.end()) {
+			fail(NEMO_INVALID_INPUT, "Non-existing source neuron id (" + std::to_string(source) + ") in synapse id query");
+		}
+	} else {
+		n = it->second.second;
+	}
+	m_queried.resize(n);
+	for(uint32_t i = 0; i < n; ++i) {
+		m_queried[i] = (uint64_t(source) << 32) | i;
+	}
+	return m_queried;
+}
+
+/* src/nemo/ConnectivityMatrix.cpp:374-391 */
+const Simulation::Aux&
+Simulation::aux(synapse_id id) const
+{
+	if(m_writeOnly) {
+		fail(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
+	}
+	uint32_t neuron = uint32_t(id >> 32);
+	auto it = m_auxRange.find(neuron);
+	if(it == m_auxRange.end()) {
+		fail(NEMO_INVALID_INPUT, "Non-existing neuron id (" + std::to_string(neuron) + ") in synapse query");
+	}
+	uint32_t idx = uint32_t(id & 0xffffffffu);
+	if(idx >= it->second.second) {
+		throw std::out_of_range("synapse index out of range");
+	}
+	return m_aux[it->second.first + idx];
+}
+
+unsigned Simulation::getSynapseTarget(synapse_id id) const { return aux(id).target; }
+unsigned Simulation::getSynapseDelay(synapse_id id) const { return aux(id).delay; }
+unsigned char Simulation::getSynapsePlastic(synapse_id id) const { return aux(id).plastic; }
+
+float
+Simulation::getSynapseWeight(synapse_id id)
+{
+	const Aux& a = aux(id);
+	if(!m_fcmHostValid) {
+		m_fcmHost.resize(m_nsyn);
+		if(m_nsyn) {
+			NEMO_CUDA(cudaMemcpyAsync(m_fcmHost.data(), m_net.fcm, m_nsyn * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
+			NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+		}
+		m_fcmHostValid = true;
+	}
+	return fixToFloat(int32_t(m_fcmHost[a.fcmPos].y), m_fbits);
+}
+
+unsigned long
+Simulation::elapsedWallclock() const
+{
+	return (unsigned long) std::chrono::duration_cast<std::chrono::milliseconds>(
+			std::chrono::steady_clock::now() - m_wallStart).count();
+}
+
+void
+Simulation::resetTimer()
+{
+	m_wallStart = std::chrono::steady_clock::now();
+	m_timerBase = m_cycle;
+	if(m_graphExec) {
+		cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
+		m_graphExec = nullptr;
+		m_graphCycles = 0;
+	}
+}
+
+void
+Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n)
+{
+	const LibmTables& t = libmTables();
+	cudaStream_t stream = STREAM(m_stream);
+	uint32_t *d1, *d2, *ds, *dl;
+	float* dout;
+	NEMO_CUDA(cudaMalloc(&d1, n * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&d2, n * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&dout, n * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&ds, t.sinCodes.size() * 4));
+	NEMO_CUDA(cudaMalloc(&dl, t.logCodes.size() * 4));
+	NEMO_CUDA(cudaMemcpyAsync(d1, u1, n * 4, cudaMemcpyHostToDevice, stream));
+	NEMO_CUDA(cudaMemcpyAsync(d2, u2, n * 4, cudaMemcpyHostToDevice, stream));
+	NEMO_CUDA(cudaMemcpyAsync(ds, t.sinCodes.data(), t.sinCodes.size() * 4, cudaMemcpyHostToDevice, stream));
+	NEMO_CUDA(cudaMemcpyAsync(dl, t.logCodes.data(), t.logCodes.size() * 4, cudaMemcpyHostToDevice, stream));
+	launchNrandProbe(d1, d2, dout, n, ds, dl, m_stream);
+	NEMO_CUDA(cudaMemcpyAsync(out, dout, n * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	cudaFree(d1);
+	cudaFree(d2);
+	cudaFree(dout);
+	cudaFree(ds);
+	cudaFree(dl);
+}
+
+uint64_t
+Simulation::libmCheck()
+{
+	using namespace libm;
+	const LibmTables& t = libmTables();
+	cudaStream_t stream = STREAM(m_stream);
+	float *dsin, *dlog;
+	uint32_t *ds, *dl;
+	NEMO_CUDA(cudaMalloc(&dsin, size_t(TABLE_ENTRIES) * 4));
+	NEMO_CUDA(cudaMalloc(&dlog, size_t(TABLE_ENTRIES) * 4));
+	NEMO_CUDA(cudaMalloc(&ds, t.sinCodes.size() * 4));
+	NEMO_CUDA(cudaMalloc(&dl, t.logCodes.size() * 4));
+	NEMO_CUDA(cudaMemcpyAsync(ds, t.sinCodes.data(), t.sinCodes.size() * 4, cudaMemcpyHostToDevice, stream));
+	NEMO_CUDA(cudaMemcpyAsync(dl, t.logCodes.data(), t.logCodes.size() * 4, cudaMemcpyHostToDevice, stream));
+	launchLibmEval(dsin, dlog, ds, dl, m_stream);
+	std::vector<float> hs(TABLE_ENTRIES), hl(TABLE_ENTRIES);
+	NEMO_CUDA(cudaMemcpyAsync(hs.data(), dsin, size_t(TABLE_ENTRIES) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaMemcpyAsync(hl.data(), dlog, size_t(TABLE_ENTRIES) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	cudaFree(dsin);
+	cudaFree(dlog);
+	cudaFree(ds);
+	cudaFree(dl);
+	unsigned nth = std::max(1u, std::thread::hardware_concurrency());
+	std::vector<uint64_t> bad(nth, 0);
+	std::vector<std::thread> pool;
+	for(unsigned k = 0; k < nth; ++k) {
+		pool.emplace_back([&, k]() {
+			for(uint32_t idx = k; idx < TABLE_ENTRIES; idx += nth) {
+				float fu = libm_value(idx);
+				volatile float gs = sinf(sin_argument(fu));
+				volatile float gl = logf(log_argument(fu));
+				if(f2u(gs) != f2u(hs[idx]) || f2u(gl) != f2u(hl[idx])) bad[k]++;
+			}
+		});
+	}
+	for(auto& th : pool) th.join();
+	uint64_t total = 0;
+	for(uint64_t b : bad) total += b;
+	return total;
+}
+
+} // namespace nemo_b200

@@ -1,0 +1,151 @@
+#ifndef NEMO_B200_SIMULATION_HPP
+#define NEMO_B200_SIMULATION_HPP
+
+/* The B200 simulation backend: the role of the reference's
+ * nemo::SimulationBackend implementations (src/nemo/SimulationBackend.hpp:
+ * 45-147, cpu/Simulation.cpp, cuda/Simulation.cpp), with the per-cycle work
+ * done by the kernels of kernels.cu. */
+
+#include <chrono>
+#include <cstdint>
+#include <unordered_map>
+#include <vector>
+
+#include "kernels.hpp"
+#include "network.hpp"
+
+namespace nemo_b200 {
+
+class Simulation {
+public:
+	Simulation(const Network& net, const Configuration& conf);
+	~Simulation();
+
+	/* One cycle with stimulus; returns the fired neurons (user indices) in
+	 * ascending simulation order (src/nemo/nemo_c.cpp:439-461). */
+	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
+			const unsigned* inidx, const float* icur, size_t ni);
+
+	/* Device-resident run of `cycles` cycles without stimulus, captured as a
+	 * CUDA graph; per-cycle fired counts and synaptic events (fired x
+	 * out-degree) are returned when the pointers are non-null. */
+	void run(unsigned cycles, uint32_t* firedCounts, uint64_t* events);
+
+	/* Fired neurons of one of the last cycles run (device firing ring). */
+	const std::vector<unsigned>& firedAt(uint64_t cycle);
+
+	void applyStdp(float reward);
+
+	float getNeuronState(unsigned gidx, unsigned var);
+	float getNeuronParameter(unsigned gidx, unsigned param) const;
+	float getMembranePotential(unsigned gidx);
+	void setNeuron(unsigned gidx, unsigned nargs, const float* args);
+	void setNeuronState(unsigned gidx, unsigned var, float val);
+	void setNeuronParameter(unsigned gidx, unsigned param, float val);
+
+	const std::vector<synapse_id>& getSynapsesFrom(unsigned source);
+	unsigned getSynapseTarget(synapse_id id) const;
+	unsigned getSynapseDelay(synapse_id id) const;
+	float getSynapseWeight(synapse_id id);
+	unsigned char getSynapsePlastic(synapse_id id) const;
+
+	unsigned long elapsedWallclock() const;
+	unsigned long elapsedSimulation() const { return (unsigned long) (m_cycle - m_timerBase); }
+	void resetTimer();
+
+	uint64_t cycle() const { return m_cycle; }
+	size_t synapseCount() const { return m_nsyn; }
+	unsigned neuronCount() const { return m_nNeurons; }
+	void synchronize();
+
+	/* device-side probe of the noise generator (tests) */
+	void nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n);
+
+	/* Evaluate the device sinf/logf on all reachable noise inputs and count
+	 * the results that differ from host glibc (tests; expected 0). */
+	uint64_t libmCheck();
+
+private:
+	struct Group {
+		NeuronType type;
+		uint32_t localBase;   /* contiguous simulation index of the first neuron */
+		uint32_t devBase;     /* device index (multiple of 32) */
+		uint32_t count;
+		std::vector<float> param;   /* host copy, [nParam][count] */
+		std::vector<float> state;   /* host copy, [nState][count] */
+		float* dParam = nullptr;
+		float* dState = nullptr;
+		uint4* dRng = nullptr;
+	};
+
+	struct Aux {            /* per synapse, in per-source id order */
+		uint32_t fcmPos;
+		uint32_t target;    /* user index */
+		uint8_t delay;
+		uint8_t plastic;
+	};
+
+	uint32_t devIndex(unsigned gidx) const;
+	Group& groupOfDev(uint32_t dev, uint32_t* i);
+	const Group& groupOfDev(uint32_t dev, uint32_t* i) const;
+	const Aux& aux(synapse_id id) const;
+	void launchCycle(uint32_t offset);
+	void syncStateToHost();
+	void buildGraph(unsigned cycles);
+	void* alloc(size_t bytes);
+	void decodeFired(const uint32_t* words, std::vector<unsigned>& out) const;
+
+	unsigned m_nNeurons;
+	uint32_t m_nDev;
+	uint32_t m_maxDelay;
+	uint32_t m_fbits;
+	size_t m_nsyn;
+	uint64_t m_nrcm;
+	std::vector<Group> m_groups;
+	std::unordered_map<uint32_t, uint32_t> m_g2d;  /* user index -> device index */
+	std::vector<uint32_t> m_d2g;                   /* device index -> user index (~0: padding) */
+	std::vector<int32_t> m_d2group;                /* device index -> group (-1: padding) */
+
+	NetDev m_net;
+	bool m_stdpOn;
+	StdpRule m_rule;
+	StdpFunction m_stdpFn;
+	uint32_t m_ring;
+
+	/* synapse queries */
+	bool m_writeOnly;
+	std::unordered_map<uint32_t, std::pair<size_t, uint32_t>> m_auxRange;
+	std::vector<Aux> m_aux;
+	std::vector<synapse_id> m_queried;
+	std::vector<uint2> m_fcmHost;
+	bool m_fcmHostValid;
+
+	/* state */
+	uint64_t m_cycle;          /* cycles simulated */
+	uint64_t m_counter;        /* value of the device cycle counter */
+	uint64_t m_timerBase;
+	bool m_stateDirty;
+	std::chrono::steady_clock::time_point m_wallStart;
+
+	void* m_stream;
+	std::vector<void*> m_allocs;
+	uint32_t* m_dCounter;
+
+	/* pinned staging */
+	uint32_t* m_hWords;        /* one firing bitmap */
+	uint32_t* m_hStim;         /* fstim + istim indices */
+	float* m_hCur;
+	uint32_t* m_dStim;
+	float* m_dCur;
+	size_t m_stimCap;
+
+	std::vector<unsigned> m_fired;
+	std::vector<uint32_t> m_stimScratch;
+
+	void* m_graphExec;
+	unsigned m_graphCycles;
+};
+
+} // namespace nemo_b200
+
+#endif

@@ -1,0 +1,107 @@
+"""CPU checks of the product library boundary: it loads, exports every entry
+point declared in include/*.h, and its host-side network construction and
+queries agree with the oracle (no GPU needed for these calls)."""
+
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from nemo_b200 import netgen
+from nemo_b200.nemo import PRODUCT_LIBRARY, Library, NemoError, Network
+
+
+def _declared_functions():
+    names = []
+    for h in ("nemo.h", "nemo_b200.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"\b(nemo_\w+)\s*\(", text)
+    return sorted(set(n for n in names if not n.endswith("_t")))
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(PRODUCT_LIBRARY), "build with __graft_entry__.build()"
+    out = subprocess.check_output(["nm", "-D", "--defined-only", PRODUCT_LIBRARY], text=True)
+    exported = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    declared = _declared_functions()
+    assert len(declared) > 60
+    missing = [n for n in declared if n not in exported]
+    assert not missing, missing
+
+
+def test_oracle_exports_the_reference_abi():
+    from conftest import ensure_oracle
+    out = subprocess.check_output(["nm", "-D", "--defined-only", ensure_oracle()], text=True)
+    exported = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    text = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "nemo.h")).read(), flags=re.S)
+    declared = set(re.findall(r"\b(nemo_\w+)\s*\(", text))
+    assert not [n for n in declared if n not in exported]
+
+
+def test_network_construction_matches_oracle(oracle_lib):
+    gpu = Library()
+    spec = netgen.izhikevich_random(200, 30, dmax=15, seed=9, stdp=True)
+    a = spec.build(Network(gpu))
+    b = spec.build(Network(oracle_lib))
+    assert a.neuron_count() == b.neuron_count() == 200
+    for src in (0, 17, 199):
+        ia, ib = a.get_synapses_from(src), b.get_synapses_from(src)
+        assert list(ia) == list(ib)
+        for sid in ia:
+            assert a.get_synapse_target(sid) == b.get_synapse_target(sid)
+            assert a.get_synapse_delay(sid) == b.get_synapse_delay(sid)
+            assert a.get_synapse_weight(sid) == b.get_synapse_weight(sid)
+            assert a.get_synapse_plastic(sid) == b.get_synapse_plastic(sid)
+    assert a.get_neuron_parameter(5, 2) == b.get_neuron_parameter(5, 2)
+    assert a.get_neuron_state(150, 0) == b.get_neuron_state(150, 0)
+
+
+@pytest.mark.parametrize("which", ["b200", "oracle"])
+def test_network_errors(which, oracle_lib):
+    lib = Library() if which == "b200" else oracle_lib
+    net = Network(lib)
+    with pytest.raises(NemoError) as e:
+        net.add_neuron_type("NoSuchModel")
+    assert e.value.status == 6
+    iz = net.add_neuron_type("Izhikevich")
+    assert net.add_neuron_type("Izhikevich") == iz
+    with pytest.raises(NemoError):
+        net.add_neuron(iz, 0, 1.0, 2.0)
+    with pytest.raises(NemoError):
+        net.add_synapse(0, 1, 0, 1.0, False)
+    with pytest.raises(NemoError):
+        net.get_neuron_state(3, 0)
+    assert len(net.get_synapses_from(12345)) == 0
+    sid = net.add_synapse(7, 8, 3, 0.5, True)
+    assert sid == (7 << 32)
+    assert net.add_synapse(7, 9, 3, 0.5, True) == (7 << 32) | 1
+    with pytest.raises(NemoError) as e:
+        net.get_synapse_target((7 << 32) | 5)
+    assert e.value.status == 14  # std::out_of_range in the reference
+
+
+def test_plugin_descriptors_parse():
+    gpu = Library()
+    net = Network(gpu)
+    for name, nargs in [("Izhikevich", 7), ("IF_curr_exp", 13), ("QIF", 2), ("HH", 5),
+                        ("PoissonSource", 1), ("Input", 0)]:
+        t = net.add_neuron_type(name)
+        net.add_neuron(t, 1000 + t, *([0.0] * nargs))
+
+
+def test_simulation_without_gpu_fails_loudly():
+    """On a machine without a GPU the library reports a CUDA error instead of
+    falling back to any CPU path."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from nemo_b200.nemo import Configuration, Simulation
+    gpu = Library()
+    net = netgen.ring(64).build(Network(gpu))
+    with pytest.raises(NemoError, match="CUDA"):
+        Simulation(net, Configuration(gpu))

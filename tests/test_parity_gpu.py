@@ -1,0 +1,179 @@
+"""Parity of the B200 library with the oracle on the same seeded networks:
+bit-exact firing traces per cycle, bit-exact neuron state (float bits) and
+bit-exact fixed-point weights after STDP. Everything here runs the sm_100a
+kernels through the C ABI."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from nemo_b200 import netgen
+from nemo_b200.nemo import Configuration, Library, Network, Simulation
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(spec, oracle_lib, stdp=None, write_only=False):
+    sims = []
+    for lib in (Library(), oracle_lib):
+        net = spec.build(Network(lib))
+        conf = Configuration(lib)
+        if stdp is not None:
+            pre, post, limits = stdp
+            conf.set_stdp_function(pre, post, *limits)
+        if write_only:
+            conf.set_write_only_synapses()
+        if lib is oracle_lib:
+            conf.set_cpu_backend()
+        sims.append((net, Simulation(net, conf)))
+    return sims[0], sims[1]
+
+
+def _state_bits(sim, spec, var):
+    return np.array([np.float32(sim.get_neuron_state(int(i), var)).view(np.uint32)
+                     for p in spec.populations for i in p.idx], dtype=np.uint32)
+
+
+def test_libm_exhaustive(oracle_lib):
+    """The device noise path reproduces host glibc sinf/logf on all 83886081
+    reachable inputs."""
+    lib = Library()
+    net = netgen.ring(32).build(Network(lib))
+    sim = Simulation(net, Configuration(lib))
+    mism = ctypes.c_uint64(99)
+    lib.dll.nemo_b200_libm_check.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+    lib.call("nemo_b200_libm_check", sim.handle, ctypes.byref(mism))
+    assert mism.value == 0
+
+
+def test_nrand_probe_matches_glibc():
+    lib = Library()
+    net = netgen.ring(32).build(Network(lib))
+    sim = Simulation(net, Configuration(lib))
+    rng = np.random.default_rng(0)
+    u1 = rng.integers(0, 2**32, 20000, dtype=np.uint64).astype(np.uint32)
+    u2 = rng.integers(0, 2**32, 20000, dtype=np.uint64).astype(np.uint32)
+    edges = np.array([0, 1, 2**24 - 1, 2**24, 2**24 + 1, 2**31, 2**32 - 129, 2**32 - 128, 2**32 - 1], np.uint32)
+    u1 = np.concatenate([u1, edges, edges[::-1]])
+    u2 = np.concatenate([u2, edges[::-1], edges])
+    out = np.empty(u1.size, np.float32)
+    P = ctypes.POINTER
+    lib.dll.nemo_b200_nrand_probe.argtypes = [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_uint32),
+                                              P(ctypes.c_float), ctypes.c_size_t]
+    lib.call("nemo_b200_nrand_probe", sim.handle, u1.ctypes.data_as(P(ctypes.c_uint32)),
+             u2.ctypes.data_as(P(ctypes.c_uint32)), out.ctypes.data_as(P(ctypes.c_float)), u1.size)
+    libm = ctypes.CDLL("libm.so.6")
+    libm.sinf.restype = libm.logf.restype = libm.sqrtf.restype = ctypes.c_float
+    libm.sinf.argtypes = libm.logf.argtypes = libm.sqrtf.argtypes = [ctypes.c_float]
+    C = np.float32(1.4629180792671596810513378043098e-9)
+    S = np.float32(0.00000000023283064365386962890625)
+    for k in range(u1.size):
+        a = np.float32(np.float32(u1[k]) * C)
+        b = np.float32(np.float32(u2[k]) * S)
+        r = np.float32(libm.sqrtf(np.float32(np.float32(-2) * np.float32(libm.logf(np.float32(np.float32(1) - b))))))
+        expected = np.float32(np.float32(libm.sinf(a)) * r)
+        assert np.float32(out[k]).view(np.uint32) == expected.view(np.uint32) or (np.isnan(out[k]) and np.isnan(expected)), k
+
+
+@pytest.mark.parametrize("n,m,cycles,seed", [(1000, 100, 1000, 1), (3000, 50, 300, 2)])
+def test_izhikevich_random_network(oracle_lib, n, m, cycles, seed):
+    """The 1000-neuron benchmark network (thalamic noise sigma 5/2, 100
+    synapses per neuron, delays 1..20): identical firing every cycle and
+    identical u, v bits at the end."""
+    spec = netgen.izhikevich_random(n, m, dmax=20, seed=seed)
+    (_, g), (_, o) = _pair(spec, oracle_lib)
+    total = 0
+    for c in range(cycles):
+        a, b = g.step(), o.step()
+        assert np.array_equal(a, b), "cycle %d" % c
+        total += a.size
+    assert total > cycles  # the network is active
+    assert np.array_equal(_state_bits(g, spec, 0), _state_bits(o, spec, 0))
+    assert np.array_equal(_state_bits(g, spec, 1), _state_bits(o, spec, 1))
+
+
+def test_stdp_network_weights(oracle_lib):
+    """Exponential STDP on excitatory synapses, applyStdp every 100 cycles:
+    identical firing and identical fixed-point weights of every synapse."""
+    spec = netgen.izhikevich_random(2000, 100, dmax=20, seed=4, stdp=True)
+    pre, post = netgen.standard_stdp()
+    (gn, g), (on, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 1.0, 0.0, -1.0)))
+    for epoch in range(4):
+        for c in range(100):
+            a, b = g.step(), o.step()
+            assert np.array_equal(a, b), "epoch %d cycle %d" % (epoch, c)
+        g.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+    for src in range(0, 2000, 7):
+        for sid in g.get_synapses_from(src):
+            assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid)
+
+
+def test_mixed_models_with_stimulus(oracle_lib):
+    """Izhikevich, IF_curr_exp, QIF, PoissonSource and Input populations with
+    random firing and current stimulus every cycle."""
+    f32 = np.float32
+    spec = netgen.mixed_plugins(n_iz=700, n_lif=500, n_qif=300, n_hh=0, m=60, dmax=10, seed=5)
+    rng = np.random.default_rng(3)
+    npois, ninp = 100, 50
+    base = spec.neuron_count
+    spec.populations.append(netgen.Population("PoissonSource", np.arange(base, base + npois, dtype=np.uint32),
+                                              [rng.random(npois, dtype=f32) * f32(0.05)]))
+    spec.populations.append(netgen.Population("Input", np.arange(base + npois, base + npois + ninp, dtype=np.uint32), []))
+    n = base + npois + ninp
+    extra_src = np.arange(base, n, dtype=np.uint32).repeat(20)
+    extra_tgt = rng.integers(0, base, extra_src.size, dtype=np.uint32)
+    spec.source = np.concatenate([spec.source, extra_src])
+    spec.target = np.concatenate([spec.target, extra_tgt])
+    spec.delay = np.concatenate([spec.delay, rng.integers(1, 11, extra_src.size, dtype=np.uint32)])
+    spec.weight = np.concatenate([spec.weight, rng.random(extra_src.size, dtype=f32) * f32(2)])
+    spec.plastic = np.concatenate([spec.plastic, np.zeros(extra_src.size, np.uint8)])
+    (_, g), (_, o) = _pair(spec, oracle_lib)
+    for c in range(400):
+        fstim = np.nonzero(rng.random(n) < 0.01)[0]
+        ii = np.nonzero(rng.random(n) < 0.02)[0]
+        istim = [(int(i), float(rng.normal(5, 5))) for i in ii]
+        a, b = g.step(fstim=fstim, istim=istim), o.step(fstim=fstim, istim=istim)
+        assert np.array_equal(a, b), "cycle %d" % c
+    for p in spec.populations:
+        if p.type_name in ("PoissonSource", "Input"):
+            continue
+        for i in p.idx[::13]:
+            assert np.float32(g.get_membrane_potential(int(i))).view(np.uint32) == \
+                np.float32(o.get_membrane_potential(int(i))).view(np.uint32)
+
+
+def test_device_resident_run_matches_steps(oracle_lib):
+    """nemo_b200_run (CUDA graph of many cycles) gives the same trace as
+    stepping the oracle cycle by cycle."""
+    spec = netgen.izhikevich_random(1500, 100, dmax=20, seed=6, stdp=True)
+    pre, post = netgen.standard_stdp()
+    (_, g), (_, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 1.0, 0.0, -1.0)))
+    lib = g.lib
+    P = ctypes.POINTER
+    lib.dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    lib.dll.nemo_b200_fired_at.argtypes = [ctypes.c_void_p, ctypes.c_uint64, P(P(ctypes.c_uint)), P(ctypes.c_size_t)]
+    # a few ordinary steps first, then graph runs of two different lengths
+    for _ in range(7):
+        assert np.array_equal(g.step(), o.step())
+    cycle = 7
+    for chunk in (100, 250, 100):
+        counts = np.zeros(chunk, np.uint32)
+        events = np.zeros(chunk, np.uint64)
+        lib.call("nemo_b200_run", g.handle, chunk, counts.ctypes.data_as(P(ctypes.c_uint32)),
+                 events.ctypes.data_as(P(ctypes.c_uint64)))
+        outdeg = spec.out_degree()
+        for k in range(chunk):
+            ref = o.step()
+            ptr = P(ctypes.c_uint)()
+            cnt = ctypes.c_size_t()
+            lib.call("nemo_b200_fired_at", g.handle, cycle + k, ctypes.byref(ptr), ctypes.byref(cnt))
+            got = np.ctypeslib.as_array(ptr, shape=(cnt.value,)).copy() if cnt.value else np.zeros(0, np.uint32)
+            assert np.array_equal(got, ref), "cycle %d" % (cycle + k)
+            assert counts[k] == ref.size
+            assert events[k] == int(outdeg[ref].sum())
+        cycle += chunk
+        g.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+    assert np.array_equal(g.step(), o.step())
