@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Synaptic events/s of the NeMo step path on B200.
+
+Workload: the 1e8-synapse STDP network — 100,000 Izhikevich neurons (80%
+excitatory, thalamic noise sigma 5 / 2), 1000 outgoing synapses per neuron
+to uniform targets, delays U{1..20} ms, excitatory weights 0.5*U(0,1)
+(plastic), inhibitory -U(0,1); STDP windows 0.1*exp(-dt/20) /
+-0.12*exp(-dt/20) over 20+20 ms, excitatory weights clipped to [0, 1];
+applyStdp(1.0) every 100 cycles. Seeded synthetic network (numpy PCG64).
+
+One bench step = 100 simulated 1 ms cycles followed by applyStdp(1.0).
+
+  value : synaptic events/s (fired neurons x out-degree, the reference
+          benchmark's unit, src/examples/common.cpp:93-98) of the
+          device-resident step loop (nemo_b200_timed_steps: 100-cycle CUDA
+          graph + applyStdp kernel), timed with CUDA events on the
+          simulation's stream; the 800 MB forward matrix exceeds L2.
+  e2e   : the same metric through the reference-facing C ABI: nemo_step per
+          cycle with a one-neuron firing stimulus copied host->device and the
+          fired list copied device->host every cycle, nemo_apply_stdp every
+          100 cycles; host wall clock.
+  --impl reference : the reference CPU backend (the oracle restatement of
+          src/nemo/cpu/, OpenMP on all host cores) on the same network and
+          the same e2e protocol, rank 0 only.
+
+Multi-GPU (--gpus N under torchrun): N independent replicas of the workload,
+one per GPU (weak scaling); value = all replicas' events / max device time.
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from nemo_b200 import netgen  # noqa: E402
+from nemo_b200.nemo import Configuration, Library, Network, Simulation  # noqa: E402
+
+METRIC = "synaptic events/s"
+UNIT = "events/s"
+CYCLES_PER_STEP = 100
+REWARD = 1.0
+
+
+def workload(small=False):
+    if small:
+        return dict(name="izhikevich-20k-m1000-stdp", n=20000, m=1000, dmax=20, seed=1)
+    return dict(name="izhikevich-100k-m1000-stdp", n=100000, m=1000, dmax=20, seed=1)
+
+
+def build_sim(lib, wl, oracle=False):
+    spec = netgen.izhikevich_random(wl["n"], wl["m"], dmax=wl["dmax"], seed=wl["seed"], stdp=True)
+    net = spec.build(Network(lib))
+    conf = Configuration(lib)
+    pre, post = netgen.standard_stdp()
+    conf.set_stdp_function(pre, post, 0.0, 1.0, 0.0, -1.0)
+    conf.set_write_only_synapses()
+    if oracle:
+        conf.set_cpu_backend()
+    sim = Simulation(net, conf)
+    del net
+    return sim, spec
+
+
+def stim_stream(n, cycles, seed=7):
+    """One random neuron forced to fire per cycle (the reference benchmark's
+    --fstim option, src/examples/common.cpp:64-67)."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, n, size=cycles, dtype=np.uint32)
+
+
+def e2e_steps(sim, n, steps, seed):
+    """K steps through nemo_step / nemo_apply_stdp; returns (seconds, events)."""
+    lib = sim.lib
+    stim = stim_stream(n, steps * CYCLES_PER_STEP, seed)
+    fptr = ctypes.POINTER(ctypes.c_uint)()
+    nfired = ctypes.c_size_t()
+    outdeg = None
+    fired_total = 0
+    step = lib.dll.nemo_step
+    t0 = time.perf_counter()
+    for s in range(steps):
+        for c in range(CYCLES_PER_STEP):
+            one = stim[s * CYCLES_PER_STEP + c: s * CYCLES_PER_STEP + c + 1]
+            status = step(sim.handle, one.ctypes.data_as(ctypes.POINTER(ctypes.c_uint)), 1, None, None, 0,
+                          ctypes.byref(fptr), ctypes.byref(nfired))
+            if status != 0:
+                raise RuntimeError(lib.dll.nemo_strerror().decode())
+            fired_total += nfired.value
+        if lib.dll.nemo_apply_stdp(sim.handle, ctypes.c_float(REWARD)) != 0:
+            raise RuntimeError(lib.dll.nemo_strerror().decode())
+    t1 = time.perf_counter()
+    return t1 - t0, fired_total
+
+
+def run_oracle_steps(wl, warmup, steps, budget_s=None):
+    """The oracle (reference CPU backend restatement, OpenMP on all host
+    cores) on the workload: `warmup` untimed steps, then up to `steps` timed
+    steps of 100 cycles + applyStdp, stopping early after budget_s seconds."""
+    lib = Library(oracle_library())
+    sim, spec = build_sim(lib, wl, oracle=True)
+    m = wl["m"]
+    for s in range(warmup):
+        e2e_steps(sim, wl["n"], 1, seed=100 + s)
+    times, events = [], 0
+    t_start = time.perf_counter()
+    done = 0
+    while done < steps:
+        dt, fired = e2e_steps(sim, wl["n"], 1, seed=1000 + done)
+        times.append(dt)
+        events += fired * m
+        done += 1
+        if budget_s is not None and time.perf_counter() - t_start > budget_s:
+            break
+    total = sum(times)
+    return events / total, done, total
+
+
+def oracle_library():
+    path = os.path.join(ROOT, "oracle", "_build", "libnemo_oracle.so")
+    if not os.path.exists(path):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    return path
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        p = json.load(open(path))
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    t = json.load(open(path)).get(kernel)
+    return t
+
+
+def roofline(sim, lib, wl):
+    """Per-kernel device times over 100 individually launched cycles; the
+    dominant kernel's algorithmic bytes / time against the measured HBM copy
+    bandwidth. Algorithmic bytes: gather 8 B per delivered synapse (u32
+    target + i32 weight); neuron update 92 B per Izhikevich neuron plus the
+    scatter's 16 B per enqueued row; STDP accumulation 20 B per visited
+    synapse; applyStdp 20 B per plastic synapse."""
+    out = (ctypes.c_double * 10)()
+    lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 10]
+    lib.call("nemo_b200_profile", sim.handle, CYCLES_PER_STEP, ctypes.c_float(REWARD), out)
+    tg, tu, ts, delivered, fired, visits, updates, tapply, nplastic, generated = list(out)
+    kernels = {
+        "k_gather": (8.0 * delivered, tg, CYCLES_PER_STEP),
+        "k_update_izhikevich": (92.0 * updates + 16.0 * fired * wl["dmax"], tu, CYCLES_PER_STEP),
+        "k_stdp": (20.0 * visits, ts, CYCLES_PER_STEP),
+        "k_apply_stdp": (20.0 * nplastic, tapply, 1),
+    }
+    peak, peak_kind = measured_peaks()
+    table = {}
+    for k, (bytes_, ms, launches) in kernels.items():
+        gbs = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        table[k] = {"ms_per_launch": ms / launches, "bytes_per_launch": bytes_ / launches, "gbs": gbs,
+                    "share": 0.0}
+    tot = tg + tu + ts + tapply
+    for k, (bytes_, ms, launches) in kernels.items():
+        table[k]["share"] = ms / tot if tot else 0.0
+    dom = max(table, key=lambda k: table[k]["share"])
+    d = table[dom]
+    roof = {"kernel": dom, "bound": "hbm", "achieved": round(d["gbs"], 1), "peak": peak, "unit": "GB/s",
+            "frac": round(d["gbs"] / peak, 4), "peak_source": peak_kind, "traffic": load_traffic(dom),
+            "bytes_per_launch": d["bytes_per_launch"], "ms_per_launch": d["ms_per_launch"],
+            "per_kernel": {k: {kk: (round(vv, 5) if isinstance(vv, float) else vv) for kk, vv in v.items()}
+                           for k, v in table.items()}}
+    return roof
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    wl = workload(args.small)
+    lib = Library()
+    torch.cuda.set_device(local)
+    conf_dev = local
+
+    spec = netgen.izhikevich_random(wl["n"], wl["m"], dmax=wl["dmax"], seed=wl["seed"], stdp=True)
+    net = spec.build(Network(lib))
+    conf = Configuration(lib)
+    pre, post = netgen.standard_stdp()
+    conf.set_stdp_function(pre, post, 0.0, 1.0, 0.0, -1.0)
+    conf.set_write_only_synapses()
+    conf.set_cuda_backend(conf_dev)
+    t_build = time.perf_counter()
+    sim = Simulation(net, conf)
+    t_build = time.perf_counter() - t_build
+    del net
+    m = wl["m"]
+    n = wl["n"]
+
+    lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                              ctypes.c_float, ctypes.c_double * 4]
+    out = (ctypes.c_double * 4)()
+    # warm-up: W steps (graph instantiation, STDP dynamics settle)
+    lib.call("nemo_b200_timed_steps", sim.handle, max(args.warmup, 1), CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        lib.call("nemo_b200_timed_steps", sim.handle, args.steps, CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
+    torch.cuda.synchronize()
+    ms, fired, events, delivered = out[0], out[1], out[2], out[3]
+    if world > 1:
+        t = torch.tensor([ms, events], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, events_all = float(mx[0]), float(t[1])
+    else:
+        ms_max, events_all = ms, events
+    value = events_all / (ms_max * 1e-3)
+
+    # end to end through the C ABI (host buffers, per-cycle copies)
+    e2e_s, e2e_fired = e2e_steps(sim, n, max(1, min(args.steps, 3)), seed=11)
+    e2e_steps_n = max(1, min(args.steps, 3))
+    e2e_value = e2e_fired * m / e2e_s
+    nwords = (n + 31) // 32
+
+    roof = roofline(sim, lib, wl)
+    clk = clocks.summary()
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 fixed point + f32/f64 state",
+        "data": "synthetic (seeded generator, numpy PCG64 seed %d)" % wl["seed"],
+        "config": {"workload": wl["name"], "neurons": n, "synapses_per_neuron": m, "synapses": n * m,
+                   "delays": "U{1..%d}" % wl["dmax"], "stdp": "exc plastic, applyStdp(1.0) every 100 cycles",
+                   "cycles_per_step": CYCLES_PER_STEP, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (800 MB forward matrix)"},
+        "sim_ms_per_wall_s": round(CYCLES_PER_STEP * args.steps / (ms_max * 1e-3), 1),
+        "fired_per_cycle": round(fired / (CYCLES_PER_STEP * args.steps), 1),
+        "delivered_synapses": int(delivered), "build_s": round(t_build, 2),
+        "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
+                "h2d_bytes_per_step": 4 * CYCLES_PER_STEP,
+                "d2h_bytes_per_step": 4 * nwords * CYCLES_PER_STEP,
+                "steps": e2e_steps_n, "s_per_step": round(e2e_s / e2e_steps_n, 4)},
+        "roofline": roof,
+        "gpu_launches": args.steps * (CYCLES_PER_STEP * 3 + 2),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        del sim
+        v, nsteps, secs = run_oracle_steps(wl, 0, args.cpu_steps, budget_s=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": "%d step(s) of 100 cycles + applyStdp from a fresh network, %.1f s, "
+                                          "e2e protocol" % (nsteps, secs)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    wl = workload(args.small)
+    v, nsteps, secs = run_oracle_steps(wl, args.warmup, args.steps, budget_s=args.cpu_seconds * 6)
+    n = wl["n"]
+    line = {
+        "metric": METRIC, "value": round(v, 1), "unit": UNIT, "impl": "reference", "n_gpus": 0,
+        "steps": nsteps, "warmup": args.warmup, "ms_per_step": round(secs * 1000 / nsteps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/int64 fixed point + f32/f64 state", "data": "synthetic (seeded generator)",
+        "config": {"workload": wl["name"], "neurons": n, "synapses_per_neuron": wl["m"],
+                   "cycles_per_step": CYCLES_PER_STEP},
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": "%d step(s) of 100 cycles + applyStdp after %d warm-up step(s)"
+                                   % (nsteps, args.warmup)},
+        "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--small", action="store_true", help="20k-neuron variant (profiling)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -36,6 +36,22 @@ nemo_status_t nemo_b200_cycle(nemo_simulation_t sim, uint64_t* cycle);
 /* Wait for all device work of the simulation. */
 nemo_status_t nemo_b200_synchronize(nemo_simulation_t sim);
 
+/* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`
+ * cycles as one CUDA graph, then applyStdp(reward) when apply_stdp != 0),
+ * bracketed by CUDA events on the simulation's stream. out[0] = device ms,
+ * out[1] = neurons fired, out[2] = synaptic events generated (fired x
+ * out-degree), out[3] = synapses delivered. */
+nemo_status_t nemo_b200_timed_steps(nemo_simulation_t sim, unsigned steps, unsigned cycles_per_step,
+		int apply_stdp, float reward, double out[4]);
+
+/* Per-kernel device times over `cycles` individually launched cycles, then
+ * one applyStdp(reward) when STDP is on. out[0..2] = gather / neuron update
+ * (with scatter) / STDP accumulation ms, out[3] = synapses delivered,
+ * out[4] = neurons fired, out[5] = STDP synapse visits, out[6] = neuron
+ * updates, out[7] = applyStdp ms, out[8] = plastic synapses, out[9] =
+ * synaptic events generated. */
+nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[10]);
+
 /* Diagnostics: the device noise transform of two RNG words per sample,
  * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the
  * Izhikevich kernel (glibc-matching), for n samples. */

@@ -150,6 +150,8 @@ __device__ __forceinline__ void fireEpilogue(const NetDev& net, uint32_t t, uint
 		if(lane == 0) {
 			atomicAdd(&net.eventsRing[slotR], ev);
 			atomicAdd(&net.firedCountRing[slotR], uint32_t(__popc(word)));
+			atomicAdd(&net.stats[2], (unsigned long long) __popc(word));
+			atomicAdd(&net.stats[3], ev);
 		}
 	}
 
@@ -389,15 +391,20 @@ k_gather(NetDev net, uint32_t offset)
 	uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
 	unsigned long long* acc = reinterpret_cast<unsigned long long*>(net.acc);
+	uint64_t delivered = 0;
 	for(uint32_t r = warp; r < nrows; r += nwarps) {
 		uint32_t row = rows[r];
 		uint64_t b = net.rowStart[row];
 		uint64_t e = net.rowStart[row + 1];
+		delivered += e - b;
 		for(uint64_t j = b + lane; j < e; j += 32) {
 			uint2 syn = net.fcm[j];
 			int32_t w = int32_t(syn.y);
 			atomicAdd(&acc[2 * size_t(syn.x) + (w < 0 ? 1 : 0)], (unsigned long long) (long long) w);
 		}
+	}
+	if(lane == 0 && delivered) {
+		atomicAdd(&net.stats[0], (unsigned long long) delivered);
 	}
 }
 
@@ -455,9 +462,11 @@ k_stdp(NetDev net, StdpRule rule, uint32_t offset)
 	uint32_t lane = threadIdx.x & 31u;
 	uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 	uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	uint64_t visited = 0;
 	for(uint32_t w = warp; w < count; w += nwarps) {
 		uint32_t target = list[w];
 		uint64_t b = net.rcmStart[target], e = net.rcmStart[target + 1];
+		visited += e - b;
 		for(uint64_t j = b + lane; j < e; j += 32) {
 			uint32_t sd = net.rcmSrcDelay[j];
 			uint64_t pre = shr64(net.recentFiring[sd >> 6], (sd & 63u) + 1u);
@@ -466,6 +475,9 @@ k_stdp(NetDev net, StdpRule rule, uint32_t offset)
 				net.rcmAcc[j] = int32_t(uint32_t(net.rcmAcc[j]) + uint32_t(dw));
 			}
 		}
+	}
+	if(lane == 0 && visited) {
+		atomicAdd(&net.stats[1], (unsigned long long) visited);
 	}
 }
 

@@ -66,6 +66,11 @@ struct NetDev {
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;
 	const uint32_t* logTab;
+
+	/* cumulative counters: [0] synapses delivered by gather, [1] synapses
+	 * visited by STDP accumulation, [2] neurons fired, [3] synaptic events
+	 * generated (fired x out-degree) */
+	unsigned long long* stats;
 };
 
 struct GroupDev {

@@ -315,6 +315,19 @@ nemo_b200_nrand_probe(nemo_simulation_t s, const uint32_t u1[], const uint32_t u
 }
 
 nemo_status_t
+nemo_b200_timed_steps(nemo_simulation_t s, unsigned steps, unsigned cycles_per_step, int apply_stdp,
+		float reward, double out[4])
+{
+	RETURN_CALL(s->sim.timedSteps(steps, cycles_per_step, apply_stdp != 0, reward, out));
+}
+
+nemo_status_t
+nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out[10])
+{
+	RETURN_CALL(s->sim.profile(cycles, reward, out));
+}
+
+nemo_status_t
 nemo_b200_libm_check(nemo_simulation_t s, uint64_t* mismatches)
 {
 	RETURN_CALL(*mismatches = s->sim.libmCheck());

@@ -312,6 +312,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.firedCountRing = (uint32_t*) alloc(size_t(m_ring) * 4);
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
+	m_net.stats = (unsigned long long*) alloc(4 * 8);
 	m_net.stdp = m_stdpOn ? 1 : 0;
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
@@ -794,6 +795,129 @@ Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_
 	cudaFree(dout);
 	cudaFree(ds);
 	cudaFree(dl);
+}
+
+void
+Simulation::readStats(uint64_t out[4])
+{
+	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 4 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+}
+
+void
+Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4])
+{
+	if(cyclesPerStep == 0 || cyclesPerStep > m_ring) {
+		fail(NEMO_INVALID_INPUT, "timed steps: cycles per step must be in 1.." + std::to_string(m_ring));
+	}
+	if(apply && !m_stdpOn) {
+		fail(NEMO_LOGIC_ERROR, "applyStdp called, but no STDP model specified");
+	}
+	int32_t fx = apply ? toFix(reward, m_fbits) : 0;
+	cudaStream_t stream = STREAM(m_stream);
+	if(m_counter != m_cycle) {
+		uint32_t c = uint32_t(m_cycle);
+		NEMO_CUDA(cudaMemcpyAsync(m_dCounter, &c, 4, cudaMemcpyHostToDevice, stream));
+		m_counter = m_cycle;
+	}
+	if(!m_graphExec || m_graphCycles != cyclesPerStep) {
+		buildGraph(cyclesPerStep);
+	}
+	uint64_t before[4], after[4];
+	readStats(before);
+	cudaEvent_t e0, e1;
+	NEMO_CUDA(cudaEventCreate(&e0));
+	NEMO_CUDA(cudaEventCreate(&e1));
+	NEMO_CUDA(cudaEventRecord(e0, stream));
+	for(unsigned s = 0; s < steps; ++s) {
+		NEMO_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(m_graphExec), stream));
+		if(apply && m_nrcm) {
+			launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
+		}
+	}
+	NEMO_CUDA(cudaEventRecord(e1, stream));
+	NEMO_CUDA(cudaEventSynchronize(e1));
+	float ms = 0;
+	NEMO_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	NEMO_CUDA(cudaGetLastError());
+	m_cycle += uint64_t(steps) * cyclesPerStep;
+	m_counter = m_cycle;
+	m_stateDirty = true;
+	m_fcmHostValid = false;
+	readStats(after);
+	out[0] = ms;
+	out[1] = double(after[2] - before[2]);
+	out[2] = double(after[3] - before[3]);
+	out[3] = double(after[0] - before[0]);
+}
+
+void
+Simulation::profile(unsigned cycles, float reward, double out[10])
+{
+	cudaStream_t stream = STREAM(m_stream);
+	/* all cycles are enqueued before the first wait, so the queue runs ahead
+	 * of the GPU and the events bracket device execution only */
+	std::vector<cudaEvent_t> ev(size_t(cycles) * 4 + 4);
+	for(auto& e : ev) NEMO_CUDA(cudaEventCreate(&e));
+	uint64_t before[4], after[4];
+	readStats(before);
+	for(unsigned c = 0; c < cycles; ++c) {
+		uint32_t offset = uint32_t(m_cycle - m_counter);
+		NEMO_CUDA(cudaEventRecord(ev[4 * c + 0], stream));
+		launchGather(m_net, offset, m_stream);
+		NEMO_CUDA(cudaEventRecord(ev[4 * c + 1], stream));
+		bool first = true;
+		for(const Group& g : m_groups) {
+			GroupDev gd{g.devBase, g.count, uint32_t(m_timerBase), g.dParam, g.dState, g.dRng};
+			launchUpdate(int(g.type.kind), m_net, gd, offset, first, m_stream);
+			first = false;
+		}
+		NEMO_CUDA(cudaEventRecord(ev[4 * c + 2], stream));
+		if(m_stdpOn) {
+			launchStdp(m_net, m_rule, offset, m_stream);
+		}
+		NEMO_CUDA(cudaEventRecord(ev[4 * c + 3], stream));
+		m_cycle++;
+	}
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	double tg = 0, tu = 0, ts = 0;
+	for(unsigned c = 0; c < cycles; ++c) {
+		float a, b, d;
+		NEMO_CUDA(cudaEventElapsedTime(&a, ev[4 * c + 0], ev[4 * c + 1]));
+		NEMO_CUDA(cudaEventElapsedTime(&b, ev[4 * c + 1], ev[4 * c + 2]));
+		NEMO_CUDA(cudaEventElapsedTime(&d, ev[4 * c + 2], ev[4 * c + 3]));
+		tg += a;
+		tu += b;
+		ts += d;
+	}
+	readStats(after);
+	double tapply = 0;
+	if(m_stdpOn && m_nrcm) {
+		int32_t fx = toFix(reward, m_fbits);
+		NEMO_CUDA(cudaEventRecord(ev[0], stream));
+		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
+		NEMO_CUDA(cudaEventRecord(ev[1], stream));
+		NEMO_CUDA(cudaEventSynchronize(ev[1]));
+		float a;
+		NEMO_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+		tapply = a;
+		m_fcmHostValid = false;
+	}
+	for(auto& e : ev) cudaEventDestroy(e);
+	NEMO_CUDA(cudaGetLastError());
+	m_stateDirty = true;
+	out[0] = tg;
+	out[1] = tu;
+	out[2] = ts;
+	out[3] = double(after[0] - before[0]);
+	out[4] = double(after[2] - before[2]);
+	out[5] = double(after[1] - before[1]);
+	out[6] = double(m_nNeurons) * cycles;
+	out[7] = tapply;
+	out[8] = double(m_nrcm);
+	out[9] = double(after[3] - before[3]);
 }
 
 uint64_t

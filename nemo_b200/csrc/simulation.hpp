@@ -65,6 +65,22 @@ public:
 	 * the results that differ from host glibc (tests; expected 0). */
 	uint64_t libmCheck();
 
+	/* Device-timed throughput loop: `steps` x (graph of `cyclesPerStep`
+	 * cycles, then applyStdp(reward) if applyEvery), bracketed by CUDA events
+	 * on the simulation's stream. out: [0] device ms, [1] neurons fired,
+	 * [2] synaptic events generated, [3] synapses delivered. */
+	void timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4]);
+
+	/* Per-stage device times over `cycles` individually launched cycles
+	 * (CUDA events between stages). out: [0] gather ms, [1] update ms,
+	 * [2] stdp ms, [3] synapses delivered, [4] neurons fired,
+	 * [5] STDP synapse visits, [6] neuron updates, [7] applyStdp ms (one
+	 * call after the cycles, when STDP is on), [8] plastic synapses,
+	 * [9] synaptic events generated. */
+	void profile(unsigned cycles, float reward, double out[10]);
+
+	void readStats(uint64_t out[4]);
+
 private:
 	struct Group {
 		NeuronType type;
