@@ -12,9 +12,10 @@ One bench step = 100 simulated 1 ms cycles followed by applyStdp(1.0).
 
   value : synaptic events/s (fired neurons x out-degree, the reference
           benchmark's unit, src/examples/common.cpp:93-98) of the
-          device-resident step loop (nemo_b200_timed_steps: 100-cycle CUDA
-          graph + applyStdp kernel), timed with CUDA events on the
-          simulation's stream; the 800 MB forward matrix exceeds L2.
+          device-resident step loop (nemo_b200_timed_steps: one persistent
+          launch of 100 cycles + the applyStdp kernel per step), timed with
+          CUDA events on the simulation's stream; the 800 MB forward matrix
+          exceeds L2. The default 100 steps are the workload's 10,000 cycles.
   e2e   : the same metric through the reference-facing C ABI: nemo_step per
           cycle with a one-neuron firing stimulus copied host->device and the
           fired list copied device->host every cycle, nemo_apply_stdp every
@@ -203,20 +204,19 @@ def load_traffic(kernel):
 
 
 def roofline(sim, lib, wl):
-    """Per-kernel device times over 100 individually launched cycles; the
-    dominant kernel's algorithmic bytes / time against the measured HBM copy
-    bandwidth. Algorithmic bytes: gather 8 B per delivered synapse (u32
-    target + i32 weight); neuron update 92 B per Izhikevich neuron plus the
-    scatter's 16 B per enqueued row; STDP accumulation 20 B per visited
-    synapse; applyStdp 20 B per plastic synapse."""
+    """Device times of one step's two kernels — the persistent step kernel
+    (100 cycles of update, spike push and STDP accumulation) and applyStdp —
+    and the dominant one's algorithmic bytes / time against the measured HBM
+    copy bandwidth. Algorithmic bytes: spike push 8 B per pushed synapse
+    (packed target/delay + i32 weight); Izhikevich update 92 B per neuron per
+    cycle; STDP accumulation 20 B per visited synapse; applyStdp 20 B per
+    plastic synapse."""
     out = (ctypes.c_double * 10)()
     lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 10]
     lib.call("nemo_b200_profile", sim.handle, CYCLES_PER_STEP, ctypes.c_float(REWARD), out)
-    tg, tu, ts, delivered, fired, visits, updates, tapply, nplastic, generated = list(out)
+    tcyc, blocks, _, pushed, fired, visits, updates, tapply, nplastic, generated = list(out)
     kernels = {
-        "k_gather": (8.0 * delivered, tg, CYCLES_PER_STEP),
-        "k_update_izhikevich": (92.0 * updates + 16.0 * fired * wl["dmax"], tu, CYCLES_PER_STEP),
-        "k_stdp": (20.0 * visits, ts, CYCLES_PER_STEP),
+        "k_cycles": (8.0 * pushed + 92.0 * updates + 20.0 * visits, tcyc, 1),
         "k_apply_stdp": (20.0 * nplastic, tapply, 1),
     }
     peak, peak_kind = measured_peaks()
@@ -225,7 +225,7 @@ def roofline(sim, lib, wl):
         gbs = bytes_ / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
         table[k] = {"ms_per_launch": ms / launches, "bytes_per_launch": bytes_ / launches, "gbs": gbs,
                     "share": 0.0}
-    tot = tg + tu + ts + tapply
+    tot = tcyc + tapply
     for k, (bytes_, ms, launches) in kernels.items():
         table[k]["share"] = ms / tot if tot else 0.0
     dom = max(table, key=lambda k: table[k]["share"])
@@ -234,7 +234,10 @@ def roofline(sim, lib, wl):
             "frac": round(d["gbs"] / peak, 4), "peak_source": peak_kind, "traffic": load_traffic(dom),
             "bytes_per_launch": d["bytes_per_launch"], "ms_per_launch": d["ms_per_launch"],
             "per_kernel": {k: {kk: (round(vv, 5) if isinstance(vv, float) else vv) for kk, vv in v.items()}
-                           for k, v in table.items()}}
+                           for k, v in table.items()},
+            "work_per_step": {"cycles": CYCLES_PER_STEP, "pushed_synapses": int(pushed), "fired": int(fired),
+                              "stdp_visits": int(visits), "neuron_updates": int(updates),
+                              "plastic_synapses": int(nplastic), "grid_blocks": int(blocks)}}
     return roof
 
 
@@ -270,14 +273,17 @@ def run_b200(args):
     lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_double * 4]
     out = (ctypes.c_double * 4)()
-    # warm-up: W steps (graph instantiation, STDP dynamics settle)
-    lib.call("nemo_b200_timed_steps", sim.handle, max(args.warmup, 1), CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+    # the clock sampler runs through warm-up and the timed region, so that the
+    # GPU is under the same load for every sample
     with ClockSampler(local) as clocks:
+        # warm-up: W steps
+        lib.call("nemo_b200_timed_steps", sim.handle, max(args.warmup, 1), CYCLES_PER_STEP, 1,
+                 ctypes.c_float(REWARD), out)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         lib.call("nemo_b200_timed_steps", sim.handle, args.steps, CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
-    torch.cuda.synchronize()
+        torch.cuda.synchronize()
     ms, fired, events, delivered = out[0], out[1], out[2], out[3]
     if world > 1:
         t = torch.tensor([ms, events], dtype=torch.float64, device="cuda")
@@ -315,7 +321,7 @@ def run_b200(args):
                 "d2h_bytes_per_step": 4 * nwords * CYCLES_PER_STEP,
                 "steps": e2e_steps_n, "s_per_step": round(e2e_s / e2e_steps_n, 4)},
         "roofline": roof,
-        "gpu_launches": args.steps * (CYCLES_PER_STEP * 3 + 2),
+        "gpu_launches": args.steps * 2,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -355,7 +361,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--small", action="store_true", help="20k-neuron variant (profiling)")

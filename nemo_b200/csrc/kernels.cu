@@ -4,9 +4,10 @@
  * rounding is observable goes through an explicit round-to-nearest intrinsic
  * (__fadd_rn, __dmul_rn, ...) so that neither contraction nor reassociation can
  * change the operation order of the reference CPU plugins
- * (src/nemo/cpu/plugins/*.cpp). Integer current accumulation is exact and
- * order-independent, which is what makes atomics bit-exact here. */
+ * (src/nemo/cpu/plugins/<Model>.cpp). Integer current accumulation is exact
+ * and order-independent, which is what makes the atomics bit-exact here. */
 
+#include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -19,15 +20,18 @@ namespace nemo_b200 {
 namespace {
 
 const unsigned FULL = 0xffffffffu;
+const unsigned BLOCK = 256;
 
 /* 64-bit shifts by a count that may reach 64, evaluated like the x86-64
  * shift the reference runs on (count modulo 64). */
 __device__ __forceinline__ uint64_t shl64(uint64_t x, unsigned n) { return x << (n & 63u); }
 __device__ __forceinline__ uint64_t shr64(uint64_t x, unsigned n) { return x >> (n & 63u); }
 
-__device__ __forceinline__ uint32_t cycleOf(const NetDev& net, uint32_t offset)
+__device__ __forceinline__ unsigned long long globalTimer()
 {
-	return *net.cycleBase + offset;
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
 }
 
 /* wfx_toFloat: saturate the int64 sum to int32, convert, scale
@@ -52,11 +56,11 @@ __device__ __forceinline__ uint32_t urand(uint4& s)
 
 /* Box-Muller sine branch (src/nemo/RNG.cpp:26-34) with glibc-matching
  * sinf/logf (libm_match.cuh) and IEEE sqrtf. */
-__device__ __forceinline__ float nrand(uint4& s, const uint32_t* sinTab, const uint32_t* logTab)
+__device__ __forceinline__ float nrandWords(uint32_t u1, uint32_t u2, const uint32_t* sinTab, const uint32_t* logTab)
 {
 	using namespace libm;
-	float f1 = __uint2float_rn(urand(s));
-	float f2 = __uint2float_rn(urand(s));
+	float f1 = __uint2float_rn(u1);
+	float f2 = __uint2float_rn(u2);
 	float a = sin_argument(f1);
 	float y = log_argument(f2);
 	float L = apply_code(log_candidate(y), table_code(logTab, libm_index(f2)));
@@ -65,10 +69,17 @@ __device__ __forceinline__ float nrand(uint4& s, const uint32_t* sinTab, const u
 	return __fmul_rn(S, r);
 }
 
-/* Read and clear this cycle's E/I sums of neuron n */
-__device__ __forceinline__ void takeCurrents(const NetDev& net, uint32_t n, float& E, float& I)
+__device__ __forceinline__ float nrand(uint4& s, const uint32_t* sinTab, const uint32_t* logTab)
 {
-	longlong2* acc = reinterpret_cast<longlong2*>(net.acc);
+	uint32_t u1 = urand(s);
+	uint32_t u2 = urand(s);
+	return nrandWords(u1, u2, sinTab, logTab);
+}
+
+/* Read and clear neuron n's E/I sums for the current cycle's slot */
+__device__ __forceinline__ void takeCurrents(const NetDev& net, uint32_t slot, uint32_t n, float& E, float& I)
+{
+	longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
 	longlong2 a = acc[n];
 	if(a.x | a.y) {
 		acc[n] = make_longlong2(0, 0);
@@ -99,312 +110,413 @@ __device__ __forceinline__ uint32_t takeStimWord(const NetDev& net, uint32_t n, 
 	return __shfl_sync(FULL, w, 0);
 }
 
-/* Epilogue shared by all models, run by every lane of a warp that owns the
- * 32 neurons starting at n - lane:
- *  - history shift and firing bitmap of cycle t,
- *  - scatter: every fired neuron enqueues its non-empty rows (one per outgoing
- *    delay d) into spike-queue slot t+d; one atomicAdd per (warp, delay),
- *  - the STDP post-spike list (neurons whose history bit P is set),
- *  - per-cycle counters of fired neurons and synaptic events. */
-__device__ __forceinline__ void fireEpilogue(const NetDev& net, uint32_t t, uint32_t n, uint32_t lane,
-		bool valid, bool fired)
-{
-	uint64_t rf = 0;
-	if(valid) {
-		rf = (net.recentFiring[n] << 1) | uint64_t(fired);
-		net.recentFiring[n] = rf;
-	}
-	uint32_t word = __ballot_sync(FULL, fired);
-	uint32_t slotR = t & net.ringMask;
-	if(lane == 0) {
-		net.firedRing[size_t(slotR) * net.nWords + (n >> 5)] = word;
-	}
-
-	/* scatter into the delay-bucketed spike queue */
-	uint64_t delays = fired ? net.delayBits[n] : 0ull;
-	uint32_t anyLo = __reduce_or_sync(FULL, uint32_t(delays));
-	uint32_t anyHi = __reduce_or_sync(FULL, uint32_t(delays >> 32));
-	uint64_t any = (uint64_t(anyHi) << 32) | anyLo;
-	const uint32_t lt = (1u << lane) - 1u;
-	while(any) {
-		uint32_t k = uint32_t(__ffsll((long long) any) - 1);
-		any &= any - 1;
-		bool has = (delays >> k) & 1ull;
-		uint32_t mask = __ballot_sync(FULL, has);
-		uint32_t slot = (t + k + 1) & net.qMask;
-		uint32_t leader = __ffs(mask) - 1;
-		uint32_t base = 0;
-		if(lane == leader) {
-			base = atomicAdd(&net.queueFill[slot], __popc(mask));
-		}
-		base = __shfl_sync(FULL, base, leader);
-		if(has) {
-			net.queue[size_t(slot) * net.qCap + base + __popc(mask & lt)] = n * net.rowStride + k;
-		}
-	}
-
-	/* counters */
-	if(word) {
-		uint32_t deg = fired ? net.outDegree[n] : 0u;
-		unsigned long long ev = __reduce_add_sync(FULL, deg);
-		if(lane == 0) {
-			atomicAdd(&net.eventsRing[slotR], ev);
-			atomicAdd(&net.firedCountRing[slotR], uint32_t(__popc(word)));
-			atomicAdd(&net.stats[2], (unsigned long long) __popc(word));
-			atomicAdd(&net.stats[3], ev);
-		}
-	}
-
-	/* STDP: targets that fired P cycles ago (src/nemo/ConnectivityMatrix.cpp:237) */
-	if(net.stdp) {
-		bool post = valid && ((rf >> net.postShift) & 1ull);
-		uint32_t pm = __ballot_sync(FULL, post);
-		if(pm) {
-			uint32_t par = t & 1u;
-			uint32_t leader = __ffs(pm) - 1;
-			uint32_t base = 0;
-			if(lane == leader) {
-				base = atomicAdd(&net.postCount[par], __popc(pm));
-			}
-			base = __shfl_sync(FULL, base, leader);
-			if(post) {
-				net.postList[size_t(par) * net.nDev + base + __popc(pm & lt)] = n;
-			}
-		}
-	}
-}
-
-/* Common prologue: cycle, warp-level bounds. Returns false for warps past
- * the group's padded range (they must not touch the next group's words). */
-__device__ __forceinline__ bool groupThread(const NetDev& net, const GroupDev& g, uint32_t offset, bool resetSlot,
-		uint32_t& t, uint32_t& i, uint32_t& n, uint32_t& lane, bool& valid)
-{
-	t = cycleOf(net, offset);
-	i = blockIdx.x * blockDim.x + threadIdx.x;
-	lane = threadIdx.x & 31u;
-	if(resetSlot && i == 0) {
-		/* slot t was drained by this cycle's gather; nothing writes it during
-		 * cycle t because slots > maxDelay */
-		net.queueFill[t & net.qMask] = 0;
-	}
-	if((i & ~31u) >= g.count) {
-		return false;
-	}
-	n = g.devBase + i;
-	valid = i < g.count;
-	return true;
-}
-
-/* ---------------- neuron models ---------------- */
+/* ---------------- neuron models (one neuron per thread) ---------------- */
 
 /* Izhikevich (src/nemo/cpu/plugins/Izhikevich.cpp:53-97). Parameters a, b, c,
  * d, sigma; state u, v. The v update evaluates its bracket in double (double
  * literals in the reference), the u update in float. */
-__global__ void __launch_bounds__(256)
-k_update_izhikevich(NetDev net, GroupDev g, uint32_t offset, int resetSlot)
+__device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		uint32_t slot, bool stim)
 {
-	uint32_t t, i, n, lane;
-	bool valid;
-	if(!groupThread(net, g, offset, resetSlot, t, i, n, lane, valid)) return;
-	uint32_t stim = takeStimWord(net, n, lane);
-	bool fired = false;
-	if(valid) {
-		const size_t c = g.count;
-		float E, I;
-		takeCurrents(net, n, E, I);
-		float In = __fadd_rn(__fadd_rn(E, I), takeExternal(net, n));
-		float sigma = g.param[4 * c + i];
-		if(sigma != 0.0f) {
-			uint4 s = g.rng[i];
-			In = __fadd_rn(In, __fmul_rn(sigma, nrand(s, net.sinTab, net.logTab)));
-			g.rng[i] = s;
-		}
-		float a = g.param[0 * c + i];
-		float b = g.param[1 * c + i];
-		float u = g.state[0 * c + i];
-		float v = g.state[1 * c + i];
-		for(int k = 0; k < 4; ++k) {
-			if(!fired) {
-				double vd = double(v);
-				double br = __dadd_rn(__dsub_rn(__dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(0.04, vd), 5.0), vd), 140.0),
-							double(u)), double(In));
-				v = __double2float_rn(__dadd_rn(vd, __dmul_rn(0.25, br)));
-				u = __fadd_rn(u, __fmul_rn(0.25f, __fmul_rn(a, __fsub_rn(__fmul_rn(b, v), u))));
-				fired = v >= 30.0f;
-			}
-		}
-		fired = fired || ((stim >> lane) & 1u);
-		if(fired) {
-			v = g.param[2 * c + i];
-			u = __fadd_rn(u, g.param[3 * c + i]);
-		}
-		g.state[0 * c + i] = u;
-		g.state[1 * c + i] = v;
+	const size_t c = g.count;
+	float E, I;
+	takeCurrents(net, slot, n, E, I);
+	float In = __fadd_rn(__fadd_rn(E, I), takeExternal(net, n));
+	float sigma = g.param[4 * c + i];
+	if(sigma != 0.0f) {
+		uint4 s = g.rng[i];
+		In = __fadd_rn(In, __fmul_rn(sigma, nrand(s, net.sinTab, net.logTab)));
+		g.rng[i] = s;
 	}
-	fireEpilogue(net, t, n, lane, valid, fired);
+	float a = g.param[0 * c + i];
+	float b = g.param[1 * c + i];
+	float u = g.state[0 * c + i];
+	float v = g.state[1 * c + i];
+	bool fired = false;
+	for(int k = 0; k < 4; ++k) {
+		if(!fired) {
+			double vd = double(v);
+			double br = __dadd_rn(__dsub_rn(__dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(0.04, vd), 5.0), vd), 140.0),
+						double(u)), double(In));
+			v = __double2float_rn(__dadd_rn(vd, __dmul_rn(0.25, br)));
+			u = __fadd_rn(u, __fmul_rn(0.25f, __fmul_rn(a, __fsub_rn(__fmul_rn(b, v), u))));
+			fired = v >= 30.0f;
+		}
+	}
+	fired = fired || stim;
+	if(fired) {
+		v = g.param[2 * c + i];
+		u = __fadd_rn(u, g.param[3 * c + i]);
+	}
+	g.state[0 * c + i] = u;
+	g.state[1 * c + i] = v;
+	return fired;
 }
 
 /* IF_curr_exp (src/nemo/cpu/plugins/IF_curr_exp.cpp:74-121). Parameters in
  * IF_curr_exp.h order; state v, ie, ii, lastfire. Fires on v > v_thresh. */
-__global__ void __launch_bounds__(256)
-k_update_if_curr_exp(NetDev net, GroupDev g, uint32_t offset, int resetSlot)
+__device__ __forceinline__ bool modelIfCurrExp(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		uint32_t slot, bool stim)
 {
-	uint32_t t, i, n, lane;
-	bool valid;
-	if(!groupThread(net, g, offset, resetSlot, t, i, n, lane, valid)) return;
-	uint32_t stim = takeStimWord(net, n, lane);
-	bool fired = false;
-	if(valid) {
-		const size_t c = g.count;
-		const float* P = g.param;
-		float* S = g.state;
-		float E, I;
-		takeCurrents(net, n, E, I);
-		float v_rest = P[0 * c + i], v_reset = P[1 * c + i], c_m = P[2 * c + i], tau_m = P[3 * c + i];
-		float tau_refrac = P[4 * c + i], tau_e = P[5 * c + i], tau_i = P[6 * c + i];
-		float v_thresh = P[7 * c + i], i_offset = P[8 * c + i];
-		float ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_e)), S[1 * c + i]), E);
-		float ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_i)), S[2 * c + i]), I);
-		float In = __fadd_rn(__fadd_rn(__fadd_rn(ie, ii), takeExternal(net, n)), i_offset);
-		S[1 * c + i] = ie;
-		S[2 * c + i] = ii;
-		float v = S[0 * c + i];
-		float lastfire = S[3 * c + i];
-		bool refractory = lastfire <= tau_refrac;
-		if(!refractory) {
-			v = __fadd_rn(v, __fadd_rn(__fdiv_rn(In, c_m), __fdiv_rn(__fsub_rn(v_rest, v), tau_m)));
-		}
-		fired = (!refractory && v > v_thresh) || ((stim >> lane) & 1u);
-		if(fired) {
-			S[3 * c + i] = 1.0f;
-			S[0 * c + i] = v_reset;
-		} else {
-			S[3 * c + i] = __fadd_rn(lastfire, 1.0f);
-			S[0 * c + i] = v;
-		}
+	const size_t c = g.count;
+	const float* P = g.param;
+	float* S = g.state;
+	float E, I;
+	takeCurrents(net, slot, n, E, I);
+	float v_rest = P[0 * c + i], v_reset = P[1 * c + i], c_m = P[2 * c + i], tau_m = P[3 * c + i];
+	float tau_refrac = P[4 * c + i], tau_e = P[5 * c + i], tau_i = P[6 * c + i];
+	float v_thresh = P[7 * c + i], i_offset = P[8 * c + i];
+	float ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_e)), S[1 * c + i]), E);
+	float ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_i)), S[2 * c + i]), I);
+	float In = __fadd_rn(__fadd_rn(__fadd_rn(ie, ii), takeExternal(net, n)), i_offset);
+	S[1 * c + i] = ie;
+	S[2 * c + i] = ii;
+	float v = S[0 * c + i];
+	float lastfire = S[3 * c + i];
+	bool refractory = lastfire <= tau_refrac;
+	if(!refractory) {
+		v = __fadd_rn(v, __fadd_rn(__fdiv_rn(In, c_m), __fdiv_rn(__fsub_rn(v_rest, v), tau_m)));
 	}
-	fireEpilogue(net, t, n, lane, valid, fired);
+	bool fired = (!refractory && v > v_thresh) || stim;
+	if(fired) {
+		S[3 * c + i] = 1.0f;
+		S[0 * c + i] = v_reset;
+	} else {
+		S[3 * c + i] = __fadd_rn(lastfire, 1.0f);
+		S[0 * c + i] = v;
+	}
+	return fired;
 }
 
 /* QIF (src/nemo/cpu/plugins/QIF.cpp:45-106): 10 RK4 substeps of 0.1 ms,
  * threshold 1, reset 0. */
-__global__ void __launch_bounds__(256)
-k_update_qif(NetDev net, GroupDev g, uint32_t offset, int resetSlot)
+__device__ __forceinline__ bool modelQif(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		uint32_t slot, bool stim)
 {
-	uint32_t t, i, n, lane;
-	bool valid;
-	if(!groupThread(net, g, offset, resetSlot, t, i, n, lane, valid)) return;
-	uint32_t stim = takeStimWord(net, n, lane);
+	const float dt = 0.1f;
+	const float a1 = __fmul_rn(0.5f, dt);
+	const float a2 = dt;
+	const float bb1 = __fdiv_rn(dt, 6.0f);
+	float E, I;
+	takeCurrents(net, slot, n, E, I);
+	float X = takeExternal(net, n);
+	float v = g.state[i];
+	float a = g.param[i];
 	bool fired = false;
-	if(valid) {
-		const float dt = 0.1f;
-		const float a1 = __fmul_rn(0.5f, dt);
-		const float a2 = dt;
-		const float bb1 = __fdiv_rn(dt, 6.0f);
-		float E, I;
-		takeCurrents(net, n, E, I);
-		float X = takeExternal(net, n);
-		float v = g.state[i];
-		float a = g.param[i];
-		for(int k = 0; k < 10; ++k) {
-			if(!fired) {
-				float In = __fmul_rn(__fadd_rn(__fadd_rn(E, I), X), 0.015f);
-				float k1 = __fadd_rn(__fmul_rn(__fmul_rn(a, v), __fsub_rn(v, 1.0f)), In);
-				float x2 = __fadd_rn(v, __fmul_rn(a1, k1));
-				float k2 = __fadd_rn(__fmul_rn(__fmul_rn(a, x2), __fsub_rn(x2, 1.0f)), In);
-				float x3 = __fadd_rn(v, __fmul_rn(a1, k2));
-				float k3 = __fadd_rn(__fmul_rn(__fmul_rn(a, x3), __fsub_rn(x3, 1.0f)), In);
-				float x4 = __fadd_rn(v, __fmul_rn(a2, k3));
-				float k4 = __fadd_rn(__fmul_rn(__fmul_rn(a, x4), __fsub_rn(x4, 1.0f)), In);
-				float sum = __fadd_rn(__fadd_rn(__fadd_rn(k1, __fmul_rn(2.0f, k2)), __fmul_rn(2.0f, k3)), k4);
-				v = __fadd_rn(v, __fmul_rn(bb1, sum));
-				fired = v >= 1.0f;
-			}
+	for(int k = 0; k < 10; ++k) {
+		if(!fired) {
+			float In = __fmul_rn(__fadd_rn(__fadd_rn(E, I), X), 0.015f);
+			float k1 = __fadd_rn(__fmul_rn(__fmul_rn(a, v), __fsub_rn(v, 1.0f)), In);
+			float x2 = __fadd_rn(v, __fmul_rn(a1, k1));
+			float k2 = __fadd_rn(__fmul_rn(__fmul_rn(a, x2), __fsub_rn(x2, 1.0f)), In);
+			float x3 = __fadd_rn(v, __fmul_rn(a1, k2));
+			float k3 = __fadd_rn(__fmul_rn(__fmul_rn(a, x3), __fsub_rn(x3, 1.0f)), In);
+			float x4 = __fadd_rn(v, __fmul_rn(a2, k3));
+			float k4 = __fadd_rn(__fmul_rn(__fmul_rn(a, x4), __fsub_rn(x4, 1.0f)), In);
+			float sum = __fadd_rn(__fadd_rn(__fadd_rn(k1, __fmul_rn(2.0f, k2)), __fmul_rn(2.0f, k3)), k4);
+			v = __fadd_rn(v, __fmul_rn(bb1, sum));
+			fired = v >= 1.0f;
 		}
-		fired = fired || ((stim >> lane) & 1u);
-		if(fired) {
-			v = 0.0f;
-		}
-		g.state[i] = v;
 	}
-	fireEpilogue(net, t, n, lane, valid, fired);
+	fired = fired || stim;
+	if(fired) {
+		v = 0.0f;
+	}
+	g.state[i] = v;
+	return fired;
 }
 
-/* PoissonSource (src/nemo/cpu/plugins/PoissonSource.cpp:21-29) */
-__global__ void __launch_bounds__(256)
-k_update_poisson(NetDev net, GroupDev g, uint32_t offset, int resetSlot)
+/* PoissonSource (src/nemo/cpu/plugins/PoissonSource.cpp:21-29). Currents are
+ * cleared (every neuron's slot must be) but unused. */
+__device__ __forceinline__ bool modelPoisson(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		uint32_t slot, bool stim)
 {
-	uint32_t t, i, n, lane;
-	bool valid;
-	if(!groupThread(net, g, offset, resetSlot, t, i, n, lane, valid)) return;
-	uint32_t stim = takeStimWord(net, n, lane);
-	bool fired = false;
-	if(valid) {
-		float E, I;
-		takeCurrents(net, n, E, I); /* currents are cleared but unused */
-		(void) takeExternal(net, n);
-		uint32_t p0 = uint32_t(__fmul_rn(g.param[i], 65536.0f));
-		uint4 s = g.rng[i];
-		uint32_t p1 = urand(s) & 0xffffu;
-		g.rng[i] = s;
-		fired = p1 < p0 || ((stim >> lane) & 1u);
-	}
-	fireEpilogue(net, t, n, lane, valid, fired);
+	float E, I;
+	takeCurrents(net, slot, n, E, I);
+	(void) takeExternal(net, n);
+	uint32_t p0 = uint32_t(__fmul_rn(g.param[i], 65536.0f));
+	uint4 s = g.rng[i];
+	uint32_t p1 = urand(s) & 0xffffu;
+	g.rng[i] = s;
+	return p1 < p0 || stim;
 }
 
 /* Input (src/nemo/cpu/plugins/Input.cpp:56-60) */
-__global__ void __launch_bounds__(256)
-k_update_input(NetDev net, GroupDev g, uint32_t offset, int resetSlot)
+__device__ __forceinline__ bool modelInput(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		uint32_t slot, bool stim)
 {
-	uint32_t t, i, n, lane;
-	bool valid;
-	if(!groupThread(net, g, offset, resetSlot, t, i, n, lane, valid)) return;
-	uint32_t stim = takeStimWord(net, n, lane);
-	bool fired = false;
-	if(valid) {
-		float E, I;
-		takeCurrents(net, n, E, I);
-		(void) takeExternal(net, n);
-		fired = (stim >> lane) & 1u;
-	}
-	fireEpilogue(net, t, n, lane, valid, fired);
+	float E, I;
+	takeCurrents(net, slot, n, E, I);
+	(void) takeExternal(net, n);
+	return stim;
 }
 
-/* ---------------- gather ---------------- */
+/* ---------------- STDP rule (src/nemo/StdpProcess.cpp:68-138) ---------------- */
 
-/* Drain spike-queue slot t: each warp takes a row (source, delay) and adds
- * its weights into the target accumulators, excitatory (w >= 0) into E and
- * inhibitory into I (src/nemo/cpu/Simulation.cpp:293-308). 64-bit integer
- * reductions in L2 are exact in any order. */
-__global__ void __launch_bounds__(256)
-k_gather(NetDev net, uint32_t offset)
+__device__ __forceinline__ int32_t updateRegion(uint64_t arrivals, const StdpRule& R)
 {
-	uint32_t t = cycleOf(net, offset);
-	if(blockIdx.x == 0 && threadIdx.x == 0) {
-		net.eventsRing[t & net.ringMask] = 0;
-		net.firedCountRing[t & net.ringMask] = 0;
-	}
-	uint32_t slot = t & net.qMask;
-	uint32_t nrows = net.queueFill[slot];
-	const uint32_t* rows = net.queue + size_t(slot) * net.qCap;
-	uint32_t lane = threadIdx.x & 31u;
-	uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-	unsigned long long* acc = reinterpret_cast<unsigned long long*>(net.acc);
-	uint64_t delivered = 0;
-	for(uint32_t r = warp; r < nrows; r += nwarps) {
-		uint32_t row = rows[r];
-		uint64_t b = net.rowStart[row];
-		uint64_t e = net.rowStart[row + 1];
-		delivered += e - b;
-		for(uint64_t j = b + lane; j < e; j += 32) {
-			uint2 syn = net.fcm[j];
-			int32_t w = int32_t(syn.y);
-			atomicAdd(&acc[2 * size_t(syn.x) + (w < 0 ? 1 : 0)], (unsigned long long) (long long) w);
+	if(!arrivals) return 0;
+	const uint32_t NONE = 0xffffffffu;
+	uint64_t vpre = arrivals & R.prePostBits;
+	uint32_t dtPre = vpre ? uint32_t(__ffsll((long long) shr64(vpre, R.postPreWindow)) - 1) : NONE;
+	uint64_t vpost = arrivals & R.postPreBits;
+	uint32_t dtPost = vpost ? uint32_t(__clzll((long long) shl64(vpost, 64u - R.postPreWindow))) : NONE;
+	if(dtPre < dtPost) return R.fnPre[dtPre];
+	if(dtPost < dtPre) return R.fnPost[dtPost];
+	return 0;
+}
+
+__device__ __forceinline__ int32_t weightChange(uint64_t pre, const StdpRule& R)
+{
+	return int32_t(uint32_t(updateRegion(pre & R.potentiation, R)) + uint32_t(updateRegion(pre & R.depression, R)));
+}
+
+__device__ __forceinline__ int32_t updatedWeight(int32_t wOld, int32_t wDiff, const StdpRule& R)
+{
+	int32_t sum = int32_t(uint32_t(wOld) + uint32_t(wDiff));
+	if(wOld > 0) return min(R.maxE, max(sum, R.minE));
+	if(wOld < 0) return min(R.minI, max(sum, R.maxI));
+	return 0;
+}
+
+/* ---------------- grid barrier with a bounded wait ---------------- */
+
+/* Sense-reversal barrier over all blocks of the cooperative launch. A block
+ * that waits longer than timeoutNs sets the error word and returns false;
+ * every waiting block also gives up as soon as it sees the error word, so the
+ * kernel always terminates. */
+__device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeoutNs)
+{
+	__shared__ int ok;
+	__syncthreads();
+	if(threadIdx.x == 0) {
+		cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
+		cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(bar[1]);
+		cuda::atomic_ref<unsigned, cuda::thread_scope_device> err(bar[2]);
+		int good = 1;
+		unsigned g = gen.load(cuda::memory_order_acquire);
+		__threadfence();
+		unsigned arrived = count.fetch_add(1u, cuda::memory_order_acq_rel);
+		if(arrived == gridDim.x - 1) {
+			count.store(0u, cuda::memory_order_relaxed);
+			gen.fetch_add(1u, cuda::memory_order_release);
+		} else {
+			unsigned long long start = globalTimer();
+			unsigned spins = 0;
+			while(gen.load(cuda::memory_order_acquire) == g) {
+				if(err.load(cuda::memory_order_relaxed)) {
+					good = 0;
+					break;
+				}
+				if((++spins & 255u) == 0 && globalTimer() - start > timeoutNs) {
+					err.store(1u, cuda::memory_order_relaxed);
+					good = 0;
+					break;
+				}
+				__nanosleep(32);
+			}
 		}
+		__threadfence();
+		ok = good;
 	}
-	if(lane == 0 && delivered) {
-		atomicAdd(&net.stats[0], (unsigned long long) delivered);
+	__syncthreads();
+	return ok != 0;
+}
+
+/* ---------------- the persistent step kernel ---------------- */
+
+__global__ void __launch_bounds__(BLOCK)
+k_cycles(const __grid_constant__ CycleArgs A)
+{
+	extern __shared__ uint32_t shLists[];
+	uint32_t* sFired = shLists;
+	uint32_t* sPost = shLists + A.listCap;
+	__shared__ uint32_t sNFired, sNPost, sPostBase;
+	__shared__ unsigned long long sEvents;
+
+	const NetDev& net = A.net;
+	const uint32_t tid = threadIdx.x;
+	const uint32_t lane = tid & 31u;
+	const uint32_t lt = (1u << lane) - 1u;
+	const uint32_t warpsPerBlock = blockDim.x >> 5;
+	const uint32_t gridWarps = gridDim.x * warpsPerBlock;
+	const uint32_t myWarp = blockIdx.x * warpsPerBlock + (tid >> 5);
+	const uint32_t totalWarps = A.groupWarp[A.ngroups];
+	const size_t nDev = net.nDev;
+
+	for(uint32_t k = 0; k <= A.cycles; ++k) {
+		const uint32_t t = A.firstCycle + k;
+		const bool doUpdate = k < A.cycles;
+
+		if(tid == 0) {
+			sNFired = 0;
+			sNPost = 0;
+			sEvents = 0;
+			if(doUpdate && blockIdx.x == 0) {
+				/* consumed in the previous phase; refilled in the next */
+				if(net.stdp) net.postCount[(t + 1) % 3u] = 0;
+				net.firedCountRing[(t + 1) & net.ringMask] = 0;
+				net.eventsRing[(t + 1) & net.ringMask] = 0;
+			}
+		}
+		__syncthreads();
+
+		/* ---- neuron update of cycle t ---- */
+		if(doUpdate) {
+			const uint32_t slot = t & net.qMask;
+			const uint64_t* rfIn = net.rf + (t & 1u) * nDev;
+			uint64_t* rfOut = net.rf + ((t + 1) & 1u) * nDev;
+			for(uint32_t gw = myWarp; gw < totalWarps; gw += gridWarps) {
+				int gi = 0;
+				while(gw >= A.groupWarp[gi + 1]) ++gi;
+				const GroupDev& G = A.groups[gi];
+				const uint32_t i = (gw - A.groupWarp[gi]) * 32u + lane;
+				const uint32_t n = G.devBase + i;
+				const bool valid = i < G.count;
+				const uint32_t stimWord = takeStimWord(net, n, lane);
+				bool fired = false;
+				if(valid) {
+					const bool stim = (stimWord >> lane) & 1u;
+					switch(G.kind) {
+						case 0: fired = modelIzhikevich(net, G, i, n, slot, stim); break;
+						case 1: fired = modelIfCurrExp(net, G, i, n, slot, stim); break;
+						case 2: fired = modelQif(net, G, i, n, slot, stim); break;
+						case 4: fired = modelPoisson(net, G, i, n, slot, stim); break;
+						default: fired = modelInput(net, G, i, n, slot, stim); break;
+					}
+				}
+				uint64_t rfNew = 0;
+				if(valid) {
+					rfNew = (rfIn[n] << 1) | uint64_t(fired);
+					rfOut[n] = rfNew;
+				}
+				const uint32_t word = __ballot_sync(FULL, fired);
+				if(lane == 0) {
+					net.firedRing[size_t(t & net.ringMask) * net.nWords + (n >> 5)] = word;
+				}
+				if(word) {
+					uint32_t base = 0;
+					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
+					base = __shfl_sync(FULL, base, 0);
+					if(fired) sFired[base + __popc(word & lt)] = n;
+					uint32_t deg = fired ? net.outDegree[n] : 0u;
+					uint32_t ev = __reduce_add_sync(FULL, deg);
+					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
+				}
+				if(net.stdp) {
+					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
+					const bool post = valid && ((rfNew >> net.postShift) & 1ull);
+					const uint32_t pm = __ballot_sync(FULL, post);
+					if(pm) {
+						uint32_t base = 0;
+						if(lane == 0) base = atomicAdd(&sNPost, uint32_t(__popc(pm)));
+						base = __shfl_sync(FULL, base, 0);
+						if(post) sPost[base + __popc(pm & lt)] = n;
+					}
+				}
+			}
+		}
+		__syncthreads();
+
+		if(doUpdate) {
+			if(tid == 0) {
+				if(sNPost) sPostBase = atomicAdd(&net.postCount[t % 3u], sNPost);
+				if(sNFired) {
+					atomicAdd(&net.firedCountRing[t & net.ringMask], sNFired);
+					atomicAdd(&net.eventsRing[t & net.ringMask], sEvents);
+					atomicAdd(&net.stats[2], (unsigned long long) sNFired);
+					atomicAdd(&net.stats[3], sEvents);
+					if(net.deliver) atomicAdd(&net.stats[0], sEvents);
+				}
+			}
+			__syncthreads();
+			uint32_t* postOut = net.postList + size_t(t % 3u) * nDev + sPostBase;
+			for(uint32_t j = tid; j < sNPost; j += blockDim.x) {
+				postOut[j] = sPost[j];
+			}
+
+			/* ---- spike push: fired sources stream their synapses into the
+			 * current slots of cycles t + delay ---- */
+			if(net.deliver) {
+				unsigned long long* acc = reinterpret_cast<unsigned long long*>(net.acc);
+				const uint32_t stride = blockDim.x;
+				for(uint32_t f = 0; f < sNFired; ++f) {
+					const uint32_t s = sFired[f];
+					const uint64_t b = net.rowStart[size_t(s) * net.rowStride];
+					const uint64_t e = net.rowStart[size_t(s + 1) * net.rowStride];
+					for(uint64_t j0 = b + tid; j0 < e; j0 += 4 * uint64_t(stride)) {
+						uint2 syn[4];
+#pragma unroll
+						for(int u = 0; u < 4; ++u) {
+							uint64_t j = j0 + uint64_t(u) * stride;
+							syn[u] = j < e ? net.fcm[j] : make_uint2(0u, 0u);
+						}
+#pragma unroll
+						for(int u = 0; u < 4; ++u) {
+							if(j0 + uint64_t(u) * stride < e) {
+								const uint32_t target = syn[u].x >> 6;
+								const uint32_t slot = (t + (syn[u].x & 63u) + 1u) & net.qMask;
+								const int32_t w = int32_t(syn[u].y);
+								atomicAdd(&acc[(size_t(slot) * nDev + target) * 2 + (w < 0 ? 1 : 0)],
+										(unsigned long long) (long long) w);
+							}
+						}
+					}
+				}
+			}
+		}
+
+		/* ---- STDP accumulation of cycle t-1 (ConnectivityMatrix.cpp:224-258):
+		 * 128-synapse chunks of each post-spiking target, one chunk per warp;
+		 * every accumulator has a single writer ---- */
+		if(net.stdp && k > 0) {
+			const uint32_t tp = t - 1;
+			const uint32_t buf = tp % 3u;
+			const uint32_t cnt = net.postCount[buf];
+			const uint32_t* list = net.postList + size_t(buf) * nDev;
+			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
+			const uint32_t items = cnt * net.stdpChunks;
+			uint64_t visited = 0;
+			for(uint32_t it = myWarp; it < items; it += gridWarps) {
+				const uint32_t target = list[it / net.stdpChunks];
+				const uint64_t end = net.rcmStart[target + 1];
+				const uint64_t b = net.rcmStart[target] + uint64_t(it % net.stdpChunks) * 128u;
+				if(b >= end) continue;
+				const uint64_t e = b + 128u < end ? b + 128u : end;
+				visited += e - b;
+				uint32_t sd[4];
+#pragma unroll
+				for(int u = 0; u < 4; ++u) {
+					uint64_t j = b + lane + 32u * u;
+					sd[u] = j < e ? net.rcmSrcDelay[j] : 0u;
+				}
+				uint64_t pre[4];
+#pragma unroll
+				for(int u = 0; u < 4; ++u) {
+					uint64_t j = b + lane + 32u * u;
+					pre[u] = j < e ? shr64(rfAfter[sd[u] >> 6], (sd[u] & 63u) + 1u) : 0ull;
+				}
+#pragma unroll
+				for(int u = 0; u < 4; ++u) {
+					uint64_t j = b + lane + 32u * u;
+					if(j < e) {
+						int32_t dw = weightChange(pre[u], A.rule);
+						if(dw != 0) {
+							net.rcmAcc[j] = int32_t(uint32_t(net.rcmAcc[j]) + uint32_t(dw));
+						}
+					}
+				}
+			}
+			if(lane == 0 && visited) {
+				atomicAdd(&net.stats[1], (unsigned long long) visited);
+			}
+		}
+
+		if(k < A.cycles) {
+			if(!gridSync(net.barrier, A.timeoutNs)) {
+				return;
+			}
+		}
 	}
 }
 
@@ -424,75 +536,9 @@ k_stimulus(NetDev net, StimDev s)
 	}
 }
 
-/* ---------------- STDP ---------------- */
-
-/* src/nemo/StdpProcess.cpp:68-113 */
-__device__ __forceinline__ int32_t updateRegion(uint64_t arrivals, const StdpRule& R)
-{
-	if(!arrivals) return 0;
-	const uint32_t NONE = 0xffffffffu;
-	uint64_t vpre = arrivals & R.prePostBits;
-	uint32_t dtPre = vpre ? uint32_t(__ffsll((long long) shr64(vpre, R.postPreWindow)) - 1) : NONE;
-	uint64_t vpost = arrivals & R.postPreBits;
-	uint32_t dtPost = vpost ? uint32_t(__clzll((long long) shl64(vpost, 64u - R.postPreWindow))) : NONE;
-	if(dtPre < dtPost) return R.fnPre[dtPre];
-	if(dtPost < dtPre) return R.fnPost[dtPost];
-	return 0;
-}
-
-/* src/nemo/StdpProcess.cpp:116-124 */
-__device__ __forceinline__ int32_t weightChange(uint64_t pre, const StdpRule& R)
-{
-	return int32_t(uint32_t(updateRegion(pre & R.potentiation, R)) + uint32_t(updateRegion(pre & R.depression, R)));
-}
-
-/* Accumulate (src/nemo/ConnectivityMatrix.cpp:224-258): one warp per target
- * that fired P cycles ago walks its plastic in-synapses. Each accumulator has
- * a single writer, so plain read-modify-write is exact. */
-__global__ void __launch_bounds__(256)
-k_stdp(NetDev net, StdpRule rule, uint32_t offset)
-{
-	uint32_t t = cycleOf(net, offset);
-	uint32_t par = t & 1u;
-	if(blockIdx.x == 0 && threadIdx.x == 0) {
-		net.postCount[par ^ 1u] = 0; /* consumed by the next cycle's update */
-	}
-	uint32_t count = net.postCount[par];
-	const uint32_t* list = net.postList + size_t(par) * net.nDev;
-	uint32_t lane = threadIdx.x & 31u;
-	uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-	uint64_t visited = 0;
-	for(uint32_t w = warp; w < count; w += nwarps) {
-		uint32_t target = list[w];
-		uint64_t b = net.rcmStart[target], e = net.rcmStart[target + 1];
-		visited += e - b;
-		for(uint64_t j = b + lane; j < e; j += 32) {
-			uint32_t sd = net.rcmSrcDelay[j];
-			uint64_t pre = shr64(net.recentFiring[sd >> 6], (sd & 63u) + 1u);
-			int32_t dw = weightChange(pre, rule);
-			if(dw != 0) {
-				net.rcmAcc[j] = int32_t(uint32_t(net.rcmAcc[j]) + uint32_t(dw));
-			}
-		}
-	}
-	if(lane == 0 && visited) {
-		atomicAdd(&net.stats[1], (unsigned long long) visited);
-	}
-}
-
-/* src/nemo/StdpProcess.cpp:128-138 */
-__device__ __forceinline__ int32_t updatedWeight(int32_t wOld, int32_t wDiff, const StdpRule& R)
-{
-	int32_t sum = int32_t(uint32_t(wOld) + uint32_t(wDiff));
-	if(wOld > 0) return min(R.maxE, max(sum, R.minE));
-	if(wOld < 0) return min(R.minI, max(sum, R.maxI));
-	return 0;
-}
-
 /* applyStdp (src/nemo/ConnectivityMatrix.cpp:272-325): every plastic synapse
  * gets w = clamp(w + (reward * acc) >> f) and its accumulator cleared. */
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(BLOCK)
 k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t nrcm)
 {
 	uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -512,28 +558,11 @@ k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t nrcm)
 }
 
 __global__ void
-k_advance_cycle(uint32_t* counter, uint32_t by)
-{
-	*counter += by;
-}
-
-__global__ void
 k_nrand_probe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n, const uint32_t* sinTab, const uint32_t* logTab)
 {
 	size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
 	if(i < n) {
-		/* a state whose next two outputs are u1[i], u2[i]: with x=y=z=0 and
-		 * w chosen, xorshift returns w ^ (w >> 19) ^ 0 ... instead evaluate
-		 * the transform directly on the given words */
-		using namespace libm;
-		float f1 = __uint2float_rn(u1[i]);
-		float f2 = __uint2float_rn(u2[i]);
-		float a = sin_argument(f1);
-		float y = log_argument(f2);
-		float L = apply_code(log_candidate(y), table_code(logTab, libm_index(f2)));
-		float r = __fsqrt_rn(__fmul_rn(-2.0f, L));
-		float S = apply_code(sin_candidate(a), table_code(sinTab, libm_index(f1)));
-		out[i] = __fmul_rn(S, r);
+		out[i] = nrandWords(u1[i], u2[i], sinTab, logTab);
 	}
 }
 
@@ -552,14 +581,9 @@ k_libm_eval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t
 }
 
 int g_smCount = 0;
+int g_blocksPerSm = 0;
 
 } // namespace
-
-void
-launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream)
-{
-	k_libm_eval<<<smCount() * 8, 256, 0, static_cast<cudaStream_t>(stream)>>>(sinOut, logOut, sinTab, logTab);
-}
 
 int
 smCount()
@@ -583,32 +607,48 @@ launchStimulus(const NetDev& net, const StimDev& stim, void* stream)
 	k_stimulus<<<(n + 255) / 256, 256, 0, S(stream)>>>(net, stim);
 }
 
+/* Co-resident grid: as many blocks per SM as the kernel's registers allow
+ * (shared memory is small), times the SM count. */
 void
-launchGather(const NetDev& net, uint32_t offset, void* stream)
+cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap)
 {
-	k_gather<<<smCount() * 4, 256, 0, S(stream)>>>(net, offset);
-}
-
-void
-launchUpdate(int model, const NetDev& net, const GroupDev& g, uint32_t offset, bool resetSlot, void* stream)
-{
-	uint32_t blocks = (g.count + 255) / 256;
-	if(blocks == 0) blocks = 1;
-	int rs = resetSlot ? 1 : 0;
-	switch(model) {
-		case 0: k_update_izhikevich<<<blocks, 256, 0, S(stream)>>>(net, g, offset, rs); break;
-		case 1: k_update_if_curr_exp<<<blocks, 256, 0, S(stream)>>>(net, g, offset, rs); break;
-		case 2: k_update_qif<<<blocks, 256, 0, S(stream)>>>(net, g, offset, rs); break;
-		case 4: k_update_poisson<<<blocks, 256, 0, S(stream)>>>(net, g, offset, rs); break;
-		case 5: k_update_input<<<blocks, 256, 0, S(stream)>>>(net, g, offset, rs); break;
-		default: break;
+	const uint32_t warpsPerBlock = BLOCK / 32;
+	int sms = smCount();
+	/* the list capacity depends on the grid, and the shared memory on the
+	 * capacity; the fixed point is reached in two rounds for these sizes */
+	uint32_t cap = BLOCK;
+	for(int round = 0; round < 3; ++round) {
+		int perSm = 0;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles, BLOCK, size_t(2) * cap * 4);
+		if(perSm <= 0) perSm = 1;
+		g_blocksPerSm = perSm;
+		unsigned b = unsigned(sms * perSm);
+		uint32_t gridWarps = b * warpsPerBlock;
+		uint32_t perWarp = (totalWarps + gridWarps - 1) / gridWarps;
+		if(perWarp == 0) perWarp = 1;
+		uint32_t need = perWarp * warpsPerBlock * 32;
+		*blocks = b;
+		if(need <= cap) break;
+		cap = need;
 	}
+	*listCap = cap;
 }
 
-void
-launchStdp(const NetDev& net, const StdpRule& rule, uint32_t offset, void* stream)
+unsigned
+launchCycles(const CycleArgs& args, void* stream)
 {
-	k_stdp<<<smCount() * 4, 256, 0, S(stream)>>>(net, rule, offset);
+	unsigned blocks;
+	uint32_t cap;
+	cyclesGrid(args.groupWarp[args.ngroups], &blocks, &cap);
+	CycleArgs a = args;
+	a.listCap = cap;
+	size_t smem = size_t(2) * cap * 4;
+	if(smem > 48 * 1024) {
+		cudaFuncSetAttribute(k_cycles, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+	}
+	void* params[] = {&a};
+	cudaLaunchCooperativeKernel((const void*) k_cycles, dim3(blocks), dim3(BLOCK), params, smem, S(stream));
+	return blocks;
 }
 
 void
@@ -622,17 +662,17 @@ launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_
 }
 
 void
-launchAdvanceCycle(uint32_t* counter, uint32_t by, void* stream)
-{
-	k_advance_cycle<<<1, 1, 0, S(stream)>>>(counter, by);
-}
-
-void
 launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream)
 {
 	if(n == 0) return;
 	k_nrand_probe<<<uint32_t((n + 255) / 256), 256, 0, S(stream)>>>(u1, u2, out, n, sinTab, logTab);
+}
+
+void
+launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream)
+{
+	k_libm_eval<<<smCount() * 8, 256, 0, S(stream)>>>(sinOut, logOut, sinTab, logTab);
 }
 
 } // namespace nemo_b200

@@ -10,13 +10,22 @@
  * warp owns whole 32-bit words of every per-neuron bitmap. Padding slots
  * never fire and have no synapses.
  *
- * Per-cycle data flow (cycle t):
- *   gather  : drain spike-queue slot t into the int64 E/I accumulators
- *   update  : per type; currents -> state, firing bitmap for t, and the
- *             scatter epilogue that enqueues each fired neuron's rows into
- *             slots t+d, plus the STDP post-spike list
- *   stdp    : accumulate weight changes for targets that fired at t-P
- */
+ * The step path is one persistent cooperative kernel (k_cycles) that runs a
+ * block of cycles with one grid barrier per cycle. Phase t:
+ *   - neuron update of cycle t: read and clear the cycle's current slot
+ *     acc[t mod Q], integrate, fire, shift the firing history
+ *     (rf[t&1] -> rf[(t+1)&1]), record the firing bitmap and the STDP
+ *     post-spike list of cycle t;
+ *   - spike push: every neuron fired at t streams its outgoing synapses (one
+ *     contiguous range per source, sorted by delay) and adds each weight into
+ *     acc[(t+d) mod Q][target] (E or I by sign) with fire-and-forget 64-bit
+ *     reductions in L2 — the reference's deliverSpikes at cycle t+d
+ *     (src/nemo/cpu/Simulation.cpp:259-308) moved to fire time;
+ *   - STDP accumulation of cycle t-1 (targets that fired P cycles before it),
+ *     which only reads rf[t&1] and so overlaps the update of cycle t;
+ *   - grid barrier.
+ * A final half phase accumulates STDP for the last cycle. Integer sums are
+ * exact in any order, so the result is bit-identical to the CPU reference. */
 
 #include <cstdint>
 
@@ -24,30 +33,27 @@
 
 namespace nemo_b200 {
 
+const int MAX_GROUPS = 8;
+
 struct NetDev {
 	uint32_t nDev;          /* device neurons, multiple of 32 */
 	uint32_t nWords;        /* nDev / 32 */
 	uint32_t rowStride;     /* rows per source: max(maxDelay, 1) */
-	uint32_t qMask;         /* spike-queue slots - 1 (power of two > maxDelay) */
-	uint64_t qCap;          /* rows per slot: number of non-empty rows */
+	uint32_t qMask;         /* current slots - 1 (power of two > maxDelay) */
 	uint32_t ringMask;      /* firing-ring cycles - 1 */
 	uint32_t fbits;         /* fractional bits of the Q(31-f).f weights */
+	int deliver;            /* 0 when no delay is deliverable (max delay 64) */
 
-	const uint32_t* cycleBase;     /* device cycle counter (advanced by graph runs) */
-
-	/* forward connectivity: row r = source * rowStride + delay - 1 */
+	/* forward connectivity: row r = source * rowStride + delay - 1; the rows
+	 * of one source are contiguous, so [rowStart[s*rowStride],
+	 * rowStart[(s+1)*rowStride]) is all of its synapses in delay order */
 	const uint64_t* rowStart;      /* [nDev * rowStride + 1] */
-	uint2* fcm;                    /* {target device index, int32 weight} */
-	const uint64_t* delayBits;     /* [nDev] deliverable delays, bit d-1 */
+	uint2* fcm;                    /* {target << 6 | (delay - 1), int32 weight} */
 	const uint32_t* outDegree;     /* [nDev] synapses per source */
 
-	/* spike queue: slot s holds row ids to deliver at cycles = s (mod slots) */
-	uint32_t* queue;               /* [slots * qCap] */
-	uint32_t* queueFill;           /* [slots] */
-
-	long long* acc;                /* [2 * nDev] int64 E at 2n, I at 2n+1 */
-	uint64_t* recentFiring;        /* [nDev] firing history, bit 0 = last cycle */
-	uint32_t* firedRing;           /* [ring * nWords] firing bitmaps by cycle */
+	long long* acc;                /* [slots][nDev][2] int64 E, I current of a future cycle */
+	uint64_t* rf;                  /* [2][nDev] firing history, bit 0 = last cycle */
+	uint32_t* firedRing;           /* [ring][nWords] firing bitmaps by cycle */
 	unsigned long long* eventsRing;/* [ring] synaptic events (fired x out-degree) */
 	uint32_t* firedCountRing;      /* [ring] */
 	float* ext;                    /* [nDev] external current, cleared after use */
@@ -56,8 +62,9 @@ struct NetDev {
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
-	uint32_t* postList;            /* [2 * nDev] */
-	uint32_t* postCount;           /* [2] */
+	uint32_t stdpChunks;           /* 128-synapse chunks per target (max in-degree) */
+	uint32_t* postList;            /* [3][nDev] */
+	uint32_t* postCount;           /* [3] */
 	const uint64_t* rcmStart;      /* [nDev + 1] */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
 	const uint32_t* rcmForward;    /* index into fcm */
@@ -67,16 +74,19 @@ struct NetDev {
 	const uint32_t* sinTab;
 	const uint32_t* logTab;
 
-	/* cumulative counters: [0] synapses delivered by gather, [1] synapses
-	 * visited by STDP accumulation, [2] neurons fired, [3] synaptic events
-	 * generated (fired x out-degree) */
+	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
+	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */
 	unsigned long long* stats;
+
+	/* grid barrier: [0] arrivals, [1] generation, [2] error (timeout) */
+	unsigned* barrier;
 };
 
 struct GroupDev {
 	uint32_t devBase;       /* first device index (multiple of 32) */
 	uint32_t count;
 	uint32_t timerBase;     /* cycle at the last timer reset (HH counts from it) */
+	int kind;               /* ModelKind */
 	float* param;           /* [nParam][count] */
 	float* state;           /* [nState][count] */
 	uint4* rng;             /* [count] xorshift128 state */
@@ -94,6 +104,18 @@ struct StdpRule {
 	int32_t fnPost[64];
 };
 
+struct CycleArgs {
+	NetDev net;
+	StdpRule rule;
+	GroupDev groups[MAX_GROUPS];
+	uint32_t groupWarp[MAX_GROUPS + 1];  /* prefix of 32-neuron warps per group */
+	int ngroups;
+	uint32_t firstCycle;
+	uint32_t cycles;
+	uint32_t listCap;                    /* per-block shared list capacity */
+	unsigned long long timeoutNs;        /* grid-barrier wait limit */
+};
+
 struct StimDev {
 	const uint32_t* fstim;  /* device indices */
 	uint32_t nf;
@@ -102,14 +124,13 @@ struct StimDev {
 	uint32_t ni;
 };
 
-/* Launchers (kernels.cu). All launch on `stream`; `offset` is added to the
- * device cycle counter to obtain the cycle. */
+/* Launchers (kernels.cu), all on `stream`. */
 void launchStimulus(const NetDev& net, const StimDev& stim, void* stream);
-void launchGather(const NetDev& net, uint32_t offset, void* stream);
-void launchUpdate(int model, const NetDev& net, const GroupDev& g, uint32_t offset, bool resetSlot, void* stream);
-void launchStdp(const NetDev& net, const StdpRule& rule, uint32_t offset, void* stream);
+/* Cooperative launch of k_cycles; returns the grid size used. */
+unsigned launchCycles(const CycleArgs& args, void* stream);
+/* Largest co-resident grid and the shared-memory list capacity it needs. */
+void cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap);
 void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, void* stream);
-void launchAdvanceCycle(uint32_t* counter, uint32_t by, void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);

@@ -77,22 +77,19 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_writeOnly(conf.writeOnlySynapses),
 	m_fcmHostValid(false),
 	m_cycle(0),
-	m_counter(0),
 	m_timerBase(0),
 	m_stateDirty(false),
 	m_stream(nullptr),
-	m_dCounter(nullptr),
 	m_hWords(nullptr),
 	m_hStim(nullptr),
 	m_hCur(nullptr),
 	m_dStim(nullptr),
 	m_dCur(nullptr),
-	m_stimCap(0),
-	m_graphExec(nullptr),
-	m_graphCycles(0)
+	m_stimCap(0)
 {
 	std::memset(&m_net, 0, sizeof(m_net));
 	std::memset(&m_rule, 0, sizeof(m_rule));
+	std::memset(&m_args, 0, sizeof(m_args));
 
 	if(m_nNeurons == 0) {
 		fail(NEMO_INVALID_INPUT, "Cannot create simulation from empty network");
@@ -221,38 +218,36 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	for(size_t r = 0; r < nrows; ++r) rowStart[r + 1] += rowStart[r];
 	std::vector<uint2> fcm(S);
 	std::vector<uint32_t> fcmPos(S);
-	std::vector<uint64_t> delayBits(m_nDev, 0);
 	std::vector<uint32_t> outDegree(m_nDev, 0);
 	{
 		std::vector<uint64_t> fill(rowStart.begin(), rowStart.end() - 1);
 		for(size_t s = 0; s < S; ++s) {
 			size_t r = size_t(dsrc[s]) * Ds + net.dly[s] - 1;
 			uint64_t pos = fill[r]++;
-			fcm[pos] = make_uint2(dtgt[s], uint32_t(toFix(net.wgt[s], m_fbits)));
+			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(toFix(net.wgt[s], m_fbits)));
 			fcmPos[s] = uint32_t(pos);
-			delayBits[dsrc[s]] |= uint64_t(1) << (net.dly[s] - 1);
 			outDegree[dsrc[s]]++;
 		}
 	}
 	/* deliverable delays: the reference masks the history with
 	 * ~(~0 << maxDelay), a shift evaluated modulo 64 on x86-64
-	 * (src/nemo/cpu/Simulation.cpp:264) */
-	uint64_t validSpikes = ~shl64(~uint64_t(0), m_maxDelay);
-	uint64_t qCap = 0;
-	for(uint32_t n = 0; n < m_nDev; ++n) {
-		delayBits[n] &= validSpikes;
-		qCap += __builtin_popcountll(delayBits[n]);
-	}
+	 * (src/nemo/cpu/Simulation.cpp:264): every delay up to 63 ms is
+	 * delivered, and with a 64 ms synapse present none is */
+	const bool deliver = S > 0 && m_maxDelay < 64;
 	uint32_t slots = 2;
-	while(slots <= m_maxDelay) slots *= 2;
+	while(deliver && slots <= m_maxDelay) slots *= 2;
 
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
 	std::vector<uint64_t> rcmStart;
 	std::vector<uint32_t> rcmSrcDelay, rcmForward;
+	uint64_t maxIn = 0;
 	if(m_stdpOn) {
 		rcmStart.assign(size_t(m_nDev) + 1, 0);
 		for(size_t s = 0; s < S; ++s) if(net.plastic[s]) rcmStart[dtgt[s] + 1]++;
-		for(uint32_t n = 0; n < m_nDev; ++n) rcmStart[n + 1] += rcmStart[n];
+		for(uint32_t n = 0; n < m_nDev; ++n) {
+			maxIn = std::max<uint64_t>(maxIn, rcmStart[n + 1]);
+			rcmStart[n + 1] += rcmStart[n];
+		}
 		m_nrcm = rcmStart[m_nDev];
 		rcmSrcDelay.resize(m_nrcm);
 		rcmForward.resize(m_nrcm);
@@ -263,6 +258,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 			rcmSrcDelay[j] = (dsrc[s] << 6) | (net.dly[s] - 1);
 			rcmForward[j] = fcmPos[s];
 		}
+	}
+	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + 127) / 128);
+	if(uint64_t(m_nDev) * stdpChunks >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 plastic synapses per target neuron");
 	}
 
 	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
@@ -294,30 +293,27 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.nWords = m_nDev / 32;
 	m_net.rowStride = Ds;
 	m_net.qMask = slots - 1;
-	m_net.qCap = std::max<uint64_t>(qCap, 1);
 	m_net.ringMask = m_ring - 1;
 	m_net.fbits = m_fbits;
-	m_dCounter = (uint32_t*) alloc(sizeof(uint32_t));
-	m_net.cycleBase = m_dCounter;
+	m_net.deliver = deliver ? 1 : 0;
 	m_net.rowStart = (const uint64_t*) put(rowStart.data(), rowStart.size() * 8);
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
-	m_net.delayBits = (const uint64_t*) put(delayBits.data(), delayBits.size() * 8);
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
-	m_net.queue = (uint32_t*) alloc(size_t(slots) * m_net.qCap * 4);
-	m_net.queueFill = (uint32_t*) alloc(size_t(slots) * 4);
-	m_net.acc = (long long*) alloc(size_t(m_nDev) * 16);
-	m_net.recentFiring = (uint64_t*) alloc(size_t(m_nDev) * 8);
+	m_net.acc = (long long*) alloc(size_t(slots) * m_nDev * 16);
+	m_net.rf = (uint64_t*) alloc(size_t(2) * m_nDev * 8);
 	m_net.firedRing = (uint32_t*) alloc(size_t(m_ring) * m_net.nWords * 4);
 	m_net.eventsRing = (unsigned long long*) alloc(size_t(m_ring) * 8);
 	m_net.firedCountRing = (uint32_t*) alloc(size_t(m_ring) * 4);
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
 	m_net.stats = (unsigned long long*) alloc(4 * 8);
+	m_net.barrier = (unsigned*) alloc(4 * 4);
 	m_net.stdp = m_stdpOn ? 1 : 0;
+	m_net.stdpChunks = uint32_t(stdpChunks);
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
-		m_net.postList = (uint32_t*) alloc(size_t(m_nDev) * 2 * 4);
-		m_net.postCount = (uint32_t*) alloc(2 * 4);
+		m_net.postList = (uint32_t*) alloc(size_t(m_nDev) * 3 * 4);
+		m_net.postCount = (uint32_t*) alloc(3 * 4);
 		m_net.rcmStart = (const uint64_t*) put(rcmStart.data(), rcmStart.size() * 8);
 		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
 		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
@@ -346,7 +342,24 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		m_net.logTab = (const uint32_t*) put(t.logCodes.data(), t.logCodes.size() * 4);
 	}
 
-	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords) * 4));
+	/* the persistent kernel's arguments, except the cycle range */
+	if(m_groups.size() > size_t(MAX_GROUPS)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most " + std::to_string(MAX_GROUPS)
+				+ " neuron types per simulation");
+	}
+	m_args.net = m_net;
+	m_args.rule = m_rule;
+	m_args.ngroups = int(m_groups.size());
+	m_args.groupWarp[0] = 0;
+	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
+		const Group& g = m_groups[gi];
+		m_args.groups[gi] = GroupDev{g.devBase, g.count, 0u, int(g.type.kind), g.dParam, g.dState, g.dRng};
+		m_args.groupWarp[gi + 1] = m_args.groupWarp[gi] + (g.count + 31) / 32;
+	}
+	/* a grid barrier that waits this long has lost a block: give up */
+	m_args.timeoutNs = 10ull * 1000 * 1000 * 1000;
+
+	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords + 1) * 4));
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	m_wallStart = std::chrono::steady_clock::now();
 }
@@ -354,7 +367,6 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 Simulation::~Simulation()
 {
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
-	if(m_graphExec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_hWords) cudaFreeHost(m_hWords);
 	if(m_hStim) cudaFreeHost(m_hStim);
@@ -390,24 +402,27 @@ Simulation::groupOfDev(uint32_t dev, uint32_t* i) const
 	return g;
 }
 
+/* One persistent launch for cycles [first, first + cycles) */
 void
-Simulation::launchCycle(uint32_t offset)
+Simulation::launchBlock(uint64_t first, unsigned cycles)
 {
-	launchGather(m_net, offset, m_stream);
-	bool first = true;
-	for(const Group& g : m_groups) {
-		GroupDev gd;
-		gd.devBase = g.devBase;
-		gd.count = g.count;
-		gd.timerBase = uint32_t(m_timerBase);
-		gd.param = g.dParam;
-		gd.state = g.dState;
-		gd.rng = g.dRng;
-		launchUpdate(int(g.type.kind), m_net, gd, offset, first, m_stream);
-		first = false;
+	CycleArgs a = m_args;
+	a.firstCycle = uint32_t(first);
+	a.cycles = cycles;
+	for(int gi = 0; gi < a.ngroups; ++gi) {
+		a.groups[gi].timerBase = uint32_t(m_timerBase);
 	}
-	if(m_stdpOn) {
-		launchStdp(m_net, m_rule, offset, m_stream);
+	launchCycles(a, m_stream);
+	NEMO_CUDA(cudaGetLastError());
+}
+
+/* The grid barrier gives up after its time limit and leaves an error word
+ * instead of hanging the GPU; report it. */
+void
+Simulation::checkDeviceError()
+{
+	if(m_hWords[m_net.nWords] != 0) {
+		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
 	}
 }
 
@@ -481,38 +496,18 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
 	}
 
-	launchCycle(uint32_t(m_cycle - m_counter));
+	launchBlock(m_cycle, 1);
 	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
 				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	NEMO_CUDA(cudaGetLastError());
+	checkDeviceError();
 	m_cycle++;
 	m_stateDirty = true;
 	decodeFired(m_hWords, m_fired);
 	return m_fired;
-}
-
-void
-Simulation::buildGraph(unsigned cycles)
-{
-	cudaStream_t stream = STREAM(m_stream);
-	if(m_graphExec) {
-		cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
-		m_graphExec = nullptr;
-	}
-	cudaGraph_t graph;
-	NEMO_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-	for(unsigned k = 0; k < cycles; ++k) {
-		launchCycle(k);
-	}
-	launchAdvanceCycle(m_dCounter, cycles, m_stream);
-	NEMO_CUDA(cudaStreamEndCapture(stream, &graph));
-	cudaGraphExec_t exec;
-	NEMO_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-	cudaGraphDestroy(graph);
-	m_graphExec = exec;
-	m_graphCycles = cycles;
 }
 
 void
@@ -523,31 +518,23 @@ Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
 	}
 	cudaStream_t stream = STREAM(m_stream);
-	if(m_counter != m_cycle) {
-		uint32_t c = uint32_t(m_cycle);
-		NEMO_CUDA(cudaMemcpyAsync(m_dCounter, &c, 4, cudaMemcpyHostToDevice, stream));
-		NEMO_CUDA(cudaStreamSynchronize(stream));
-		m_counter = m_cycle;
-	}
-	if(!m_graphExec || m_graphCycles != cycles) {
-		buildGraph(cycles);
-	}
-	NEMO_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(m_graphExec), stream));
+	launchBlock(m_cycle, cycles);
 	uint64_t first = m_cycle;
 	m_cycle += cycles;
-	m_counter += cycles;
 	m_stateDirty = true;
+	std::vector<uint32_t> fc(m_ring);
+	std::vector<uint64_t> ev(m_ring);
 	if(firedCounts || events) {
-		std::vector<uint32_t> fc(m_ring);
-		std::vector<uint64_t> ev(m_ring);
 		NEMO_CUDA(cudaMemcpyAsync(fc.data(), m_net.firedCountRing, m_ring * 4, cudaMemcpyDeviceToHost, stream));
 		NEMO_CUDA(cudaMemcpyAsync(ev.data(), m_net.eventsRing, m_ring * 8, cudaMemcpyDeviceToHost, stream));
-		NEMO_CUDA(cudaStreamSynchronize(stream));
-		for(unsigned k = 0; k < cycles; ++k) {
-			uint32_t slot = uint32_t(first + k) & m_net.ringMask;
-			if(firedCounts) firedCounts[k] = fc[slot];
-			if(events) events[k] = ev[slot];
-		}
+	}
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	checkDeviceError();
+	for(unsigned k = 0; k < cycles && (firedCounts || events); ++k) {
+		uint32_t slot = uint32_t(first + k) & m_net.ringMask;
+		if(firedCounts) firedCounts[k] = fc[slot];
+		if(events) events[k] = ev[slot];
 	}
 }
 
@@ -764,11 +751,6 @@ Simulation::resetTimer()
 {
 	m_wallStart = std::chrono::steady_clock::now();
 	m_timerBase = m_cycle;
-	if(m_graphExec) {
-		cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
-		m_graphExec = nullptr;
-		m_graphCycles = 0;
-	}
 }
 
 void
@@ -815,14 +797,6 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 	}
 	int32_t fx = apply ? toFix(reward, m_fbits) : 0;
 	cudaStream_t stream = STREAM(m_stream);
-	if(m_counter != m_cycle) {
-		uint32_t c = uint32_t(m_cycle);
-		NEMO_CUDA(cudaMemcpyAsync(m_dCounter, &c, 4, cudaMemcpyHostToDevice, stream));
-		m_counter = m_cycle;
-	}
-	if(!m_graphExec || m_graphCycles != cyclesPerStep) {
-		buildGraph(cyclesPerStep);
-	}
 	uint64_t before[4], after[4];
 	readStats(before);
 	cudaEvent_t e0, e1;
@@ -830,7 +804,8 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 	NEMO_CUDA(cudaEventCreate(&e1));
 	NEMO_CUDA(cudaEventRecord(e0, stream));
 	for(unsigned s = 0; s < steps; ++s) {
-		NEMO_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(m_graphExec), stream));
+		launchBlock(m_cycle, cyclesPerStep);
+		m_cycle += cyclesPerStep;
 		if(apply && m_nrcm) {
 			launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
 		}
@@ -842,11 +817,11 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	NEMO_CUDA(cudaGetLastError());
-	m_cycle += uint64_t(steps) * cyclesPerStep;
-	m_counter = m_cycle;
 	m_stateDirty = true;
 	m_fcmHostValid = false;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
 	readStats(after);
+	checkDeviceError();
 	out[0] = ms;
 	out[1] = double(after[2] - before[2]);
 	out[2] = double(after[3] - before[3]);
@@ -857,65 +832,43 @@ void
 Simulation::profile(unsigned cycles, float reward, double out[10])
 {
 	cudaStream_t stream = STREAM(m_stream);
-	/* all cycles are enqueued before the first wait, so the queue runs ahead
-	 * of the GPU and the events bracket device execution only */
-	std::vector<cudaEvent_t> ev(size_t(cycles) * 4 + 4);
-	for(auto& e : ev) NEMO_CUDA(cudaEventCreate(&e));
+	cudaEvent_t e0, e1, e2;
+	NEMO_CUDA(cudaEventCreate(&e0));
+	NEMO_CUDA(cudaEventCreate(&e1));
+	NEMO_CUDA(cudaEventCreate(&e2));
 	uint64_t before[4], after[4];
 	readStats(before);
-	for(unsigned c = 0; c < cycles; ++c) {
-		uint32_t offset = uint32_t(m_cycle - m_counter);
-		NEMO_CUDA(cudaEventRecord(ev[4 * c + 0], stream));
-		launchGather(m_net, offset, m_stream);
-		NEMO_CUDA(cudaEventRecord(ev[4 * c + 1], stream));
-		bool first = true;
-		for(const Group& g : m_groups) {
-			GroupDev gd{g.devBase, g.count, uint32_t(m_timerBase), g.dParam, g.dState, g.dRng};
-			launchUpdate(int(g.type.kind), m_net, gd, offset, first, m_stream);
-			first = false;
-		}
-		NEMO_CUDA(cudaEventRecord(ev[4 * c + 2], stream));
-		if(m_stdpOn) {
-			launchStdp(m_net, m_rule, offset, m_stream);
-		}
-		NEMO_CUDA(cudaEventRecord(ev[4 * c + 3], stream));
-		m_cycle++;
-	}
-	NEMO_CUDA(cudaStreamSynchronize(stream));
-	double tg = 0, tu = 0, ts = 0;
-	for(unsigned c = 0; c < cycles; ++c) {
-		float a, b, d;
-		NEMO_CUDA(cudaEventElapsedTime(&a, ev[4 * c + 0], ev[4 * c + 1]));
-		NEMO_CUDA(cudaEventElapsedTime(&b, ev[4 * c + 1], ev[4 * c + 2]));
-		NEMO_CUDA(cudaEventElapsedTime(&d, ev[4 * c + 2], ev[4 * c + 3]));
-		tg += a;
-		tu += b;
-		ts += d;
-	}
-	readStats(after);
-	double tapply = 0;
+	NEMO_CUDA(cudaEventRecord(e0, stream));
+	launchBlock(m_cycle, cycles);
+	m_cycle += cycles;
+	NEMO_CUDA(cudaEventRecord(e1, stream));
 	if(m_stdpOn && m_nrcm) {
-		int32_t fx = toFix(reward, m_fbits);
-		NEMO_CUDA(cudaEventRecord(ev[0], stream));
-		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
-		NEMO_CUDA(cudaEventRecord(ev[1], stream));
-		NEMO_CUDA(cudaEventSynchronize(ev[1]));
-		float a;
-		NEMO_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
-		tapply = a;
+		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_nrcm, m_stream);
 		m_fcmHostValid = false;
 	}
-	for(auto& e : ev) cudaEventDestroy(e);
-	NEMO_CUDA(cudaGetLastError());
+	NEMO_CUDA(cudaEventRecord(e2, stream));
+	NEMO_CUDA(cudaEventSynchronize(e2));
+	float tc = 0, ta = 0;
+	NEMO_CUDA(cudaEventElapsedTime(&tc, e0, e1));
+	NEMO_CUDA(cudaEventElapsedTime(&ta, e1, e2));
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaEventDestroy(e2);
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	readStats(after);
+	checkDeviceError();
 	m_stateDirty = true;
-	out[0] = tg;
-	out[1] = tu;
-	out[2] = ts;
+	unsigned blocks;
+	uint32_t cap;
+	cyclesGrid(m_args.groupWarp[m_args.ngroups], &blocks, &cap);
+	out[0] = tc;
+	out[1] = blocks;
+	out[2] = 0;
 	out[3] = double(after[0] - before[0]);
 	out[4] = double(after[2] - before[2]);
 	out[5] = double(after[1] - before[1]);
 	out[6] = double(m_nNeurons) * cycles;
-	out[7] = tapply;
+	out[7] = (m_stdpOn && m_nrcm) ? ta : 0.0;
 	out[8] = double(m_nrcm);
 	out[9] = double(after[3] - before[3]);
 }

@@ -4,7 +4,7 @@
 /* The B200 simulation backend: the role of the reference's
  * nemo::SimulationBackend implementations (src/nemo/SimulationBackend.hpp:
  * 45-147, cpu/Simulation.cpp, cuda/Simulation.cpp), with the per-cycle work
- * done by the kernels of kernels.cu. */
+ * done by the persistent kernel of kernels.cu. */
 
 #include <chrono>
 #include <cstdint>
@@ -26,8 +26,8 @@ public:
 	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
 			const unsigned* inidx, const float* icur, size_t ni);
 
-	/* Device-resident run of `cycles` cycles without stimulus, captured as a
-	 * CUDA graph; per-cycle fired counts and synaptic events (fired x
+	/* Device-resident run of `cycles` cycles without stimulus in one
+	 * persistent launch; per-cycle fired counts and synaptic events (fired x
 	 * out-degree) are returned when the pointers are non-null. */
 	void run(unsigned cycles, uint32_t* firedCounts, uint64_t* events);
 
@@ -65,17 +65,16 @@ public:
 	 * the results that differ from host glibc (tests; expected 0). */
 	uint64_t libmCheck();
 
-	/* Device-timed throughput loop: `steps` x (graph of `cyclesPerStep`
-	 * cycles, then applyStdp(reward) if applyEvery), bracketed by CUDA events
-	 * on the simulation's stream. out: [0] device ms, [1] neurons fired,
-	 * [2] synaptic events generated, [3] synapses delivered. */
+	/* Device-timed throughput loop: `steps` x (one persistent launch of
+	 * `cyclesPerStep` cycles, then applyStdp(reward) if apply), bracketed by
+	 * CUDA events on the simulation's stream. out: [0] device ms, [1] neurons
+	 * fired, [2] synaptic events generated, [3] synapses pushed. */
 	void timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4]);
 
-	/* Per-stage device times over `cycles` individually launched cycles
-	 * (CUDA events between stages). out: [0] gather ms, [1] update ms,
-	 * [2] stdp ms, [3] synapses delivered, [4] neurons fired,
-	 * [5] STDP synapse visits, [6] neuron updates, [7] applyStdp ms (one
-	 * call after the cycles, when STDP is on), [8] plastic synapses,
+	/* Device times of one persistent launch of `cycles` cycles and of one
+	 * applyStdp, with the work they did. out: [0] step-kernel ms, [1] grid
+	 * blocks, [2] 0, [3] synapses pushed, [4] neurons fired, [5] STDP synapse
+	 * visits, [6] neuron updates, [7] applyStdp ms, [8] plastic synapses,
 	 * [9] synaptic events generated. */
 	void profile(unsigned cycles, float reward, double out[10]);
 
@@ -105,9 +104,9 @@ private:
 	Group& groupOfDev(uint32_t dev, uint32_t* i);
 	const Group& groupOfDev(uint32_t dev, uint32_t* i) const;
 	const Aux& aux(synapse_id id) const;
-	void launchCycle(uint32_t offset);
+	void launchBlock(uint64_t first, unsigned cycles);
+	void checkDeviceError();
 	void syncStateToHost();
-	void buildGraph(unsigned cycles);
 	void* alloc(size_t bytes);
 	void decodeFired(const uint32_t* words, std::vector<unsigned>& out) const;
 
@@ -123,6 +122,7 @@ private:
 	std::vector<int32_t> m_d2group;                /* device index -> group (-1: padding) */
 
 	NetDev m_net;
+	CycleArgs m_args;
 	bool m_stdpOn;
 	StdpRule m_rule;
 	StdpFunction m_stdpFn;
@@ -138,17 +138,15 @@ private:
 
 	/* state */
 	uint64_t m_cycle;          /* cycles simulated */
-	uint64_t m_counter;        /* value of the device cycle counter */
 	uint64_t m_timerBase;
 	bool m_stateDirty;
 	std::chrono::steady_clock::time_point m_wallStart;
 
 	void* m_stream;
 	std::vector<void*> m_allocs;
-	uint32_t* m_dCounter;
 
 	/* pinned staging */
-	uint32_t* m_hWords;        /* one firing bitmap */
+	uint32_t* m_hWords;        /* one firing bitmap, then the barrier error word */
 	uint32_t* m_hStim;         /* fstim + istim indices */
 	float* m_hCur;
 	uint32_t* m_dStim;
@@ -156,10 +154,6 @@ private:
 	size_t m_stimCap;
 
 	std::vector<unsigned> m_fired;
-	std::vector<uint32_t> m_stimScratch;
-
-	void* m_graphExec;
-	unsigned m_graphCycles;
 };
 
 } // namespace nemo_b200
