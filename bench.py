@@ -303,6 +303,11 @@ def run_b200(args):
 
     roof = roofline(sim, lib, wl)
     clk = clocks.summary()
+    tr = (ctypes.c_double * 8)()
+    lib.dll.nemo_b200_trace.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double * 8]
+    lib.call("nemo_b200_trace", sim.handle, CYCLES_PER_STEP, tr)
+    phase_ns = dict(zip(["phase", "update_max", "update_mean", "push_stdp_max", "push_stdp_mean",
+                         "to_last_arrival", "barrier_release", "arrival_spread"], [round(x, 1) for x in tr]))
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -321,6 +326,7 @@ def run_b200(args):
                 "d2h_bytes_per_step": 4 * nwords * CYCLES_PER_STEP,
                 "steps": e2e_steps_n, "s_per_step": round(e2e_s / e2e_steps_n, 4)},
         "roofline": roof,
+        "phase_ns": phase_ns,
         "gpu_launches": args.steps * 2,
         "clocks": clk,
     }

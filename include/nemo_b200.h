@@ -52,6 +52,14 @@ nemo_status_t nemo_b200_timed_steps(nemo_simulation_t sim, unsigned steps, unsig
  * synaptic events generated. */
 nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[10]);
 
+/* Phase timing of the step kernel over `cycles` cycles (one traced launch;
+ * the cycles are simulated). Means over cycles, in ns: out[0] whole phase,
+ * out[1] / out[2] slowest / mean block neuron update, out[3] / out[4]
+ * slowest / mean block spike push + STDP, out[5] phase start to the last
+ * block's arrival at the grid barrier, out[6] last arrival to barrier exit,
+ * out[7] spread of the blocks' arrivals. */
+nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[8]);
+
 /* Diagnostics: the device noise transform of two RNG words per sample,
  * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the
  * Izhikevich kernel (glibc-matching), for n samples. */

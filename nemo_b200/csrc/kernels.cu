@@ -20,7 +20,7 @@ namespace nemo_b200 {
 namespace {
 
 const unsigned FULL = 0xffffffffu;
-const unsigned BLOCK = 256;
+const unsigned BLOCK = 1024;
 
 /* 64-bit shifts by a count that may reach 64, evaluated like the x86-64
  * shift the reference runs on (count modulo 64). */
@@ -76,16 +76,39 @@ __device__ __forceinline__ float nrand(uint4& s, const uint32_t* sinTab, const u
 	return nrandWords(u1, u2, sinTab, logTab);
 }
 
-/* Read and clear neuron n's E/I sums for the current cycle's slot */
+/* Read and clear neuron n's E/I sums for the current cycle's slot. With
+ * int32 accumulators the host has proven that no sum can leave the int32
+ * range, so the value equals the int64 sum and needs no saturation. */
 __device__ __forceinline__ void takeCurrents(const NetDev& net, uint32_t slot, uint32_t n, float& E, float& I)
 {
-	longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
-	longlong2 a = acc[n];
-	if(a.x | a.y) {
-		acc[n] = make_longlong2(0, 0);
+	if(net.acc32) {
+		int2* acc = reinterpret_cast<int2*>(net.acc) + size_t(slot) * net.nDev;
+		int2 a = acc[n];
+		if(a.x | a.y) {
+			acc[n] = make_int2(0, 0);
+		}
+		E = wfxToFloat(a.x, net.fbits);
+		I = wfxToFloat(a.y, net.fbits);
+	} else {
+		longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
+		longlong2 a = acc[n];
+		if(a.x | a.y) {
+			acc[n] = make_longlong2(0, 0);
+		}
+		E = wfxToFloat(a.x, net.fbits);
+		I = wfxToFloat(a.y, net.fbits);
 	}
-	E = wfxToFloat(a.x, net.fbits);
-	I = wfxToFloat(a.y, net.fbits);
+}
+
+/* Add a weight into the E (w >= 0) or I half of a current slot */
+__device__ __forceinline__ void addCurrent(const NetDev& net, uint32_t slot, uint32_t target, int half, long long w)
+{
+	size_t idx = (size_t(slot) * net.nDev + target) * 2 + half;
+	if(net.acc32) {
+		atomicAdd(reinterpret_cast<unsigned*>(net.acc) + idx, (unsigned) (int) w);
+	} else {
+		atomicAdd(reinterpret_cast<unsigned long long*>(net.acc) + idx, (unsigned long long) w);
+	}
 }
 
 __device__ __forceinline__ float takeExternal(const NetDev& net, uint32_t n)
@@ -123,8 +146,8 @@ __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDe
 	takeCurrents(net, slot, n, E, I);
 	float In = __fadd_rn(__fadd_rn(E, I), takeExternal(net, n));
 	float sigma = g.param[4 * c + i];
+	uint4 s = g.rng[i]; /* loaded with the other operands; used only with noise */
 	if(sigma != 0.0f) {
-		uint4 s = g.rng[i];
 		In = __fadd_rn(In, __fmul_rn(sigma, nrand(s, net.sinTab, net.logTab)));
 		g.rng[i] = s;
 	}
@@ -294,8 +317,10 @@ __device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeo
 		cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(bar[1]);
 		cuda::atomic_ref<unsigned, cuda::thread_scope_device> err(bar[2]);
 		int good = 1;
-		unsigned g = gen.load(cuda::memory_order_acquire);
-		__threadfence();
+		unsigned g = gen.load(cuda::memory_order_relaxed);
+		/* publish the block's writes (ordered before this thread by the
+		 * __syncthreads above) to the whole device */
+		cuda::atomic_thread_fence(cuda::memory_order_acq_rel, cuda::thread_scope_device);
 		unsigned arrived = count.fetch_add(1u, cuda::memory_order_acq_rel);
 		if(arrived == gridDim.x - 1) {
 			count.store(0u, cuda::memory_order_relaxed);
@@ -304,19 +329,19 @@ __device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeo
 			unsigned long long start = globalTimer();
 			unsigned spins = 0;
 			while(gen.load(cuda::memory_order_acquire) == g) {
-				if(err.load(cuda::memory_order_relaxed)) {
-					good = 0;
-					break;
+				if((++spins & 1023u) == 0) {
+					if(err.load(cuda::memory_order_relaxed)) {
+						good = 0;
+						break;
+					}
+					if(globalTimer() - start > timeoutNs) {
+						err.store(1u, cuda::memory_order_relaxed);
+						good = 0;
+						break;
+					}
 				}
-				if((++spins & 255u) == 0 && globalTimer() - start > timeoutNs) {
-					err.store(1u, cuda::memory_order_relaxed);
-					good = 0;
-					break;
-				}
-				__nanosleep(32);
 			}
 		}
-		__threadfence();
 		ok = good;
 	}
 	__syncthreads();
@@ -325,47 +350,68 @@ __device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeo
 
 /* ---------------- the persistent step kernel ---------------- */
 
-__global__ void __launch_bounds__(BLOCK)
+/* Work lists of a block, in global memory (per-block regions of listCap
+ * entries of {neuron, first synapse, synapse count}):
+ *   fired[listCap]   sources fired by this block's neurons in this cycle,
+ *   post[2][listCap] this block's post-spiking targets of the last two cycles.
+ * Push and STDP work is split into 128-synapse items, one per warp, four
+ * independent synapses per lane. */
+__global__ void __launch_bounds__(BLOCK, 1)
 k_cycles(const __grid_constant__ CycleArgs A)
 {
-	extern __shared__ uint32_t shLists[];
-	uint32_t* sFired = shLists;
-	uint32_t* sPost = shLists + A.listCap;
-	__shared__ uint32_t sNFired, sNPost, sPostBase;
+	__shared__ uint32_t sNFired;
+	__shared__ uint32_t sNPost[2];
 	__shared__ unsigned long long sEvents;
 
 	const NetDev& net = A.net;
 	const uint32_t tid = threadIdx.x;
 	const uint32_t lane = tid & 31u;
+	const uint32_t warp = tid >> 5;
 	const uint32_t lt = (1u << lane) - 1u;
 	const uint32_t warpsPerBlock = blockDim.x >> 5;
 	const uint32_t gridWarps = gridDim.x * warpsPerBlock;
-	const uint32_t myWarp = blockIdx.x * warpsPerBlock + (tid >> 5);
+	/* 32-neuron warps are dealt to blocks round-robin, so that every block
+	 * updates (and then pushes and learns for) a similar share */
+	const uint32_t myWarp = warp * gridDim.x + blockIdx.x;
 	const uint32_t totalWarps = A.groupWarp[A.ngroups];
 	const size_t nDev = net.nDev;
+	const uint32_t cap = A.listCap;
+	uint32_t* firedList = net.lists + size_t(blockIdx.x) * cap * 9u;
+	uint32_t* postLists = firedList + size_t(cap) * 3u;
+
+	if(tid == 0) {
+		sNPost[0] = 0;
+		sNPost[1] = 0;
+	}
 
 	for(uint32_t k = 0; k <= A.cycles; ++k) {
-		const uint32_t t = A.firstCycle + k;
+		const uint64_t t64 = A.firstCycle + k;
+		const uint32_t t = uint32_t(t64);
+		const uint32_t slotT = uint32_t(t64 % net.slots);   /* current slot of cycle t */
 		const bool doUpdate = k < A.cycles;
+		const uint32_t pb = t & 1u;
 
 		if(tid == 0) {
 			sNFired = 0;
-			sNPost = 0;
 			sEvents = 0;
-			if(doUpdate && blockIdx.x == 0) {
-				/* consumed in the previous phase; refilled in the next */
-				if(net.stdp) net.postCount[(t + 1) % 3u] = 0;
-				net.firedCountRing[(t + 1) & net.ringMask] = 0;
-				net.eventsRing[(t + 1) & net.ringMask] = 0;
+			if(doUpdate) {
+				sNPost[pb] = 0;
+				if(blockIdx.x == 0) {
+					net.firedCountRing[(t + 1) & net.ringMask] = 0;
+					net.eventsRing[(t + 1) & net.ringMask] = 0;
+				}
 			}
 		}
 		__syncthreads();
+		unsigned long long* trace = A.trace ? A.trace + (size_t(k) * gridDim.x + blockIdx.x) * 4u : nullptr;
+		if(trace && tid == 0) trace[0] = globalTimer();
 
 		/* ---- neuron update of cycle t ---- */
 		if(doUpdate) {
-			const uint32_t slot = t & net.qMask;
+			const uint32_t slot = slotT;
 			const uint64_t* rfIn = net.rf + (t & 1u) * nDev;
 			uint64_t* rfOut = net.rf + ((t + 1) & 1u) * nDev;
+			uint32_t* postOut = postLists + size_t(pb) * cap * 3u;
 			for(uint32_t gw = myWarp; gw < totalWarps; gw += gridWarps) {
 				int gi = 0;
 				while(gw >= A.groupWarp[gi + 1]) ++gi;
@@ -374,6 +420,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const uint32_t n = G.devBase + i;
 				const bool valid = i < G.count;
 				const uint32_t stimWord = takeStimWord(net, n, lane);
+				uint64_t rfPrev = valid ? rfIn[n] : 0ull;
 				bool fired = false;
 				if(valid) {
 					const bool stim = (stimWord >> lane) & 1u;
@@ -385,9 +432,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						default: fired = modelInput(net, G, i, n, slot, stim); break;
 					}
 				}
-				uint64_t rfNew = 0;
+				const uint64_t rfNew = (rfPrev << 1) | uint64_t(fired);
 				if(valid) {
-					rfNew = (rfIn[n] << 1) | uint64_t(fired);
 					rfOut[n] = rfNew;
 				}
 				const uint32_t word = __ballot_sync(FULL, fired);
@@ -398,8 +444,16 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					uint32_t base = 0;
 					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
 					base = __shfl_sync(FULL, base, 0);
-					if(fired) sFired[base + __popc(word & lt)] = n;
-					uint32_t deg = fired ? net.outDegree[n] : 0u;
+					uint32_t deg = 0;
+					if(fired) {
+						uint64_t b = net.rowStart[size_t(n) * net.rowStride];
+						uint64_t e = net.rowStart[size_t(n + 1) * net.rowStride];
+						deg = uint32_t(e - b);
+						uint32_t* entry = firedList + size_t(base + __popc(word & lt)) * 3u;
+						entry[0] = n;
+						entry[1] = uint32_t(b);
+						entry[2] = deg;
+					}
 					uint32_t ev = __reduce_add_sync(FULL, deg);
 					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
 				}
@@ -409,100 +463,59 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t pm = __ballot_sync(FULL, post);
 					if(pm) {
 						uint32_t base = 0;
-						if(lane == 0) base = atomicAdd(&sNPost, uint32_t(__popc(pm)));
+						if(lane == 0) base = atomicAdd(&sNPost[pb], uint32_t(__popc(pm)));
 						base = __shfl_sync(FULL, base, 0);
-						if(post) sPost[base + __popc(pm & lt)] = n;
-					}
-				}
-			}
-		}
-		__syncthreads();
-
-		if(doUpdate) {
-			if(tid == 0) {
-				if(sNPost) sPostBase = atomicAdd(&net.postCount[t % 3u], sNPost);
-				if(sNFired) {
-					atomicAdd(&net.firedCountRing[t & net.ringMask], sNFired);
-					atomicAdd(&net.eventsRing[t & net.ringMask], sEvents);
-					atomicAdd(&net.stats[2], (unsigned long long) sNFired);
-					atomicAdd(&net.stats[3], sEvents);
-					if(net.deliver) atomicAdd(&net.stats[0], sEvents);
-				}
-			}
-			__syncthreads();
-			uint32_t* postOut = net.postList + size_t(t % 3u) * nDev + sPostBase;
-			for(uint32_t j = tid; j < sNPost; j += blockDim.x) {
-				postOut[j] = sPost[j];
-			}
-
-			/* ---- spike push: fired sources stream their synapses into the
-			 * current slots of cycles t + delay ---- */
-			if(net.deliver) {
-				unsigned long long* acc = reinterpret_cast<unsigned long long*>(net.acc);
-				const uint32_t stride = blockDim.x;
-				for(uint32_t f = 0; f < sNFired; ++f) {
-					const uint32_t s = sFired[f];
-					const uint64_t b = net.rowStart[size_t(s) * net.rowStride];
-					const uint64_t e = net.rowStart[size_t(s + 1) * net.rowStride];
-					for(uint64_t j0 = b + tid; j0 < e; j0 += 4 * uint64_t(stride)) {
-						uint2 syn[4];
-#pragma unroll
-						for(int u = 0; u < 4; ++u) {
-							uint64_t j = j0 + uint64_t(u) * stride;
-							syn[u] = j < e ? net.fcm[j] : make_uint2(0u, 0u);
-						}
-#pragma unroll
-						for(int u = 0; u < 4; ++u) {
-							if(j0 + uint64_t(u) * stride < e) {
-								const uint32_t target = syn[u].x >> 6;
-								const uint32_t slot = (t + (syn[u].x & 63u) + 1u) & net.qMask;
-								const int32_t w = int32_t(syn[u].y);
-								atomicAdd(&acc[(size_t(slot) * nDev + target) * 2 + (w < 0 ? 1 : 0)],
-										(unsigned long long) (long long) w);
-							}
+						if(post) {
+							uint64_t b = net.rcmStart[n];
+							uint64_t e = net.rcmStart[n + 1];
+							uint32_t* entry = postOut + size_t(base + __popc(pm & lt)) * 3u;
+							entry[0] = n;
+							entry[1] = uint32_t(b);
+							entry[2] = uint32_t(e - b);
 						}
 					}
 				}
 			}
 		}
-
-		/* ---- STDP accumulation of cycle t-1 (ConnectivityMatrix.cpp:224-258):
-		 * 128-synapse chunks of each post-spiking target, one chunk per warp;
-		 * every accumulator has a single writer ---- */
+		/* ---- STDP accumulation of cycle t-1 (ConnectivityMatrix.cpp:224-258)
+		 * for this block's targets that fired P cycles before it; every
+		 * accumulator has a single writer. It only reads the history after
+		 * cycle t-1, so warps start on it as soon as their own update of
+		 * cycle t is done ---- */
 		if(net.stdp && k > 0) {
-			const uint32_t tp = t - 1;
-			const uint32_t buf = tp % 3u;
-			const uint32_t cnt = net.postCount[buf];
-			const uint32_t* list = net.postList + size_t(buf) * nDev;
+			const uint32_t* postIn = postLists + size_t(pb ^ 1u) * cap * 3u;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
-			const uint32_t items = cnt * net.stdpChunks;
+			const uint32_t items = sNPost[pb ^ 1u] * net.stdpChunks;
 			uint64_t visited = 0;
-			for(uint32_t it = myWarp; it < items; it += gridWarps) {
-				const uint32_t target = list[it / net.stdpChunks];
-				const uint64_t end = net.rcmStart[target + 1];
-				const uint64_t b = net.rcmStart[target] + uint64_t(it % net.stdpChunks) * 128u;
-				if(b >= end) continue;
-				const uint64_t e = b + 128u < end ? b + 128u : end;
-				visited += e - b;
+			for(uint32_t it = warp; it < items; it += warpsPerBlock) {
+				const uint32_t* entry = postIn + size_t(it / net.stdpChunks) * 3u;
+				const uint32_t off = (it % net.stdpChunks) * 128u;
+				const uint32_t len = entry[2];
+				if(off >= len) continue;
+				const uint64_t b = uint64_t(entry[1]) + off;
+				const uint32_t cnt = len - off < 128u ? len - off : 128u;
+				visited += cnt;
 				uint32_t sd[4];
 #pragma unroll
 				for(int u = 0; u < 4; ++u) {
-					uint64_t j = b + lane + 32u * u;
-					sd[u] = j < e ? net.rcmSrcDelay[j] : 0u;
+					uint32_t j = lane + 32u * u;
+					sd[u] = j < cnt ? net.rcmSrcDelay[b + j] : 0u;
 				}
 				uint64_t pre[4];
+				int32_t old[4];
 #pragma unroll
 				for(int u = 0; u < 4; ++u) {
-					uint64_t j = b + lane + 32u * u;
-					pre[u] = j < e ? shr64(rfAfter[sd[u] >> 6], (sd[u] & 63u) + 1u) : 0ull;
+					uint32_t j = lane + 32u * u;
+					pre[u] = j < cnt ? shr64(rfAfter[sd[u] >> 6], (sd[u] & 63u) + 1u) : 0ull;
+					old[u] = j < cnt ? net.rcmAcc[b + j] : 0;
 				}
 #pragma unroll
 				for(int u = 0; u < 4; ++u) {
-					uint64_t j = b + lane + 32u * u;
-					if(j < e) {
+					uint32_t j = lane + 32u * u;
+					if(j < cnt) {
 						int32_t dw = weightChange(pre[u], A.rule);
 						if(dw != 0) {
-							net.rcmAcc[j] = int32_t(uint32_t(net.rcmAcc[j]) + uint32_t(dw));
+							net.rcmAcc[b + j] = int32_t(uint32_t(old[u]) + uint32_t(dw));
 						}
 					}
 				}
@@ -512,11 +525,59 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			}
 		}
 
+		__syncthreads();
+		if(trace && tid == 0) trace[1] = globalTimer();
+
+		if(doUpdate) {
+			if(tid == 0 && sNFired) {
+				atomicAdd(&net.firedCountRing[t & net.ringMask], sNFired);
+				atomicAdd(&net.eventsRing[t & net.ringMask], sEvents);
+				atomicAdd(&net.stats[2], (unsigned long long) sNFired);
+				atomicAdd(&net.stats[3], sEvents);
+				if(net.deliver) atomicAdd(&net.stats[0], sEvents);
+			}
+
+			/* ---- spike push: the synapses of this block's fired sources go
+			 * into the current slots of cycles t + delay ---- */
+			if(net.deliver) {
+				const uint32_t items = sNFired * net.fireChunks;
+				for(uint32_t it = warp; it < items; it += warpsPerBlock) {
+					const uint32_t* entry = firedList + size_t(it / net.fireChunks) * 3u;
+					const uint32_t off = (it % net.fireChunks) * 128u;
+					const uint32_t len = entry[2];
+					if(off >= len) continue;
+					const uint64_t b = uint64_t(entry[1]) + off;
+					const uint32_t cnt = len - off < 128u ? len - off : 128u;
+					uint2 syn[4];
+#pragma unroll
+					for(int u = 0; u < 4; ++u) {
+						uint32_t j = lane + 32u * u;
+						syn[u] = j < cnt ? net.fcm[b + j] : make_uint2(0u, 0u);
+					}
+#pragma unroll
+					for(int u = 0; u < 4; ++u) {
+						if(lane + 32u * u < cnt) {
+							/* slot of cycle t + d, d <= maxDelay < slots */
+							uint32_t s = slotT + (syn[u].x & 63u) + 1u;
+							s = s >= net.slots ? s - net.slots : s;
+							const int32_t w = int32_t(syn[u].y);
+							addCurrent(net, s, syn[u].x >> 6, w < 0 ? 1 : 0, w);
+						}
+					}
+				}
+			}
+		}
+
+		if(trace) {
+			__syncthreads();
+			if(tid == 0) trace[2] = globalTimer();
+		}
 		if(k < A.cycles) {
 			if(!gridSync(net.barrier, A.timeoutNs)) {
 				return;
 			}
 		}
+		if(trace && tid == 0) trace[3] = globalTimer();
 	}
 }
 
@@ -537,23 +598,64 @@ k_stimulus(NetDev net, StimDev s)
 }
 
 /* applyStdp (src/nemo/ConnectivityMatrix.cpp:272-325): every plastic synapse
- * gets w = clamp(w + (reward * acc) >> f) and its accumulator cleared. */
-__global__ void __launch_bounds__(BLOCK)
-k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t nrcm)
+ * gets w = clamp(w + (reward * acc) >> f) and its accumulator cleared.
+ *
+ * The reference reads a synapse's weight when the spike arrives
+ * (deliverSpikes at cycle t0 + d), whereas the step kernel adds it when the
+ * source fires (cycle t0). For a spike still in flight when its synapse's
+ * weight changes, the arrival slot therefore holds the old weight; it is
+ * corrected here by w_new - w_old, into the same E/I half (the sign of a
+ * weight never changes, and a weight that reaches 0 contributes 0 to E). The
+ * in-flight spikes of a synapse with delay d are the set bits 0..d-1 of its
+ * source's firing history after the last completed cycle (cycleNow - 1):
+ * bit k fired at cycleNow-1-k and arrives at cycleNow-1-k+d.
+ *
+ * The synapses are processed in APPLY_WINDOW-sized windows of the forward
+ * matrix, one launch per window, so that the weights a launch rewrites stay
+ * in L2 (each target's plastic synapses are sorted by forward position, and
+ * rcmWindow locates the range of each target in each window). One warp per
+ * target. */
+__global__ void __launch_bounds__(256)
+k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint32_t window)
 {
-	uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for(uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < nrcm; j += stride) {
+	const uint64_t* rfNow = net.rf + size_t(cycleNow & 1u) * net.nDev;
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+	for(uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < net.nDev; t += nwarps) {
+	const uint64_t base = net.rcmStart[t];
+	const uint32_t* win = net.rcmWindow + size_t(t) * (net.windows + 1) + window;
+	const uint64_t e = base + win[1];
+	for(uint64_t j = base + win[0] + lane; j < e; j += 32) {
 		uint32_t f = net.rcmForward[j];
 		int32_t acc = net.rcmAcc[j];
-		int32_t wOld = int32_t(net.fcm[f].y);
+		uint2 syn = net.fcm[f];
+		int32_t wOld = int32_t(syn.y);
 		int32_t diff = int32_t((int64_t(reward) * int64_t(acc)) >> net.fbits);
 		int32_t wNew = updatedWeight(wOld, diff, rule);
 		if(wNew != wOld) {
 			net.fcm[f].y = uint32_t(wNew);
+			if(net.deliver) {
+				uint32_t sd = net.rcmSrcDelay[j];
+				uint32_t d = (sd & 63u) + 1u;
+				uint64_t pending = rfNow[sd >> 6] & ((uint64_t(1) << d) - 1u);
+				if(pending) {
+					size_t target = syn.x >> 6;
+					long long delta = (long long) wNew - (long long) wOld;
+					int half = wOld >= 0 ? 0 : 1;
+					while(pending) {
+						uint32_t k = uint32_t(__ffsll((long long) pending) - 1);
+						pending &= pending - 1;
+						/* fired at cycleNow-1-k >= 0, arrives at cycleNow-1-k+d */
+						uint32_t slot = uint32_t((cycleNow - 1u - k + d) % net.slots);
+						addCurrent(net, slot, uint32_t(target), half, delta);
+					}
+				}
+			}
 		}
 		if(acc) {
 			net.rcmAcc[j] = 0;
 		}
+	}
 	}
 }
 
@@ -607,58 +709,43 @@ launchStimulus(const NetDev& net, const StimDev& stim, void* stream)
 	k_stimulus<<<(n + 255) / 256, 256, 0, S(stream)>>>(net, stim);
 }
 
-/* Co-resident grid: as many blocks per SM as the kernel's registers allow
- * (shared memory is small), times the SM count. */
+/* Co-resident grid for the cooperative launch: as many 1024-thread blocks per
+ * SM as the registers allow (one), times the SM count. */
 void
 cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap)
 {
 	const uint32_t warpsPerBlock = BLOCK / 32;
-	int sms = smCount();
-	/* the list capacity depends on the grid, and the shared memory on the
-	 * capacity; the fixed point is reached in two rounds for these sizes */
-	uint32_t cap = BLOCK;
-	for(int round = 0; round < 3; ++round) {
+	if(g_blocksPerSm == 0) {
 		int perSm = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles, BLOCK, size_t(2) * cap * 4);
-		if(perSm <= 0) perSm = 1;
-		g_blocksPerSm = perSm;
-		unsigned b = unsigned(sms * perSm);
-		uint32_t gridWarps = b * warpsPerBlock;
-		uint32_t perWarp = (totalWarps + gridWarps - 1) / gridWarps;
-		if(perWarp == 0) perWarp = 1;
-		uint32_t need = perWarp * warpsPerBlock * 32;
-		*blocks = b;
-		if(need <= cap) break;
-		cap = need;
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles, BLOCK, 0);
+		g_blocksPerSm = perSm > 0 ? perSm : 1;
 	}
-	*listCap = cap;
-}
-
-unsigned
-launchCycles(const CycleArgs& args, void* stream)
-{
-	unsigned blocks;
-	uint32_t cap;
-	cyclesGrid(args.groupWarp[args.ngroups], &blocks, &cap);
-	CycleArgs a = args;
-	a.listCap = cap;
-	size_t smem = size_t(2) * cap * 4;
-	if(smem > 48 * 1024) {
-		cudaFuncSetAttribute(k_cycles, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-	}
-	void* params[] = {&a};
-	cudaLaunchCooperativeKernel((const void*) k_cycles, dim3(blocks), dim3(BLOCK), params, smem, S(stream));
-	return blocks;
+	unsigned b = unsigned(smCount() * g_blocksPerSm);
+	uint32_t gridWarps = b * warpsPerBlock;
+	uint32_t perWarp = (totalWarps + gridWarps - 1) / gridWarps;
+	if(perWarp == 0) perWarp = 1;
+	*blocks = b;
+	*listCap = perWarp * warpsPerBlock * 32;
 }
 
 void
-launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, void* stream)
+launchCycles(const CycleArgs& args, unsigned blocks, void* stream)
 {
-	uint64_t blocks = (nrcm + 255) / 256;
+	void* params[] = {const_cast<CycleArgs*>(&args)};
+	cudaLaunchCooperativeKernel((const void*) k_cycles, dim3(blocks), dim3(BLOCK), params, 0, S(stream));
+}
+
+void
+launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, uint64_t cycleNow, void* stream)
+{
+	if(nrcm == 0) return;
+	/* one warp per target per window */
+	uint64_t blocks = (uint64_t(net.nDev) * 32 + 255) / 256;
 	uint64_t cap = uint64_t(smCount()) * 8;
 	if(blocks > cap) blocks = cap;
-	if(blocks == 0) blocks = 1;
-	k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, nrcm);
+	for(uint32_t w = 0; w < net.windows; ++w) {
+		k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow, w);
+	}
 }
 
 void

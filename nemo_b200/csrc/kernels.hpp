@@ -35,11 +35,16 @@ namespace nemo_b200 {
 
 const int MAX_GROUPS = 8;
 
+/* applyStdp window: 4M synapses = 32 MB of the forward matrix, small enough
+ * to stay resident in the 126 MB L2 while its weights are updated */
+const uint64_t APPLY_WINDOW = uint64_t(1) << 22;
+
 struct NetDev {
 	uint32_t nDev;          /* device neurons, multiple of 32 */
 	uint32_t nWords;        /* nDev / 32 */
 	uint32_t rowStride;     /* rows per source: max(maxDelay, 1) */
-	uint32_t qMask;         /* current slots - 1 (power of two > maxDelay) */
+	uint32_t slots;         /* current slots: maxDelay + 1 (cycle t uses slot t mod slots) */
+	int acc32;              /* int32 accumulators (proven not to overflow), else int64 */
 	uint32_t ringMask;      /* firing-ring cycles - 1 */
 	uint32_t fbits;         /* fractional bits of the Q(31-f).f weights */
 	int deliver;            /* 0 when no delay is deliverable (max delay 64) */
@@ -51,7 +56,7 @@ struct NetDev {
 	uint2* fcm;                    /* {target << 6 | (delay - 1), int32 weight} */
 	const uint32_t* outDegree;     /* [nDev] synapses per source */
 
-	long long* acc;                /* [slots][nDev][2] int64 E, I current of a future cycle */
+	void* acc;                     /* [slots][nDev][2] E, I current of a future cycle (int32 or int64) */
 	uint64_t* rf;                  /* [2][nDev] firing history, bit 0 = last cycle */
 	uint32_t* firedRing;           /* [ring][nWords] firing bitmaps by cycle */
 	unsigned long long* eventsRing;/* [ring] synaptic events (fired x out-degree) */
@@ -59,16 +64,22 @@ struct NetDev {
 	float* ext;                    /* [nDev] external current, cleared after use */
 	uint32_t* fstim;               /* [nWords] firing stimulus, cleared after use */
 
+	/* per-block work lists of the step kernel: [blocks][9 * listCap] */
+	uint32_t* lists;
+	uint32_t fireChunks;           /* 128-synapse chunks per source (max out-degree) */
+
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
 	uint32_t stdpChunks;           /* 128-synapse chunks per target (max in-degree) */
-	uint32_t* postList;            /* [3][nDev] */
-	uint32_t* postCount;           /* [3] */
 	const uint64_t* rcmStart;      /* [nDev + 1] */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
-	const uint32_t* rcmForward;    /* index into fcm */
+	const uint32_t* rcmForward;    /* index into fcm, ascending within a target */
 	int32_t* rcmAcc;
+	/* [nDev][windows + 1]: first synapse of each target in each forward
+	 * window of APPLY_WINDOW synapses (applyStdp works window by window) */
+	const uint32_t* rcmWindow;
+	uint32_t windows;
 
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;
@@ -110,10 +121,13 @@ struct CycleArgs {
 	GroupDev groups[MAX_GROUPS];
 	uint32_t groupWarp[MAX_GROUPS + 1];  /* prefix of 32-neuron warps per group */
 	int ngroups;
-	uint32_t firstCycle;
+	uint64_t firstCycle;
 	uint32_t cycles;
-	uint32_t listCap;                    /* per-block shared list capacity */
+	uint32_t listCap;                    /* entries per per-block work list */
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
+	/* optional phase timestamps (%globaltimer ns), [cycle][block][4]: phase
+	 * start, update done, push and STDP done, barrier passed */
+	unsigned long long* trace;
 };
 
 struct StimDev {
@@ -126,11 +140,13 @@ struct StimDev {
 
 /* Launchers (kernels.cu), all on `stream`. */
 void launchStimulus(const NetDev& net, const StimDev& stim, void* stream);
-/* Cooperative launch of k_cycles; returns the grid size used. */
-unsigned launchCycles(const CycleArgs& args, void* stream);
-/* Largest co-resident grid and the shared-memory list capacity it needs. */
+/* Cooperative launch of k_cycles over `blocks` blocks (from cyclesGrid). */
+void launchCycles(const CycleArgs& args, unsigned blocks, void* stream);
+/* The co-resident grid (one block per SM) and the per-block list capacity
+ * (the most neurons one block updates in a cycle). */
 void cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap);
-void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, void* stream);
+void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, uint64_t cycleNow,
+		void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);

@@ -328,6 +328,12 @@ nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out
 }
 
 nemo_status_t
+nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[8])
+{
+	RETURN_CALL(s->sim.trace(cycles, out));
+}
+
+nemo_status_t
 nemo_b200_libm_check(nemo_simulation_t s, uint64_t* mismatches)
 {
 	RETURN_CALL(*mismatches = s->sim.libmCheck());

@@ -218,6 +218,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	for(size_t r = 0; r < nrows; ++r) rowStart[r + 1] += rowStart[r];
 	std::vector<uint2> fcm(S);
 	std::vector<uint32_t> fcmPos(S);
+	std::vector<uint32_t> synAt(S);   /* synapse at each forward position */
 	std::vector<uint32_t> outDegree(m_nDev, 0);
 	{
 		std::vector<uint64_t> fill(rowStart.begin(), rowStart.end() - 1);
@@ -226,6 +227,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 			uint64_t pos = fill[r]++;
 			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(toFix(net.wgt[s], m_fbits)));
 			fcmPos[s] = uint32_t(pos);
+			synAt[pos] = uint32_t(s);
 			outDegree[dsrc[s]]++;
 		}
 	}
@@ -234,12 +236,36 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	 * (src/nemo/cpu/Simulation.cpp:264): every delay up to 63 ms is
 	 * delivered, and with a 64 ms synapse present none is */
 	const bool deliver = S > 0 && m_maxDelay < 64;
-	uint32_t slots = 2;
-	while(deliver && slots <= m_maxDelay) slots *= 2;
+	/* current slots: arrivals for cycle c go to slot c mod (maxDelay + 1);
+	 * a slot is drained at its cycle before any spike for the cycle one
+	 * revolution later can be pushed */
+	const uint32_t slots = deliver ? m_maxDelay + 1 : 1;
+
+	/* int32 accumulators are exact when no slot can leave the int32 range:
+	 * a slot of target t only ever holds at most one arrival per incoming
+	 * synapse, so it is bounded by the sum of its in-weights, taking each
+	 * plastic weight at its STDP limit if that is larger */
+	bool acc32 = true;
+	{
+		std::vector<int64_t> pos(m_nDev, 0), neg(m_nDev, 0);
+		for(size_t s = 0; s < S; ++s) {
+			int64_t w = int32_t(fcm[fcmPos[s]].y);
+			if(m_stdpOn && net.plastic[s]) {
+				if(w > 0) w = std::max<int64_t>(w, m_rule.maxE);
+				else if(w < 0) w = std::min<int64_t>(w, m_rule.maxI);
+			}
+			if(w >= 0) pos[dtgt[s]] += w;
+			else neg[dtgt[s]] += w;
+		}
+		for(uint32_t n = 0; n < m_nDev && acc32; ++n) {
+			acc32 = pos[n] <= INT32_MAX && neg[n] >= INT32_MIN;
+		}
+	}
 
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
 	std::vector<uint64_t> rcmStart;
-	std::vector<uint32_t> rcmSrcDelay, rcmForward;
+	std::vector<uint32_t> rcmSrcDelay, rcmForward, rcmWindow;
+	m_windows = 1;
 	uint64_t maxIn = 0;
 	if(m_stdpOn) {
 		rcmStart.assign(size_t(m_nDev) + 1, 0);
@@ -251,17 +277,38 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		m_nrcm = rcmStart[m_nDev];
 		rcmSrcDelay.resize(m_nrcm);
 		rcmForward.resize(m_nrcm);
+		/* filled in forward order, so each target's synapses are sorted by
+		 * their position in the forward matrix */
 		std::vector<uint64_t> fill(rcmStart.begin(), rcmStart.end() - 1);
-		for(size_t s = 0; s < S; ++s) {
+		for(size_t pos = 0; pos < S; ++pos) {
+			size_t s = synAt[pos];
 			if(!net.plastic[s]) continue;
 			uint64_t j = fill[dtgt[s]]++;
 			rcmSrcDelay[j] = (dsrc[s] << 6) | (net.dly[s] - 1);
-			rcmForward[j] = fcmPos[s];
+			rcmForward[j] = uint32_t(pos);
+		}
+		/* applyStdp works through the forward matrix in windows small enough
+		 * to stay in L2; rcmWindow[t][k] is the first of target t's synapses
+		 * at forward position >= k * APPLY_WINDOW */
+		m_windows = uint32_t((S + APPLY_WINDOW - 1) / APPLY_WINDOW);
+		if(m_windows == 0) m_windows = 1;
+		const uint32_t K = m_windows;
+		rcmWindow.assign(size_t(m_nDev) * (K + 1), 0);
+		for(uint32_t t = 0; t < m_nDev; ++t) {
+			uint64_t base = rcmStart[t], len = rcmStart[t + 1] - base, j = 0;
+			for(uint32_t k = 0; k <= K; ++k) {
+				while(j < len && rcmForward[base + j] < uint64_t(k) * APPLY_WINDOW) j++;
+				rcmWindow[size_t(t) * (K + 1) + k] = uint32_t(k == K ? len : j);
+			}
 		}
 	}
+	/* 128-synapse work items per post-spiking target / per fired source */
 	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + 127) / 128);
-	if(uint64_t(m_nDev) * stdpChunks >= (uint64_t(1) << 32)) {
-		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 plastic synapses per target neuron");
+	uint64_t maxOut = 0;
+	for(uint32_t n = 0; n < m_nDev; ++n) maxOut = std::max<uint64_t>(maxOut, outDegree[n]);
+	const uint64_t fireChunks = std::max<uint64_t>(1, (maxOut + 127) / 128);
+	if(uint64_t(m_nDev) * std::max(stdpChunks, fireChunks) >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 synapses per neuron");
 	}
 
 	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
@@ -292,14 +339,15 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.nDev = m_nDev;
 	m_net.nWords = m_nDev / 32;
 	m_net.rowStride = Ds;
-	m_net.qMask = slots - 1;
+	m_net.slots = slots;
+	m_net.acc32 = acc32 ? 1 : 0;
 	m_net.ringMask = m_ring - 1;
 	m_net.fbits = m_fbits;
 	m_net.deliver = deliver ? 1 : 0;
 	m_net.rowStart = (const uint64_t*) put(rowStart.data(), rowStart.size() * 8);
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
-	m_net.acc = (long long*) alloc(size_t(slots) * m_nDev * 16);
+	m_net.acc = alloc(size_t(slots) * m_nDev * (acc32 ? 8 : 16));
 	m_net.rf = (uint64_t*) alloc(size_t(2) * m_nDev * 8);
 	m_net.firedRing = (uint32_t*) alloc(size_t(m_ring) * m_net.nWords * 4);
 	m_net.eventsRing = (unsigned long long*) alloc(size_t(m_ring) * 8);
@@ -310,14 +358,23 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.barrier = (unsigned*) alloc(4 * 4);
 	m_net.stdp = m_stdpOn ? 1 : 0;
 	m_net.stdpChunks = uint32_t(stdpChunks);
+	m_net.fireChunks = uint32_t(fireChunks);
+	{
+		uint32_t totalWarps = 0;
+		for(const Group& g : m_groups) totalWarps += (g.count + 31) / 32;
+		uint32_t cap;
+		cyclesGrid(totalWarps, &m_blocks, &cap);
+		m_args.listCap = cap;
+		m_net.lists = (uint32_t*) alloc(size_t(m_blocks) * cap * 9 * 4);
+	}
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
-		m_net.postList = (uint32_t*) alloc(size_t(m_nDev) * 3 * 4);
-		m_net.postCount = (uint32_t*) alloc(3 * 4);
 		m_net.rcmStart = (const uint64_t*) put(rcmStart.data(), rcmStart.size() * 8);
 		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
 		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
 		m_net.rcmAcc = (int32_t*) alloc(size_t(m_nrcm) * 4);
+		m_net.rcmWindow = (const uint32_t*) put(rcmWindow.data(), rcmWindow.size() * 4);
+		m_net.windows = m_windows;
 	}
 
 	/* per-neuron RNG seeds by simulation index (src/nemo/RNG.cpp:39-62):
@@ -407,12 +464,12 @@ void
 Simulation::launchBlock(uint64_t first, unsigned cycles)
 {
 	CycleArgs a = m_args;
-	a.firstCycle = uint32_t(first);
+	a.firstCycle = first;
 	a.cycles = cycles;
 	for(int gi = 0; gi < a.ngroups; ++gi) {
 		a.groups[gi].timerBase = uint32_t(m_timerBase);
 	}
-	launchCycles(a, m_stream);
+	launchCycles(a, m_blocks, m_stream);
 	NEMO_CUDA(cudaGetLastError());
 }
 
@@ -573,7 +630,7 @@ Simulation::applyStdp(float reward)
 		fail(NEMO_INVALID_INPUT, msg.str());
 	}
 	if(m_nrcm) {
-		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
+		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_cycle, m_stream);
 	}
 	m_fcmHostValid = false;
 }
@@ -807,7 +864,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 		launchBlock(m_cycle, cyclesPerStep);
 		m_cycle += cyclesPerStep;
 		if(apply && m_nrcm) {
-			launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_stream);
+			launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_cycle, m_stream);
 		}
 	}
 	NEMO_CUDA(cudaEventRecord(e1, stream));
@@ -843,7 +900,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	m_cycle += cycles;
 	NEMO_CUDA(cudaEventRecord(e1, stream));
 	if(m_stdpOn && m_nrcm) {
-		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_nrcm, m_stream);
+		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_nrcm, m_cycle, m_stream);
 		m_fcmHostValid = false;
 	}
 	NEMO_CUDA(cudaEventRecord(e2, stream));
@@ -858,11 +915,8 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	readStats(after);
 	checkDeviceError();
 	m_stateDirty = true;
-	unsigned blocks;
-	uint32_t cap;
-	cyclesGrid(m_args.groupWarp[m_args.ngroups], &blocks, &cap);
 	out[0] = tc;
-	out[1] = blocks;
+	out[1] = m_blocks;
 	out[2] = 0;
 	out[3] = double(after[0] - before[0]);
 	out[4] = double(after[2] - before[2]);
@@ -871,6 +925,60 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	out[7] = (m_stdpOn && m_nrcm) ? ta : 0.0;
 	out[8] = double(m_nrcm);
 	out[9] = double(after[3] - before[3]);
+}
+
+void
+Simulation::trace(unsigned cycles, double out[8])
+{
+	if(cycles == 0) {
+		fail(NEMO_INVALID_INPUT, "trace: no cycles");
+	}
+	cudaStream_t stream = STREAM(m_stream);
+	size_t words = size_t(cycles + 1) * m_blocks * 4;
+	unsigned long long* dTrace;
+	NEMO_CUDA(cudaMalloc(&dTrace, words * 8));
+	NEMO_CUDA(cudaMemsetAsync(dTrace, 0, words * 8, stream));
+	CycleArgs a = m_args;
+	a.firstCycle = m_cycle;
+	a.cycles = cycles;
+	a.trace = dTrace;
+	for(int gi = 0; gi < a.ngroups; ++gi) a.groups[gi].timerBase = uint32_t(m_timerBase);
+	launchCycles(a, m_blocks, m_stream);
+	NEMO_CUDA(cudaGetLastError());
+	m_cycle += cycles;
+	m_stateDirty = true;
+	std::vector<unsigned long long> h(words);
+	NEMO_CUDA(cudaMemcpyAsync(h.data(), dTrace, words * 8, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	cudaFree(dTrace);
+	checkDeviceError();
+	double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+	for(unsigned k = 0; k < cycles; ++k) {
+		double minT0 = 1e300, maxT3 = 0, maxU = 0, sumU = 0, maxW = 0, sumW = 0, maxT2 = 0, minT2 = 1e300, sumT3 = 0;
+		for(unsigned b = 0; b < m_blocks; ++b) {
+			const unsigned long long* r = &h[(size_t(k) * m_blocks + b) * 4];
+			double t0 = double(r[0]), t1 = double(r[1]), t2 = double(r[2]), t3 = double(r[3]);
+			minT0 = std::min(minT0, t0);
+			maxT3 = std::max(maxT3, t3);
+			maxU = std::max(maxU, t1 - t0);
+			sumU += t1 - t0;
+			maxW = std::max(maxW, t2 - t1);
+			sumW += t2 - t1;
+			maxT2 = std::max(maxT2, t2);
+			minT2 = std::min(minT2, t2);
+			sumT3 += t3;
+		}
+		acc[0] += maxT3 - minT0;
+		acc[1] += maxU;
+		acc[2] += sumU / m_blocks;
+		acc[3] += maxW;
+		acc[4] += sumW / m_blocks;
+		acc[5] += maxT2 - minT0;
+		acc[6] += sumT3 / m_blocks - maxT2;
+		acc[7] += maxT2 - minT2;
+	}
+	for(int i = 0; i < 8; ++i) out[i] = acc[i] / cycles;
 }
 
 uint64_t

@@ -80,6 +80,13 @@ public:
 
 	void readStats(uint64_t out[4]);
 
+	/* Phase timing of one traced persistent launch of `cycles` cycles, means
+	 * over cycles in ns: [0] phase (first start to last barrier exit),
+	 * [1] max / [2] mean block update time, [3] max / [4] mean block push +
+	 * STDP time, [5] first start to last block done, [6] last arrival to
+	 * mean barrier exit, [7] spread of block arrivals. */
+	void trace(unsigned cycles, double out[8]);
+
 private:
 	struct Group {
 		NeuronType type;
@@ -123,6 +130,8 @@ private:
 
 	NetDev m_net;
 	CycleArgs m_args;
+	unsigned m_blocks;          /* grid of the persistent step kernel */
+	uint32_t m_windows;         /* forward-matrix windows of applyStdp */
 	bool m_stdpOn;
 	StdpRule m_rule;
 	StdpFunction m_stdpFn;
