@@ -15,8 +15,8 @@ extern "C" {
 #endif
 
 /* Run `cycles` cycles (<= 1024 per call) without stimulus, entirely on the
- * device as one CUDA graph (gather, neuron update with scatter, STDP
- * accumulation per cycle). Equivalent to `cycles` calls of nemo_step with
+ * device in one persistent launch of the step kernel (neuron update, spike
+ * push and STDP accumulation per cycle, one grid barrier per cycle). Equivalent to `cycles` calls of nemo_step with
  * empty stimulus. fired_counts[k] / events[k] (each may be NULL) receive the
  * number of neurons fired in cycle k and the synaptic events those firings
  * generate (fired neurons x out-degree, the throughput unit of the
@@ -37,19 +37,19 @@ nemo_status_t nemo_b200_cycle(nemo_simulation_t sim, uint64_t* cycle);
 nemo_status_t nemo_b200_synchronize(nemo_simulation_t sim);
 
 /* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`
- * cycles as one CUDA graph, then applyStdp(reward) when apply_stdp != 0),
+ * cycles in one persistent launch, then applyStdp(reward) when apply_stdp != 0),
  * bracketed by CUDA events on the simulation's stream. out[0] = device ms,
  * out[1] = neurons fired, out[2] = synaptic events generated (fired x
  * out-degree), out[3] = synapses delivered. */
 nemo_status_t nemo_b200_timed_steps(nemo_simulation_t sim, unsigned steps, unsigned cycles_per_step,
 		int apply_stdp, float reward, double out[4]);
 
-/* Per-kernel device times over `cycles` individually launched cycles, then
- * one applyStdp(reward) when STDP is on. out[0..2] = gather / neuron update
- * (with scatter) / STDP accumulation ms, out[3] = synapses delivered,
- * out[4] = neurons fired, out[5] = STDP synapse visits, out[6] = neuron
- * updates, out[7] = applyStdp ms, out[8] = plastic synapses, out[9] =
- * synaptic events generated. */
+/* Device times of one persistent launch of `cycles` cycles and of one
+ * applyStdp(reward) (when STDP is on), with the work they did (the cycles are
+ * simulated). out[0] = step-kernel ms, out[1] = its grid blocks, out[2] = 0,
+ * out[3] = synapses pushed, out[4] = neurons fired, out[5] = STDP synapse
+ * visits, out[6] = neuron updates, out[7] = applyStdp ms, out[8] = plastic
+ * synapses, out[9] = synaptic events generated. */
 nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[10]);
 
 /* Phase timing of the step kernel over `cycles` cycles (one traced launch;

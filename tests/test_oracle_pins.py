@@ -5,7 +5,10 @@
    oracle/_ref/lib<Model>.so by oracle/Makefile, on the same seeded inputs for
    many cycles; all outputs must agree bit for bit. Both link the same
    urand/nrand restatement (the reference RNG.cpp needs Boost).
-2. The fixed-point and RNG-seeding restatements against values derived from
+2. The same runs against tests/golden/plugins.npz, which
+   tests/golden/make_golden.py wrote from those compiled reference plugins, so
+   the pin holds where the reference sources are absent.
+3. The fixed-point and RNG-seeding restatements against values derived from
    their published definitions.
 """
 
@@ -15,80 +18,16 @@ import os
 import numpy as np
 import pytest
 
-from conftest import ORACLE_REF_DIR, ensure_oracle
+from conftest import ORACLE_REF_DIR, ROOT, ensure_oracle
+from plugin_harness import MODELS, PIN_N, UPDATE_T, _Run, drive_inputs, pin_cycles, run_digest
 
-UPDATE_T = ctypes.CFUNCTYPE(None, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
-                            ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t,
-                            ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p,
-                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
-
-# (model, nParam, nState, parameter sampler, state sampler, current scale)
-MODELS = {
-    "Izhikevich": (5, 2),
-    "IF_curr_exp": (9, 4),
-    "QIF": (1, 1),
-    "HH": (0, 5),
-    "PoissonSource": (1, 0),
-    "Input": (0, 0),
-}
+GOLDEN = os.path.join(ROOT, "tests", "golden", "plugins.npz")
 
 
-def _inputs(model, n, rng):
-    f32 = np.float32
-    if model == "Izhikevich":
-        r = rng.random(n, dtype=f32)
-        b = (f32(0.2) + f32(0.05) * r).astype(f32)
-        param = np.stack([np.full(n, 0.02, f32), b, (f32(-65) + f32(15) * r * r).astype(f32),
-                          np.full(n, 8.0, f32), (rng.random(n, dtype=f32) * f32(6)).astype(f32)])
-        param[4, ::5] = 0.0
-        v = np.full(n, -65.0, f32)
-        state = np.stack([(b * v).astype(f32), v])
-        scale = 10.0
-    elif model == "IF_curr_exp":
-        vals = [-65.0, -65.0, 1.0, 20.0, 2.0, 5.0, 5.0, -50.0, 0.5]
-        param = np.stack([np.full(n, x, f32) for x in vals])
-        state = np.stack([np.full(n, -65.0, f32), np.zeros(n, f32), np.zeros(n, f32), np.full(n, 3.0, f32)])
-        scale = 5.0
-    elif model == "QIF":
-        param = np.full((1, n), 0.04, f32)
-        state = rng.random((1, n), dtype=f32)
-        scale = 20.0
-    elif model == "HH":
-        param = np.zeros((0, n), f32)
-        vals = [-65.0, 0.3177, 0.0529, 0.5961, 0.0]
-        state = np.stack([np.full(n, x, f32) for x in vals])
-        state[0] += rng.normal(0, 3, n).astype(f32)
-        scale = 0.5
-    elif model == "PoissonSource":
-        param = (rng.random((1, n), dtype=f32) * f32(0.1)).astype(f32)
-        state = np.zeros((0, n), f32)
-        scale = 0.0
-    else:
-        param = np.zeros((0, n), f32)
-        state = np.zeros((0, n), f32)
-        scale = 0.0
-    return np.ascontiguousarray(param), np.ascontiguousarray(state), scale
-
-
-class _Run:
-    def __init__(self, fn, model, n, seed):
-        rng = np.random.default_rng(seed)
-        self.fn = fn
-        self.n = n
-        self.param, self.state, self.scale = _inputs(model, n, rng)
-        self.rng = np.ascontiguousarray(rng.integers(1, 2**31, size=(n, 4), dtype=np.uint32))
-        self.rf = np.zeros(n, np.uint64)
-        self.fired = np.zeros(n, np.uint32)
-        self.fstim = np.zeros(n, np.uint32)
-
-    def step(self, cycle, E, I, ext, fstim):
-        self.fstim[:] = fstim
-        ext = ext.copy()
-        p = lambda a: a.ctypes.data if a.size else None
-        self.fn(0, self.n, cycle, p(self.param), self.n, p(self.state), self.state.size, self.n,
-                20, p(self.fstim), p(self.rng), p(E), p(I), p(ext), p(self.rf), p(self.fired), None)
-        return self.fired.copy(), ext
+def _oracle_update(model):
+    oracle = ctypes.CDLL(ensure_oracle())
+    oracle.oracle_model_update.restype = ctypes.c_void_p
+    return UPDATE_T(oracle.oracle_model_update(model.encode()))
 
 
 @pytest.mark.parametrize("model", list(MODELS))
@@ -97,19 +36,13 @@ def test_restated_update_matches_reference_plugin(model):
     if not os.path.exists(lib_path):
         pytest.skip("reference plugin sources were not available when oracle/_ref was built")
     ref = UPDATE_T(("cpu_update_neurons", ctypes.CDLL(lib_path)))
-    oracle = ctypes.CDLL(ensure_oracle())
-    oracle.oracle_model_update.restype = ctypes.c_void_p
-    mine = UPDATE_T(oracle.oracle_model_update(model.encode()))
+    mine = _oracle_update(model)
 
-    n = 257
-    cycles = 40 if model == "HH" else 300
+    n = PIN_N
     a, b = _Run(ref, model, n, 7), _Run(mine, model, n, 7)
-    drv = np.random.default_rng(11)
-    for cycle in range(cycles):
-        E = np.ascontiguousarray((drv.random(n, dtype=np.float32) * np.float32(a.scale)).astype(np.float32))
-        I = np.ascontiguousarray((-drv.random(n, dtype=np.float32) * np.float32(a.scale) * np.float32(0.5)).astype(np.float32))
-        ext = np.ascontiguousarray(np.where(drv.random(n) < 0.1, np.float32(1.5), np.float32(0)).astype(np.float32))
-        fstim = (drv.random(n) < 0.02).astype(np.uint32)
+    inputs = drive_inputs(n, a.scale)
+    for cycle in range(pin_cycles(model)):
+        E, I, ext, fstim = next(inputs)
         fa, ea = a.step(cycle, E, I, ext, fstim)
         fb, eb = b.step(cycle, E, I, ext, fstim)
         assert np.array_equal(fa, fb), "cycle %d fired" % cycle
@@ -119,6 +52,19 @@ def test_restated_update_matches_reference_plugin(model):
         assert np.array_equal(a.rng, b.rng)
     if model in ("Izhikevich", "QIF", "PoissonSource"):
         assert a.rf.any(), "the pin should exercise firing"
+
+
+@pytest.mark.parametrize("model", list(MODELS))
+def test_restated_update_matches_golden_vectors(model):
+    """The oracle against the reference plugins' recorded outputs."""
+    g = np.load(GOLDEN)
+    fired, crcs, state, rf, rng = run_digest(_oracle_update(model), model)
+    assert np.array_equal(fired, g[model + "/fired"])
+    bad = np.nonzero(crcs != g[model + "/crc"])[0]
+    assert bad.size == 0, "first differing cycle %d" % (bad[0] if bad.size else -1)
+    assert np.array_equal(state.view(np.uint32), g[model + "/state"].view(np.uint32))
+    assert np.array_equal(rf, g[model + "/rf"])
+    assert np.array_equal(rng, g[model + "/rng"])
 
 
 def test_rng_seeds_follow_mt19937():
