@@ -36,6 +36,41 @@ nemo_status_t nemo_b200_cycle(nemo_simulation_t sim, uint64_t* cycle);
 /* Wait for all device work of the simulation. */
 nemo_status_t nemo_b200_synchronize(nemo_simulation_t sim);
 
+/* One simulation cycle like nemo_step, for callers that must not allocate
+ * memory while the simulation runs. No counterpart in the reference C ABI.
+ *
+ * nemo_step grows a device and a pinned host staging buffer with cudaMalloc /
+ * cudaMallocHost whenever a call brings more stimulus than any call before,
+ * and returns the fired list in memory the simulation owns and resizes. A
+ * device allocation synchronises the whole device and fails once the device
+ * memory is fully committed; a closed-loop controller with a hard per-cycle
+ * budget, or a host program whose device memory is owned by another
+ * allocator, cannot accept either. This call allocates nothing, on the host or
+ * the device, when it succeeds:
+ *   - the stimulus is staged through one module-static device array per
+ *     device (192 KB), so at most 16384 firing-stimulus entries and 16384
+ *     current-stimulus entries are accepted per call; more is rejected with
+ *     NEMO_INVALID_INPUT before anything runs;
+ *   - the fired neurons (user indices, ascending simulation order, as
+ *     nemo_step) are written to the caller's `fired` array, which must hold
+ *     at least the network's neuron count (`fired_capacity`), else
+ *     NEMO_INVALID_INPUT before anything runs; their number goes to
+ *     *fired_count.
+ * The simulation's device must be the calling thread's current device. The
+ * first call on a device looks up the scratch address (cudaGetSymbolAddress)
+ * and keeps it, so make one call before any latency-critical loop. Nothing in
+ * the scratch has to start at zero: each call writes the entries it reads.
+ * The scratch is shared by every simulation on the device, so calls for
+ * simulations on the same device must not overlap in time (from several host
+ * threads); calls that overlap race on the scratch. Stimulus and results are
+ * otherwise identical to nemo_step's, including repeated current-stimulus
+ * indices (the last entry wins) and invalid indices (the entries before the
+ * invalid one are applied, then NEMO_INVALID_INPUT). */
+nemo_status_t nemo_b200_step_noalloc(nemo_simulation_t sim,
+		const unsigned fstim_nidx[], size_t fstim_count,
+		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
+		unsigned fired[], size_t fired_capacity, size_t* fired_count);
+
 /* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`
  * cycles in one persistent launch, then applyStdp(reward) when apply_stdp != 0),
  * bracketed by CUDA events on the simulation's stream. out[0] = device ms,

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "kernels.hpp"
 #include "libm_match.cuh"
@@ -597,6 +598,35 @@ k_stimulus(NetDev net, StimDev s)
 	}
 }
 
+/* Stimulus of the allocation-free step, read from the per-device scratch
+ * below: [0, nf) firing-stimulus device indices, [NOALLOC_STIM_MAX,
+ * +ni) current-stimulus device indices, [2 NOALLOC_STIM_MAX, +ni) their
+ * currents (float bits). One warp walks the current stimulus in order, 32
+ * entries at a time; of equal indices within a group the highest lane writes,
+ * and __syncwarp orders the groups, so the last entry for a neuron wins as in
+ * the reference (cpu/Simulation.cpp:140-163). */
+__global__ void
+k_stimulus_scratch(NetDev net, const uint32_t* scratch, uint32_t nf, uint32_t ni)
+{
+	const uint32_t lane = threadIdx.x;
+	for(uint32_t i = lane; i < nf; i += 32) {
+		uint32_t n = scratch[i];
+		atomicOr(&net.fstim[n >> 5], 1u << (n & 31u));
+	}
+	const uint32_t* idx = scratch + NOALLOC_STIM_MAX;
+	const float* cur = reinterpret_cast<const float*>(scratch + 2 * NOALLOC_STIM_MAX);
+	for(uint32_t base = 0; base < ni; base += 32) {
+		const uint32_t i = base + lane;
+		const bool valid = i < ni;
+		const uint32_t n = valid ? idx[i] : 0xffffffffu;
+		const uint32_t same = __match_any_sync(FULL, n);
+		if(valid && 31u - uint32_t(__clz(same)) == lane) {
+			net.ext[n] = cur[i];
+		}
+		__syncwarp();
+	}
+}
+
 /* applyStdp (src/nemo/ConnectivityMatrix.cpp:272-325): every plastic synapse
  * gets w = clamp(w + (reward * acc) >> f) and its accumulator cleared.
  *
@@ -687,6 +717,35 @@ int g_blocksPerSm = 0;
 
 } // namespace
 
+/* Scratch of the allocation-free step (one copy per device, module-static so
+ * that no call allocates): 3 x NOALLOC_STIM_MAX words = 192 KB. Nothing in it
+ * has to start at zero: every call writes the entries it then reads. */
+static __device__ __align__(256) uint32_t g_noallocStim[3 * NOALLOC_STIM_MAX];
+
+namespace {
+std::mutex g_noallocMutex;
+uint32_t* g_noallocPtr[NOALLOC_MAX_DEVICES] = {};
+}
+
+int
+noallocScratch(int device, uint32_t** ptr)
+{
+	if(device < 0 || device >= NOALLOC_MAX_DEVICES) {
+		return int(cudaErrorInvalidDevice);
+	}
+	std::lock_guard<std::mutex> lock(g_noallocMutex);
+	if(g_noallocPtr[device] == nullptr) {
+		void* p = nullptr;
+		cudaError_t e = cudaGetSymbolAddress(&p, g_noallocStim);
+		if(e != cudaSuccess) {
+			return int(e);
+		}
+		g_noallocPtr[device] = static_cast<uint32_t*>(p);
+	}
+	*ptr = g_noallocPtr[device];
+	return int(cudaSuccess);
+}
+
 int
 smCount()
 {
@@ -707,6 +766,13 @@ launchStimulus(const NetDev& net, const StimDev& stim, void* stream)
 	uint32_t n = stim.nf > stim.ni ? stim.nf : stim.ni;
 	if(n == 0) return;
 	k_stimulus<<<(n + 255) / 256, 256, 0, S(stream)>>>(net, stim);
+}
+
+void
+launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, uint32_t ni, void* stream)
+{
+	if(nf + ni == 0) return;
+	k_stimulus_scratch<<<1, 32, 0, S(stream)>>>(net, scratch, nf, ni);
 }
 
 /* Co-resident grid for the cooperative launch: as many 1024-thread blocks per

@@ -138,8 +138,21 @@ struct StimDev {
 	uint32_t ni;
 };
 
+/* Allocation-free step: at most this many firing-stimulus and this many
+ * current-stimulus entries per call, staged in a module-static scratch array
+ * (one per device, shared by all simulations on it). */
+const uint32_t NOALLOC_STIM_MAX = 16384;
+const int NOALLOC_MAX_DEVICES = 64;
+
+/* Device address of the allocation-free scratch on `device`, which must be
+ * the current device. Looked up with cudaGetSymbolAddress on the first call
+ * per device, then cached. Returns a cudaError_t value. */
+int noallocScratch(int device, uint32_t** ptr);
+
 /* Launchers (kernels.cu), all on `stream`. */
 void launchStimulus(const NetDev& net, const StimDev& stim, void* stream);
+/* Stimulus from the allocation-free scratch (layout in kernels.cu). */
+void launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, uint32_t ni, void* stream);
 /* Cooperative launch of k_cycles over `blocks` blocks (from cyclesGrid). */
 void launchCycles(const CycleArgs& args, unsigned blocks, void* stream);
 /* The co-resident grid (one block per SM) and the per-block list capacity

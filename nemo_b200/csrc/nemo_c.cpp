@@ -309,6 +309,18 @@ nemo_status_t nemo_b200_cycle(nemo_simulation_t s, uint64_t* cycle) { RETURN_CAL
 nemo_status_t nemo_b200_synchronize(nemo_simulation_t s) { RETURN_CALL(s->sim.synchronize()); }
 
 nemo_status_t
+nemo_b200_step_noalloc(nemo_simulation_t s, const unsigned fstim_nidx[], size_t fstim_count,
+		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
+		unsigned fired[], size_t fired_capacity, size_t* fired_count)
+{
+	RETURN_CALL({
+		size_t n = s->sim.stepNoAlloc(fstim_nidx, fstim_count, istim_nidx, istim_current, istim_count,
+				fired, fired_capacity);
+		if(fired_count != NULL) *fired_count = n;
+	});
+}
+
+nemo_status_t
 nemo_b200_nrand_probe(nemo_simulation_t s, const uint32_t u1[], const uint32_t u2[], float out[], size_t n)
 {
 	RETURN_CALL(s->sim.nrandProbe(u1, u2, out, n));

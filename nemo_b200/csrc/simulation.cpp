@@ -567,6 +567,99 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	return m_fired;
 }
 
+/* step() without allocation. Indices are mapped on the host into a small
+ * stack buffer and copied chunk by chunk into the module-static scratch
+ * (a pageable-source cudaMemcpyAsync returns once the source has been
+ * staged, so the buffer can be reused at once); duplicates of the current
+ * stimulus are resolved on the device in call order. An invalid index raises
+ * after the entries before it have been applied, as step() does. */
+size_t
+Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+		unsigned* firedOut, size_t firedCapacity)
+{
+	if(nf > NOALLOC_STIM_MAX || ni > NOALLOC_STIM_MAX) {
+		fail(NEMO_INVALID_INPUT, "nemo_b200_step_noalloc: at most " + std::to_string(NOALLOC_STIM_MAX)
+				+ " firing-stimulus and " + std::to_string(NOALLOC_STIM_MAX)
+				+ " current-stimulus entries per call (got " + std::to_string(nf) + " and "
+				+ std::to_string(ni) + ")");
+	}
+	if(firedOut == nullptr || firedCapacity < m_nNeurons) {
+		fail(NEMO_INVALID_INPUT, "nemo_b200_step_noalloc: the fired array must hold the network's "
+				+ std::to_string(m_nNeurons) + " neurons");
+	}
+	if(m_noallocDevice < 0) {
+		cudaPointerAttributes attr;
+		NEMO_CUDA(cudaPointerGetAttributes(&attr, m_net.rf));
+		m_noallocDevice = attr.device;
+	}
+	int current = -1;
+	NEMO_CUDA(cudaGetDevice(&current));
+	if(current != m_noallocDevice) {
+		fail(NEMO_INVALID_INPUT, "nemo_b200_step_noalloc: device " + std::to_string(m_noallocDevice)
+				+ " of the simulation must be the current device (current: " + std::to_string(current) + ")");
+	}
+	uint32_t* scratch = nullptr;
+	NEMO_CUDA(noallocScratch(m_noallocDevice, &scratch));
+
+	cudaStream_t stream = STREAM(m_stream);
+	const size_t CHUNK = 1024;
+	uint32_t stage[CHUNK];
+	int err = 0;
+	unsigned badIdx = 0;
+	uint32_t nfOk = 0, niOk = 0;
+	for(size_t k0 = 0; k0 < nf && !err; k0 += CHUNK) {
+		size_t cnt = 0;
+		for(size_t k = k0; k < nf && k < k0 + CHUNK; ++k) {
+			auto it = m_g2d.find(fstim[k]);
+			if(it == m_g2d.end()) { err = 1; badIdx = fstim[k]; break; }
+			stage[cnt++] = it->second;
+		}
+		if(cnt) NEMO_CUDA(cudaMemcpyAsync(scratch + nfOk, stage, cnt * 4, cudaMemcpyHostToDevice, stream));
+		nfOk += uint32_t(cnt);
+	}
+	for(size_t k0 = 0; k0 < ni && !err; k0 += CHUNK) {
+		size_t cnt = 0;
+		for(size_t k = k0; k < ni && k < k0 + CHUNK; ++k) {
+			auto it = m_g2d.find(inidx[k]);
+			if(it == m_g2d.end()) { err = 1; badIdx = inidx[k]; break; }
+			stage[cnt++] = it->second;
+		}
+		if(cnt) {
+			NEMO_CUDA(cudaMemcpyAsync(scratch + NOALLOC_STIM_MAX + niOk, stage, cnt * 4,
+						cudaMemcpyHostToDevice, stream));
+			NEMO_CUDA(cudaMemcpyAsync(scratch + 2 * NOALLOC_STIM_MAX + niOk, icur + k0, cnt * 4,
+						cudaMemcpyHostToDevice, stream));
+		}
+		niOk += uint32_t(cnt);
+	}
+	launchStimulusScratch(m_net, scratch, nfOk, niOk, m_stream);
+	if(err) {
+		NEMO_CUDA(cudaStreamSynchronize(stream));
+		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
+	}
+
+	launchBlock(m_cycle, 1);
+	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
+				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	NEMO_CUDA(cudaGetLastError());
+	checkDeviceError();
+	m_cycle++;
+	m_stateDirty = true;
+	size_t count = 0;
+	for(uint32_t w = 0; w < m_net.nWords; ++w) {
+		uint32_t bits = m_hWords[w];
+		while(bits) {
+			uint32_t b = uint32_t(__builtin_ctz(bits));
+			bits &= bits - 1;
+			firedOut[count++] = m_d2g[w * 32 + b];
+		}
+	}
+	return count;
+}
+
 void
 Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 {

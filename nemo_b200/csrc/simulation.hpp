@@ -26,6 +26,15 @@ public:
 	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
 			const unsigned* inidx, const float* icur, size_t ni);
 
+	/* The same cycle as step(), without allocating host or device memory:
+	 * stimulus staged through the module-static scratch (at most
+	 * NOALLOC_STIM_MAX entries of each kind), fired neurons written to the
+	 * caller's array, which must hold neuronCount() entries. The first call
+	 * on a device looks up the scratch address. Calls on the same device must
+	 * not overlap. */
+	size_t stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+			unsigned* firedOut, size_t firedCapacity);
+
 	/* Device-resident run of `cycles` cycles without stimulus in one
 	 * persistent launch; per-cycle fired counts and synaptic events (fired x
 	 * out-degree) are returned when the pointers are non-null. */
@@ -163,6 +172,8 @@ private:
 	size_t m_stimCap;
 
 	std::vector<unsigned> m_fired;
+
+	int m_noallocDevice = -1;  /* device of the simulation, found on the first stepNoAlloc */
 };
 
 } // namespace nemo_b200
