@@ -153,6 +153,14 @@ class ClockSampler:
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait for its first sample so
+        # that the samples cover the region that follows
+        deadline = time.time() + 5.0
+        while time.time() < deadline and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
