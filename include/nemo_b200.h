@@ -15,9 +15,9 @@ extern "C" {
 #endif
 
 /* Run `cycles` cycles (<= 1024 per call) without stimulus, entirely on the
- * device in one persistent launch of the step kernel (neuron update, spike
- * push and STDP accumulation per cycle, one grid barrier per cycle). Equivalent to `cycles` calls of nemo_step with
- * empty stimulus. fired_counts[k] / events[k] (each may be NULL) receive the
+ * device in one persistent launch of the step kernel (spike gather, neuron
+ * update and STDP accumulation per cycle, one grid barrier per cycle).
+ * Equivalent to `cycles` calls of nemo_step with empty stimulus. fired_counts[k] / events[k] (each may be NULL) receive the
  * number of neurons fired in cycle k and the synaptic events those firings
  * generate (fired neurons x out-degree, the throughput unit of the
  * reference benchmark, src/examples/common.cpp:93-98). */
@@ -89,11 +89,13 @@ nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float re
 
 /* Phase timing of the step kernel over `cycles` cycles (one traced launch;
  * the cycles are simulated). Means over cycles, in ns: out[0] whole phase,
- * out[1] / out[2] slowest / mean block neuron update, out[3] / out[4]
- * slowest / mean block spike push + STDP, out[5] phase start to the last
- * block's arrival at the grid barrier, out[6] last arrival to barrier exit,
- * out[7] spread of the blocks' arrivals. */
-nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[8]);
+ * out[1] / out[2] slowest / mean block urgent (delay-1) spike gather,
+ * out[3] / out[4] slowest / mean block neuron update, out[5] phase start to
+ * the last block's arrival at the grid barrier, out[6] last arrival to
+ * barrier exit, out[7] spread of the blocks' arrivals, out[8] / out[9]
+ * slowest / mean block update together with the overlapped deferred gather
+ * and STDP accumulation. */
+nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[10]);
 
 /* Diagnostics: the device noise transform of two RNG words per sample,
  * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the

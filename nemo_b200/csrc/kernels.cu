@@ -136,26 +136,34 @@ __device__ __forceinline__ uint32_t takeStimWord(const NetDev& net, uint32_t n, 
 
 /* ---------------- neuron models (one neuron per thread) ---------------- */
 
+/* The models take the cycle's E and I currents from the caller (which drains
+ * the neuron's slot) and load every other operand before their first store,
+ * so that all loads of a neuron are in flight together. */
+
 /* Izhikevich (src/nemo/cpu/plugins/Izhikevich.cpp:53-97). Parameters a, b, c,
  * d, sigma; state u, v. The v update evaluates its bracket in double (double
  * literals in the reference), the u update in float. */
 __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		uint32_t slot, bool stim)
+		float E, float I, bool stim)
 {
 	const size_t c = g.count;
-	float E, I;
-	takeCurrents(net, slot, n, E, I);
-	float In = __fadd_rn(__fadd_rn(E, I), takeExternal(net, n));
-	float sigma = g.param[4 * c + i];
-	uint4 s = g.rng[i]; /* loaded with the other operands; used only with noise */
+	const float X = net.ext[n];
+	const float sigma = g.param[4 * c + i];
+	uint4 s = g.rng[i];
+	const float a = g.param[0 * c + i];
+	const float b = g.param[1 * c + i];
+	const float pc = g.param[2 * c + i];
+	const float pd = g.param[3 * c + i];
+	float u = g.state[0 * c + i];
+	float v = g.state[1 * c + i];
+	if(X != 0.0f) {
+		net.ext[n] = 0.0f;
+	}
+	float In = __fadd_rn(__fadd_rn(E, I), X);
 	if(sigma != 0.0f) {
 		In = __fadd_rn(In, __fmul_rn(sigma, nrand(s, net.sinTab, net.logTab)));
 		g.rng[i] = s;
 	}
-	float a = g.param[0 * c + i];
-	float b = g.param[1 * c + i];
-	float u = g.state[0 * c + i];
-	float v = g.state[1 * c + i];
 	bool fired = false;
 	for(int k = 0; k < 4; ++k) {
 		if(!fired) {
@@ -169,8 +177,8 @@ __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDe
 	}
 	fired = fired || stim;
 	if(fired) {
-		v = g.param[2 * c + i];
-		u = __fadd_rn(u, g.param[3 * c + i]);
+		v = pc;
+		u = __fadd_rn(u, pd);
 	}
 	g.state[0 * c + i] = u;
 	g.state[1 * c + i] = v;
@@ -180,28 +188,31 @@ __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDe
 /* IF_curr_exp (src/nemo/cpu/plugins/IF_curr_exp.cpp:74-121). Parameters in
  * IF_curr_exp.h order; state v, ie, ii, lastfire. Fires on v > v_thresh. */
 __device__ __forceinline__ bool modelIfCurrExp(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		uint32_t slot, bool stim)
+		float E, float I, bool stim)
 {
 	const size_t c = g.count;
 	const float* P = g.param;
 	float* S = g.state;
-	float E, I;
-	takeCurrents(net, slot, n, E, I);
-	float v_rest = P[0 * c + i], v_reset = P[1 * c + i], c_m = P[2 * c + i], tau_m = P[3 * c + i];
-	float tau_refrac = P[4 * c + i], tau_e = P[5 * c + i], tau_i = P[6 * c + i];
-	float v_thresh = P[7 * c + i], i_offset = P[8 * c + i];
-	float ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_e)), S[1 * c + i]), E);
-	float ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_i)), S[2 * c + i]), I);
-	float In = __fadd_rn(__fadd_rn(__fadd_rn(ie, ii), takeExternal(net, n)), i_offset);
+	const float X = net.ext[n];
+	const float v_rest = P[0 * c + i], v_reset = P[1 * c + i], c_m = P[2 * c + i], tau_m = P[3 * c + i];
+	const float tau_refrac = P[4 * c + i], tau_e = P[5 * c + i], tau_i = P[6 * c + i];
+	const float v_thresh = P[7 * c + i], i_offset = P[8 * c + i];
+	const float ie0 = S[1 * c + i], ii0 = S[2 * c + i];
+	float v = S[0 * c + i];
+	const float lastfire = S[3 * c + i];
+	if(X != 0.0f) {
+		net.ext[n] = 0.0f;
+	}
+	const float ie = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_e)), ie0), E);
+	const float ii = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, __fdiv_rn(1.0f, tau_i)), ii0), I);
+	const float In = __fadd_rn(__fadd_rn(__fadd_rn(ie, ii), X), i_offset);
 	S[1 * c + i] = ie;
 	S[2 * c + i] = ii;
-	float v = S[0 * c + i];
-	float lastfire = S[3 * c + i];
-	bool refractory = lastfire <= tau_refrac;
+	const bool refractory = lastfire <= tau_refrac;
 	if(!refractory) {
 		v = __fadd_rn(v, __fadd_rn(__fdiv_rn(In, c_m), __fdiv_rn(__fsub_rn(v_rest, v), tau_m)));
 	}
-	bool fired = (!refractory && v > v_thresh) || stim;
+	const bool fired = (!refractory && v > v_thresh) || stim;
 	if(fired) {
 		S[3 * c + i] = 1.0f;
 		S[0 * c + i] = v_reset;
@@ -215,17 +226,18 @@ __device__ __forceinline__ bool modelIfCurrExp(const NetDev& net, const GroupDev
 /* QIF (src/nemo/cpu/plugins/QIF.cpp:45-106): 10 RK4 substeps of 0.1 ms,
  * threshold 1, reset 0. */
 __device__ __forceinline__ bool modelQif(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		uint32_t slot, bool stim)
+		float E, float I, bool stim)
 {
 	const float dt = 0.1f;
 	const float a1 = __fmul_rn(0.5f, dt);
 	const float a2 = dt;
 	const float bb1 = __fdiv_rn(dt, 6.0f);
-	float E, I;
-	takeCurrents(net, slot, n, E, I);
-	float X = takeExternal(net, n);
+	const float X = net.ext[n];
 	float v = g.state[i];
-	float a = g.param[i];
+	const float a = g.param[i];
+	if(X != 0.0f) {
+		net.ext[n] = 0.0f;
+	}
 	bool fired = false;
 	for(int k = 0; k < 10; ++k) {
 		if(!fired) {
@@ -250,13 +262,12 @@ __device__ __forceinline__ bool modelQif(const NetDev& net, const GroupDev& g, u
 	return fired;
 }
 
-/* PoissonSource (src/nemo/cpu/plugins/PoissonSource.cpp:21-29). Currents are
- * cleared (every neuron's slot must be) but unused. */
+/* PoissonSource (src/nemo/cpu/plugins/PoissonSource.cpp:21-29). The
+ * currents (drained by the caller, as every neuron's slot must be) and the
+ * external current (cleared) are unused. */
 __device__ __forceinline__ bool modelPoisson(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		uint32_t slot, bool stim)
+		float, float, bool stim)
 {
-	float E, I;
-	takeCurrents(net, slot, n, E, I);
 	(void) takeExternal(net, n);
 	uint32_t p0 = uint32_t(__fmul_rn(g.param[i], 65536.0f));
 	uint4 s = g.rng[i];
@@ -266,11 +277,9 @@ __device__ __forceinline__ bool modelPoisson(const NetDev& net, const GroupDev& 
 }
 
 /* Input (src/nemo/cpu/plugins/Input.cpp:56-60) */
-__device__ __forceinline__ bool modelInput(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		uint32_t slot, bool stim)
+__device__ __forceinline__ bool modelInput(const NetDev& net, const GroupDev&, uint32_t, uint32_t n,
+		float, float, bool stim)
 {
-	float E, I;
-	takeCurrents(net, slot, n, E, I);
 	(void) takeExternal(net, n);
 	return stim;
 }
@@ -351,18 +360,68 @@ __device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeo
 
 /* ---------------- the persistent step kernel ---------------- */
 
-/* Work lists of a block, in global memory (per-block regions of listCap
- * entries of {neuron, first synapse, synapse count}):
- *   fired[listCap]   sources fired by this block's neurons in this cycle,
- *   post[2][listCap] this block's post-spiking targets of the last two cycles.
- * Push and STDP work is split into 128-synapse items, one per warp, four
- * independent synapses per lane. */
+/* Exclusive prefix of cnt[0, n) into pre[0, n], by one warp */
+__device__ __forceinline__ void warpPrefix(const uint32_t* cnt, uint32_t n, uint32_t* pre, uint32_t lane)
+{
+	const uint32_t per = (n + 31u) / 32u;
+	const uint32_t lo = min(n, lane * per), hi = min(n, lo + per);
+	uint32_t sum = 0;
+	for(uint32_t i = lo; i < hi; ++i) sum += cnt[i];
+	uint32_t incl = sum;
+#pragma unroll
+	for(int d = 1; d < 32; d <<= 1) {
+		uint32_t x = __shfl_up_sync(FULL, incl, d);
+		if(lane >= uint32_t(d)) incl += x;
+	}
+	uint32_t run = incl - sum;
+	for(uint32_t i = lo; i < hi; ++i) {
+		pre[i] = run;
+		run += cnt[i];
+	}
+	if(lane == 31) pre[n] = incl;
+}
+
+/* The list (block) holding entry j of a concatenation with prefix pre[0, n]:
+ * the last b with pre[b] <= j (j < pre[n]) */
+__device__ __forceinline__ uint32_t findList(const uint32_t* pre, uint32_t n, uint32_t j)
+{
+	uint32_t lo = 0, hi = n;
+	while(hi - lo > 1) {
+		uint32_t mid = (lo + hi) >> 1;
+		if(pre[mid] <= j) lo = mid;
+		else hi = mid;
+	}
+	return lo;
+}
+
+/* Add one forward-matrix record into current slot `slot` of its target
+ * (E for w >= 0, else I), in shared memory or in net.acc */
+template<bool SMEM>
+__device__ __forceinline__ void gatherAdd(const NetDev& net, int2* sAcc, uint32_t ownN, uint32_t ownBase, uint32_t slot,
+		uint2 r)
+{
+	const int32_t w = int32_t(r.y);
+	const uint32_t target = r.x >> 6;
+	if(SMEM) {
+		int* cell = reinterpret_cast<int*>(&sAcc[slot * ownN + (target - ownBase)]);
+		atomicAdd(cell + (w < 0 ? 1 : 0), w);
+	} else {
+		addCurrent(net, slot, target, w < 0 ? 1 : 0, w);
+	}
+}
+
+/* k_cycles: see kernels.hpp for the phase structure. SMEM: the owned current
+ * slots live in dynamic shared memory as int32 E/I pairs,
+ * sAcc[slot * ownN + local]; otherwise every access goes to net.acc. */
+template<bool SMEM>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_cycles(const __grid_constant__ CycleArgs A)
 {
-	__shared__ uint32_t sNFired;
-	__shared__ uint32_t sNPost[2];
-	__shared__ unsigned long long sEvents;
+	extern __shared__ int2 sAcc[];
+	__shared__ uint32_t sPreF[MAX_BLOCKS + 1];
+	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
+	__shared__ uint32_t sNFired, sNPost, sWork;
+	__shared__ unsigned long long sEvents, sPushed, sVisits;
 
 	const NetDev& net = A.net;
 	const uint32_t tid = threadIdx.x;
@@ -370,67 +429,119 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t warp = tid >> 5;
 	const uint32_t lt = (1u << lane) - 1u;
 	const uint32_t warpsPerBlock = blockDim.x >> 5;
-	const uint32_t gridWarps = gridDim.x * warpsPerBlock;
-	/* 32-neuron warps are dealt to blocks round-robin, so that every block
-	 * updates (and then pushes and learns for) a similar share */
-	const uint32_t myWarp = warp * gridDim.x + blockIdx.x;
-	const uint32_t totalWarps = A.groupWarp[A.ngroups];
+	const uint32_t B = gridDim.x;
+	const uint32_t b = blockIdx.x;
 	const size_t nDev = net.nDev;
-	const uint32_t cap = A.listCap;
-	uint32_t* firedList = net.lists + size_t(blockIdx.x) * cap * 9u;
-	uint32_t* postLists = firedList + size_t(cap) * 3u;
+	const uint32_t ownN = net.ownWarps * 32u;
+	const uint32_t ownBase = b * ownN;
+	const uint32_t totalWarps = A.groupWarp[A.ngroups];
+	const uint32_t firstWarp = b * net.ownWarps;
+	const uint32_t myWarps = firstWarp < totalWarps ? min(net.ownWarps, totalWarps - firstWarp) : 0u;
+	const size_t listStride = size_t(B) * ownN;  /* one parity of the lists */
+	int2* acc32 = reinterpret_cast<int2*>(net.acc);
+	const uint2* region = net.fcm + net.regionBase[b];
 
-	if(tid == 0) {
-		sNPost[0] = 0;
-		sNPost[1] = 0;
+	if(SMEM) {
+		const uint32_t total = net.slots * ownN;
+		for(uint32_t x = tid; x < total; x += blockDim.x) {
+			const uint32_t s = x / ownN, l = x - s * ownN;
+			const size_t n = size_t(ownBase) + l;
+			sAcc[x] = n < nDev ? acc32[size_t(s) * nDev + n] : make_int2(0, 0);
+		}
 	}
 
 	for(uint32_t k = 0; k <= A.cycles; ++k) {
 		const uint64_t t64 = A.firstCycle + k;
 		const uint32_t t = uint32_t(t64);
-		const uint32_t slotT = uint32_t(t64 % net.slots);   /* current slot of cycle t */
 		const bool doUpdate = k < A.cycles;
-		const uint32_t pb = t & 1u;
+		const bool doPrev = k > 0;     /* gather and learn for cycle t-1 */
+		const uint32_t slotT = uint32_t(t64 % net.slots);
 
 		if(tid == 0) {
 			sNFired = 0;
+			sNPost = 0;
+			sWork = 0;
 			sEvents = 0;
-			if(doUpdate) {
-				sNPost[pb] = 0;
-				if(blockIdx.x == 0) {
-					net.firedCountRing[(t + 1) & net.ringMask] = 0;
-					net.eventsRing[(t + 1) & net.ringMask] = 0;
-				}
+			sPushed = 0;
+			sVisits = 0;
+			if(doUpdate && b == 0) {
+				net.firedCountRing[(t + 1) & net.ringMask] = 0;
+				net.eventsRing[(t + 1) & net.ringMask] = 0;
 			}
 		}
+		if(doPrev) {
+			const uint32_t par = (t - 1u) & 1u;
+			if(warp == 0) warpPrefix(net.firedCnt + par * B, B, sPreF, lane);
+			if(warp == 1 && net.stdp) warpPrefix(net.postCnt + par * B, B, sPreP, lane);
+		}
 		__syncthreads();
-		unsigned long long* trace = A.trace ? A.trace + (size_t(k) * gridDim.x + blockIdx.x) * 4u : nullptr;
+		unsigned long long* trace = A.trace ? A.trace + (size_t(k) * B + b) * 5u : nullptr;
 		if(trace && tid == 0) trace[0] = globalTimer();
 
-		/* ---- neuron update of cycle t ---- */
+		if(doPrev && net.deliver) {
+			/* ---- urgent gather of cycle t-1: the delay-1 synapses (a
+			 * prefix of every segment) feed the update of cycle t ---- */
+			const uint32_t F = sPreF[B];
+			const uint32_t* flist = net.firedList + ((t - 1u) & 1u) * listStride;
+			uint32_t pushed = 0;
+			for(uint32_t j = tid; j < F; j += blockDim.x) {
+				const uint32_t bb = findList(sPreF, B, j);
+				const uint32_t s = flist[size_t(bb) * ownN + (j - sPreF[bb])];
+				const uint32_t beg = net.segOff[size_t(s) * B + b];
+				const uint32_t end = net.segOff[size_t(s + 1u) * B + b];
+				for(uint32_t q = beg; q < end; ++q) {
+					const uint2 r = region[q];
+					if(r.x & 63u) break;
+					gatherAdd<SMEM>(net, sAcc, ownN, ownBase, slotT, r);
+					++pushed;
+				}
+			}
+			pushed = __reduce_add_sync(FULL, pushed);
+			if(lane == 0 && pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
+		}
+		__syncthreads();
+		if(trace && tid == 0) trace[1] = globalTimer();
+
+		/* ---- neuron update of cycle t for the owned neurons ---- */
 		if(doUpdate) {
-			const uint32_t slot = slotT;
+			const uint32_t par = t & 1u;
 			const uint64_t* rfIn = net.rf + (t & 1u) * nDev;
-			uint64_t* rfOut = net.rf + ((t + 1) & 1u) * nDev;
-			uint32_t* postOut = postLists + size_t(pb) * cap * 3u;
-			for(uint32_t gw = myWarp; gw < totalWarps; gw += gridWarps) {
+			uint64_t* rfOut = net.rf + ((t + 1u) & 1u) * nDev;
+			uint32_t* firedOut = net.firedList + par * listStride + size_t(b) * ownN;
+			uint2* postOut = net.postList + par * listStride + size_t(b) * ownN;
+			for(uint32_t lw = warp; lw < myWarps; lw += warpsPerBlock) {
+				const uint32_t dw = firstWarp + lw;
 				int gi = 0;
-				while(gw >= A.groupWarp[gi + 1]) ++gi;
+				while(dw >= A.groupWarp[gi + 1]) ++gi;
 				const GroupDev& G = A.groups[gi];
-				const uint32_t i = (gw - A.groupWarp[gi]) * 32u + lane;
-				const uint32_t n = G.devBase + i;
+				const uint32_t n = dw * 32u + lane;
+				const uint32_t i = n - G.devBase;
 				const bool valid = i < G.count;
 				const uint32_t stimWord = takeStimWord(net, n, lane);
-				uint64_t rfPrev = valid ? rfIn[n] : 0ull;
+				/* operands needed after the update, loaded with its own */
+				const uint64_t rfPrev = valid ? rfIn[n] : 0ull;
+				const uint32_t deg = valid ? net.outDegree[n] : 0u;
+				uint2 rcm = make_uint2(0u, 0u);
+				if(valid && net.stdp) rcm = make_uint2(net.rcmStart[n], net.rcmStart[n + 1]);
+				float E, I;
+				if(SMEM) {
+					int2* cell = &sAcc[slotT * ownN + lw * 32u + lane];
+					const int2 a = *cell;
+					*cell = make_int2(0, 0);
+					E = wfxToFloat(a.x, net.fbits);
+					I = wfxToFloat(a.y, net.fbits);
+				} else {
+					takeCurrents(net, slotT, n, E, I);
+				}
 				bool fired = false;
 				if(valid) {
 					const bool stim = (stimWord >> lane) & 1u;
 					switch(G.kind) {
-						case 0: fired = modelIzhikevich(net, G, i, n, slot, stim); break;
-						case 1: fired = modelIfCurrExp(net, G, i, n, slot, stim); break;
-						case 2: fired = modelQif(net, G, i, n, slot, stim); break;
-						case 4: fired = modelPoisson(net, G, i, n, slot, stim); break;
-						default: fired = modelInput(net, G, i, n, slot, stim); break;
+						case 0: fired = modelIzhikevich(net, G, i, n, E, I, stim); break;
+						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
+						case 2: fired = modelQif(net, G, i, n, E, I, stim); break;
+						case 4: fired = modelPoisson(net, G, i, n, E, I, stim); break;
+						default: fired = modelInput(net, G, i, n, E, I, stim); break;
 					}
 				}
 				const uint64_t rfNew = (rfPrev << 1) | uint64_t(fired);
@@ -439,23 +550,16 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				}
 				const uint32_t word = __ballot_sync(FULL, fired);
 				if(lane == 0) {
-					net.firedRing[size_t(t & net.ringMask) * net.nWords + (n >> 5)] = word;
+					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
 				}
 				if(word) {
 					uint32_t base = 0;
 					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
 					base = __shfl_sync(FULL, base, 0);
-					uint32_t deg = 0;
 					if(fired) {
-						uint64_t b = net.rowStart[size_t(n) * net.rowStride];
-						uint64_t e = net.rowStart[size_t(n + 1) * net.rowStride];
-						deg = uint32_t(e - b);
-						uint32_t* entry = firedList + size_t(base + __popc(word & lt)) * 3u;
-						entry[0] = n;
-						entry[1] = uint32_t(b);
-						entry[2] = deg;
+						firedOut[base + __popc(word & lt)] = n;
 					}
-					uint32_t ev = __reduce_add_sync(FULL, deg);
+					const uint32_t ev = __reduce_add_sync(FULL, fired ? deg : 0u);
 					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
 				}
 				if(net.stdp) {
@@ -464,121 +568,146 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t pm = __ballot_sync(FULL, post);
 					if(pm) {
 						uint32_t base = 0;
-						if(lane == 0) base = atomicAdd(&sNPost[pb], uint32_t(__popc(pm)));
+						if(lane == 0) base = atomicAdd(&sNPost, uint32_t(__popc(pm)));
 						base = __shfl_sync(FULL, base, 0);
 						if(post) {
-							uint64_t b = net.rcmStart[n];
-							uint64_t e = net.rcmStart[n + 1];
-							uint32_t* entry = postOut + size_t(base + __popc(pm & lt)) * 3u;
-							entry[0] = n;
-							entry[1] = uint32_t(b);
-							entry[2] = uint32_t(e - b);
+							postOut[base + __popc(pm & lt)] = make_uint2(rcm.x, rcm.y - rcm.x);
 						}
 					}
 				}
 			}
+			if(trace && lane == 0 && warp < myWarps) atomicMax(&trace[2], globalTimer());
 		}
-		/* ---- STDP accumulation of cycle t-1 (ConnectivityMatrix.cpp:224-258)
-		 * for this block's targets that fired P cycles before it; every
-		 * accumulator has a single writer. It only reads the history after
-		 * cycle t-1, so warps start on it as soon as their own update of
-		 * cycle t is done ---- */
-		if(net.stdp && k > 0) {
-			const uint32_t* postIn = postLists + size_t(pb ^ 1u) * cap * 3u;
+
+		/* ---- overlapped with the update: the deferred gather of cycle t-1
+		 * (delays >= 2, into slots of cycles > t) and the STDP accumulation
+		 * of cycle t-1, as units handed out by a block counter so that warps
+		 * without neurons to update start at once. Units [0, G): 32 fired
+		 * sources each; units [G, G + S): this block's share of the grid's
+		 * 128-synapse STDP items (item u * B + b) ---- */
+		if(doPrev) {
+			const uint32_t par = (t - 1u) & 1u;
+			const uint32_t F = net.deliver ? sPreF[B] : 0u;
+			const uint32_t G = (F + 31u) / 32u;
+			const uint32_t P = net.stdp ? sPreP[B] : 0u;
+			const uint32_t chunks = net.stdpChunks;
+			const uint32_t items = P * chunks;
+			const uint32_t Sb = items > b ? (items - b + B - 1u) / B : 0u;
+			const uint32_t* flist = net.firedList + par * listStride;
+			const uint2* plist = net.postList + par * listStride;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
-			const uint32_t items = sNPost[pb ^ 1u] * net.stdpChunks;
+			const uint32_t slotPrev = uint32_t((t64 - 1u) % net.slots);
+			uint32_t pushed = 0;
 			uint64_t visited = 0;
-			for(uint32_t it = warp; it < items; it += warpsPerBlock) {
-				const uint32_t* entry = postIn + size_t(it / net.stdpChunks) * 3u;
-				const uint32_t off = (it % net.stdpChunks) * 128u;
-				const uint32_t len = entry[2];
-				if(off >= len) continue;
-				const uint64_t b = uint64_t(entry[1]) + off;
-				const uint32_t cnt = len - off < 128u ? len - off : 128u;
-				visited += cnt;
-				uint32_t sd[4];
+			for(;;) {
+				uint32_t u = 0;
+				if(lane == 0) u = atomicAdd(&sWork, 1u);
+				u = __shfl_sync(FULL, u, 0);
+				if(u >= G + Sb) break;
+				if(u < G) {
+					const uint32_t j = u * 32u + lane;
+					if(j < F) {
+						const uint32_t bb = findList(sPreF, B, j);
+						const uint32_t s = flist[size_t(bb) * ownN + (j - sPreF[bb])];
+						const uint32_t beg = net.segOff[size_t(s) * B + b];
+						const uint32_t end = net.segOff[size_t(s + 1u) * B + b];
+						for(uint32_t q = beg; q < end; q += 4u) {
+							uint2 r[4];
 #pragma unroll
-				for(int u = 0; u < 4; ++u) {
-					uint32_t j = lane + 32u * u;
-					sd[u] = j < cnt ? net.rcmSrcDelay[b + j] : 0u;
-				}
-				uint64_t pre[4];
-				int32_t old[4];
+							for(int x = 0; x < 4; ++x) {
+								r[x] = q + x < end ? region[q + x] : make_uint2(0u, 0u);
+							}
 #pragma unroll
-				for(int u = 0; u < 4; ++u) {
-					uint32_t j = lane + 32u * u;
-					pre[u] = j < cnt ? shr64(rfAfter[sd[u] >> 6], (sd[u] & 63u) + 1u) : 0ull;
-					old[u] = j < cnt ? net.rcmAcc[b + j] : 0;
-				}
+							for(int x = 0; x < 4; ++x) {
+								/* delay 1 was added by the urgent gather */
+								if(q + x < end && (r[x].x & 63u)) {
+									uint32_t slot = slotPrev + (r[x].x & 63u) + 1u;
+									slot = slot >= net.slots ? slot - net.slots : slot;
+									gatherAdd<SMEM>(net, sAcc, ownN, ownBase, slot, r[x]);
+									++pushed;
+								}
+							}
+						}
+					}
+				} else {
+					/* STDP (ConnectivityMatrix.cpp:224-258): targets that
+					 * fired P cycles before cycle t-1; every accumulator has
+					 * one writer */
+					const uint32_t it = (u - G) * B + b;
+					const uint32_t tg = it / chunks;
+					const uint32_t off = (it - tg * chunks) * 128u;
+					const uint32_t bb = findList(sPreP, B, tg);
+					const uint2 range = plist[size_t(bb) * ownN + (tg - sPreP[bb])];
+					if(off < range.y) {
+						const uint32_t b0 = range.x + off;
+						const uint32_t cnt = range.y - off < 128u ? range.y - off : 128u;
+						visited += cnt;
+						uint32_t sd[4];
 #pragma unroll
-				for(int u = 0; u < 4; ++u) {
-					uint32_t j = lane + 32u * u;
-					if(j < cnt) {
-						int32_t dw = weightChange(pre[u], A.rule);
-						if(dw != 0) {
-							net.rcmAcc[b + j] = int32_t(uint32_t(old[u]) + uint32_t(dw));
+						for(int x = 0; x < 4; ++x) {
+							const uint32_t jj = lane + 32u * x;
+							sd[x] = jj < cnt ? net.rcmSrcDelay[b0 + jj] : 0u;
+						}
+						uint64_t pre[4];
+						int32_t old[4];
+#pragma unroll
+						for(int x = 0; x < 4; ++x) {
+							const uint32_t jj = lane + 32u * x;
+							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
+							old[x] = jj < cnt ? net.rcmAcc[b0 + jj] : 0;
+						}
+#pragma unroll
+						for(int x = 0; x < 4; ++x) {
+							const uint32_t jj = lane + 32u * x;
+							if(jj < cnt) {
+								const int32_t dw = weightChange(pre[x], A.rule);
+								if(dw != 0) {
+									net.rcmAcc[b0 + jj] = int32_t(uint32_t(old[x]) + uint32_t(dw));
+								}
+							}
 						}
 					}
 				}
 			}
-			if(lane == 0 && visited) {
-				atomicAdd(&net.stats[1], (unsigned long long) visited);
+			pushed = __reduce_add_sync(FULL, pushed);
+			if(lane == 0) {
+				if(pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
+				if(visited) atomicAdd(&sVisits, (unsigned long long) visited);
 			}
 		}
-
 		__syncthreads();
-		if(trace && tid == 0) trace[1] = globalTimer();
-
-		if(doUpdate) {
-			if(tid == 0 && sNFired) {
-				atomicAdd(&net.firedCountRing[t & net.ringMask], sNFired);
-				atomicAdd(&net.eventsRing[t & net.ringMask], sEvents);
-				atomicAdd(&net.stats[2], (unsigned long long) sNFired);
-				atomicAdd(&net.stats[3], sEvents);
-				if(net.deliver) atomicAdd(&net.stats[0], sEvents);
-			}
-
-			/* ---- spike push: the synapses of this block's fired sources go
-			 * into the current slots of cycles t + delay ---- */
-			if(net.deliver) {
-				const uint32_t items = sNFired * net.fireChunks;
-				for(uint32_t it = warp; it < items; it += warpsPerBlock) {
-					const uint32_t* entry = firedList + size_t(it / net.fireChunks) * 3u;
-					const uint32_t off = (it % net.fireChunks) * 128u;
-					const uint32_t len = entry[2];
-					if(off >= len) continue;
-					const uint64_t b = uint64_t(entry[1]) + off;
-					const uint32_t cnt = len - off < 128u ? len - off : 128u;
-					uint2 syn[4];
-#pragma unroll
-					for(int u = 0; u < 4; ++u) {
-						uint32_t j = lane + 32u * u;
-						syn[u] = j < cnt ? net.fcm[b + j] : make_uint2(0u, 0u);
-					}
-#pragma unroll
-					for(int u = 0; u < 4; ++u) {
-						if(lane + 32u * u < cnt) {
-							/* slot of cycle t + d, d <= maxDelay < slots */
-							uint32_t s = slotT + (syn[u].x & 63u) + 1u;
-							s = s >= net.slots ? s - net.slots : s;
-							const int32_t w = int32_t(syn[u].y);
-							addCurrent(net, s, syn[u].x >> 6, w < 0 ? 1 : 0, w);
-						}
-					}
+		if(tid == 0) {
+			if(doUpdate) {
+				const uint32_t par = t & 1u;
+				net.firedCnt[par * B + b] = sNFired;
+				net.postCnt[par * B + b] = sNPost;
+				if(sNFired) {
+					atomicAdd(&net.firedCountRing[t & net.ringMask], sNFired);
+					atomicAdd(&net.eventsRing[t & net.ringMask], sEvents);
+					atomicAdd(&net.stats[2], (unsigned long long) sNFired);
+					atomicAdd(&net.stats[3], sEvents);
 				}
 			}
+			if(sPushed) atomicAdd(&net.stats[0], sPushed);
+			if(sVisits) atomicAdd(&net.stats[1], sVisits);
 		}
-
-		if(trace) {
-			__syncthreads();
-			if(tid == 0) trace[2] = globalTimer();
-		}
+		if(trace && tid == 0) trace[3] = globalTimer();
 		if(k < A.cycles) {
 			if(!gridSync(net.barrier, A.timeoutNs)) {
 				return;
 			}
 		}
-		if(trace && tid == 0) trace[3] = globalTimer();
+		if(trace && tid == 0) trace[4] = globalTimer();
+	}
+
+	if(SMEM) {
+		__syncthreads();
+		const uint32_t total = net.slots * ownN;
+		for(uint32_t x = tid; x < total; x += blockDim.x) {
+			const uint32_t s = x / ownN, l = x - s * ownN;
+			const size_t n = size_t(ownBase) + l;
+			if(n < nDev) acc32[size_t(s) * nDev + n] = sAcc[x];
+		}
 	}
 }
 
@@ -631,61 +760,83 @@ k_stimulus_scratch(NetDev net, const uint32_t* scratch, uint32_t nf, uint32_t ni
  * gets w = clamp(w + (reward * acc) >> f) and its accumulator cleared.
  *
  * The reference reads a synapse's weight when the spike arrives
- * (deliverSpikes at cycle t0 + d), whereas the step kernel adds it when the
- * source fires (cycle t0). For a spike still in flight when its synapse's
+ * (deliverSpikes at cycle t0 + d), whereas the step kernel adds it one cycle
+ * after the source fires. For a spike still in flight when its synapse's
  * weight changes, the arrival slot therefore holds the old weight; it is
  * corrected here by w_new - w_old, into the same E/I half (the sign of a
  * weight never changes, and a weight that reaches 0 contributes 0 to E). The
  * in-flight spikes of a synapse with delay d are the set bits 0..d-1 of its
  * source's firing history after the last completed cycle (cycleNow - 1):
- * bit k fired at cycleNow-1-k and arrives at cycleNow-1-k+d.
- *
- * The synapses are processed in APPLY_WINDOW-sized windows of the forward
- * matrix, one launch per window, so that the weights a launch rewrites stay
- * in L2 (each target's plastic synapses are sorted by forward position, and
- * rcmWindow locates the range of each target in each window). One warp per
- * target. */
+ * bit k fired at cycleNow-1-k and arrives at cycleNow-1-k+d. */
+__device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
+		const uint64_t* rfNow, uint32_t j, uint32_t f, int32_t acc, uint2 syn)
+{
+	const int32_t wOld = int32_t(syn.y);
+	const int32_t diff = int32_t((int64_t(reward) * int64_t(acc)) >> net.fbits);
+	const int32_t wNew = updatedWeight(wOld, diff, rule);
+	if(wNew != wOld) {
+		net.fcm[f].y = uint32_t(wNew);
+		if(net.deliver) {
+			const uint32_t sd = net.rcmSrcDelay[j];
+			const uint32_t d = (sd & 63u) + 1u;
+			uint64_t pending = rfNow[sd >> 6] & ((uint64_t(1) << d) - 1u);
+			if(pending) {
+				const uint32_t target = syn.x >> 6;
+				const long long delta = (long long) wNew - (long long) wOld;
+				const int half = wOld >= 0 ? 0 : 1;
+				while(pending) {
+					const uint32_t k = uint32_t(__ffsll((long long) pending) - 1);
+					pending &= pending - 1;
+					/* fired at cycleNow-1-k >= 0, arrives at cycleNow-1-k+d */
+					const uint32_t slot = uint32_t((cycleNow - 1u - k + d) % net.slots);
+					addCurrent(net, slot, target, half, delta);
+				}
+			}
+		}
+	}
+	if(acc) {
+		net.rcmAcc[j] = 0;
+	}
+}
+
+/* Items (target, 128-synapse chunk of its plastic synapses) in target order
+ * over a grid-stride loop: the items in flight at any moment are consecutive,
+ * so they rewrite only the few forward-matrix regions that own those targets
+ * (each target's synapses lie in its owner's region, sorted by position),
+ * which stay in L2 while they are rewritten. */
 __global__ void __launch_bounds__(256)
-k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint32_t window)
+k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow)
 {
 	const uint64_t* rfNow = net.rf + size_t(cycleNow & 1u) * net.nDev;
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-	for(uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < net.nDev; t += nwarps) {
-	const uint64_t base = net.rcmStart[t];
-	const uint32_t* win = net.rcmWindow + size_t(t) * (net.windows + 1) + window;
-	const uint64_t e = base + win[1];
-	for(uint64_t j = base + win[0] + lane; j < e; j += 32) {
-		uint32_t f = net.rcmForward[j];
-		int32_t acc = net.rcmAcc[j];
-		uint2 syn = net.fcm[f];
-		int32_t wOld = int32_t(syn.y);
-		int32_t diff = int32_t((int64_t(reward) * int64_t(acc)) >> net.fbits);
-		int32_t wNew = updatedWeight(wOld, diff, rule);
-		if(wNew != wOld) {
-			net.fcm[f].y = uint32_t(wNew);
-			if(net.deliver) {
-				uint32_t sd = net.rcmSrcDelay[j];
-				uint32_t d = (sd & 63u) + 1u;
-				uint64_t pending = rfNow[sd >> 6] & ((uint64_t(1) << d) - 1u);
-				if(pending) {
-					size_t target = syn.x >> 6;
-					long long delta = (long long) wNew - (long long) wOld;
-					int half = wOld >= 0 ? 0 : 1;
-					while(pending) {
-						uint32_t k = uint32_t(__ffsll((long long) pending) - 1);
-						pending &= pending - 1;
-						/* fired at cycleNow-1-k >= 0, arrives at cycleNow-1-k+d */
-						uint32_t slot = uint32_t((cycleNow - 1u - k + d) % net.slots);
-						addCurrent(net, slot, uint32_t(target), half, delta);
-					}
-				}
-			}
+	const uint32_t chunks = net.stdpChunks;
+	const uint64_t items = uint64_t(net.nDev) * chunks;
+	for(uint64_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nwarps) {
+		const uint32_t t = uint32_t(it / chunks);
+		const uint32_t c = uint32_t(it - uint64_t(t) * chunks);
+		const uint32_t b0 = net.rcmStart[t] + c * 128u;
+		const uint32_t e = net.rcmStart[t + 1];
+		if(b0 >= e) continue;
+		const uint32_t j = b0 + lane;
+		uint32_t f[4];
+		int32_t a[4];
+#pragma unroll
+		for(int u = 0; u < 4; ++u) {
+			const uint32_t jj = j + 32u * u;
+			f[u] = jj < e ? net.rcmForward[jj] : 0u;
+			a[u] = jj < e ? net.rcmAcc[jj] : 0;
 		}
-		if(acc) {
-			net.rcmAcc[j] = 0;
+		uint2 syn[4];
+#pragma unroll
+		for(int u = 0; u < 4; ++u) {
+			syn[u] = j + 32u * u < e ? net.fcm[f[u]] : make_uint2(0u, 0u);
 		}
-	}
+#pragma unroll
+		for(int u = 0; u < 4; ++u) {
+			const uint32_t jj = j + 32u * u;
+			if(jj < e) applyOne(net, rule, reward, cycleNow, rfNow, jj, f[u], a[u], syn[u]);
+		}
 	}
 }
 
@@ -713,7 +864,6 @@ k_libm_eval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t
 }
 
 int g_smCount = 0;
-int g_blocksPerSm = 0;
 
 } // namespace
 
@@ -775,43 +925,56 @@ launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, u
 	k_stimulus_scratch<<<1, 32, 0, S(stream)>>>(net, scratch, nf, ni);
 }
 
-/* Co-resident grid for the cooperative launch: as many 1024-thread blocks per
- * SM as the registers allow (one), times the SM count. */
+/* The step kernel's plan: one 1024-thread block per SM (its registers allow
+ * no more), each owning ceil(warps / blocks) neuron warps; the owned current
+ * slots go to shared memory when they are int32 and fit. */
 void
-cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap)
+cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownWarps, bool* smemAcc)
 {
-	const uint32_t warpsPerBlock = BLOCK / 32;
-	if(g_blocksPerSm == 0) {
-		int perSm = 0;
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles, BLOCK, 0);
-		g_blocksPerSm = perSm > 0 ? perSm : 1;
+	uint32_t B = uint32_t(smCount());
+	if(B > MAX_BLOCKS) B = MAX_BLOCKS;
+	uint32_t own = (totalWarps + B - 1) / B;
+	if(own == 0) own = 1;
+	const uint64_t bytes = uint64_t(slots) * own * 32u * 8u;
+	const bool smem = acc32 && bytes <= SMEM_ACC_LIMIT;
+	int perSm = 0;
+	if(smem) {
+		/* the attribute is per device and shared by all simulations: set it
+		 * to the largest size any of them uses */
+		cudaFuncSetAttribute(k_cycles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<true>, BLOCK, size_t(bytes));
+	} else {
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false>, BLOCK, 0);
 	}
-	unsigned b = unsigned(smCount() * g_blocksPerSm);
-	uint32_t gridWarps = b * warpsPerBlock;
-	uint32_t perWarp = (totalWarps + gridWarps - 1) / gridWarps;
-	if(perWarp == 0) perWarp = 1;
-	*blocks = b;
-	*listCap = perWarp * warpsPerBlock * 32;
+	*blocks = perSm >= 1 ? B : 0u;
+	*ownWarps = own;
+	*smemAcc = smem;
 }
 
 void
-launchCycles(const CycleArgs& args, unsigned blocks, void* stream)
+launchCycles(const CycleArgs& args, void* stream)
 {
 	void* params[] = {const_cast<CycleArgs*>(&args)};
-	cudaLaunchCooperativeKernel((const void*) k_cycles, dim3(blocks), dim3(BLOCK), params, 0, S(stream));
+	const NetDev& net = args.net;
+	if(net.smemAcc) {
+		const size_t bytes = size_t(net.slots) * net.ownWarps * 32u * 8u;
+		cudaLaunchCooperativeKernel((const void*) k_cycles<true>, dim3(net.blocks), dim3(BLOCK), params, bytes,
+				S(stream));
+	} else {
+		cudaLaunchCooperativeKernel((const void*) k_cycles<false>, dim3(net.blocks), dim3(BLOCK), params, 0,
+				S(stream));
+	}
 }
 
 void
-launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, uint64_t cycleNow, void* stream)
+launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow, void* stream)
 {
-	if(nrcm == 0) return;
-	/* one warp per target per window */
-	uint64_t blocks = (uint64_t(net.nDev) * 32 + 255) / 256;
-	uint64_t cap = uint64_t(smCount()) * 8;
+	/* one 128-synapse item per warp at a time, 64 warps per SM */
+	const uint64_t items = uint64_t(net.nDev) * net.stdpChunks;
+	uint64_t blocks = (items * 32 + 255) / 256;
+	const uint64_t cap = uint64_t(smCount()) * 8;
 	if(blocks > cap) blocks = cap;
-	for(uint32_t w = 0; w < net.windows; ++w) {
-		k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow, w);
-	}
+	k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow);
 }
 
 void

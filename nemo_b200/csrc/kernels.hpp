@@ -10,22 +10,29 @@
  * warp owns whole 32-bit words of every per-neuron bitmap. Padding slots
  * never fire and have no synapses.
  *
- * The step path is one persistent cooperative kernel (k_cycles) that runs a
- * block of cycles with one grid barrier per cycle. Phase t:
- *   - neuron update of cycle t: read and clear the cycle's current slot
- *     acc[t mod Q], integrate, fire, shift the firing history
- *     (rf[t&1] -> rf[(t+1)&1]), record the firing bitmap and the STDP
- *     post-spike list of cycle t;
- *   - spike push: every neuron fired at t streams its outgoing synapses (one
- *     contiguous range per source, sorted by delay) and adds each weight into
- *     acc[(t+d) mod Q][target] (E or I by sign) with fire-and-forget 64-bit
- *     reductions in L2 — the reference's deliverSpikes at cycle t+d
- *     (src/nemo/cpu/Simulation.cpp:259-308) moved to fire time;
- *   - STDP accumulation of cycle t-1 (targets that fired P cycles before it),
- *     which only reads rf[t&1] and so overlaps the update of cycle t;
+ * The step path is one persistent cooperative kernel (k_cycles) over one
+ * block per SM, with one grid barrier per cycle. Block b owns a contiguous
+ * range of ownWarps x 32 neurons: it updates them, and it alone adds spikes
+ * into their current slots, which it keeps in shared memory for the whole
+ * launch (or in global memory when they do not fit). The forward matrix is
+ * partitioned to match: region b holds, source by source, the synapses whose
+ * target block b owns, each (source, region) segment sorted by delay. Phase t:
+ *   - urgent gather: every block reads the fired sources of cycle t-1 (all
+ *     blocks' lists) and, for each, the delay-1 prefix of its segment of
+ *     region b, adding each weight into slot t mod Q of the target (E or I
+ *     by sign);
+ *   - neuron update of cycle t from slot t mod Q: firing history, bitmap,
+ *     the fired and post-spiking lists of cycle t; overlapped with
+ *   - the deferred gather of cycle t-1 (delays >= 2, into slots (t-1+d)
+ *     mod Q) and the STDP accumulation of cycle t-1 over all blocks'
+ *     post-spiking targets, dealt out over the grid in 128-synapse items.
+ *     Together the two gathers are the reference's deliverSpikes at cycle
+ *     t-1+d (src/nemo/cpu/Simulation.cpp:259-308), done one cycle after the
+ *     firing;
  *   - grid barrier.
- * A final half phase accumulates STDP for the last cycle. Integer sums are
- * exact in any order, so the result is bit-identical to the CPU reference. */
+ * A final phase gathers and learns for the last cycle, so that between
+ * launches every spike fired is in the current slots. Integer sums are exact
+ * in any order, so the result is bit-identical to the CPU reference. */
 
 #include <cstdint>
 
@@ -35,25 +42,33 @@ namespace nemo_b200 {
 
 const int MAX_GROUPS = 8;
 
-/* applyStdp window: 4M synapses = 32 MB of the forward matrix, small enough
- * to stay resident in the 126 MB L2 while its weights are updated */
-const uint64_t APPLY_WINDOW = uint64_t(1) << 22;
+/* most blocks of the step kernel (static shared prefix arrays) */
+const uint32_t MAX_BLOCKS = 256;
+/* shared memory the step kernel may use for current slots */
+const uint32_t SMEM_ACC_LIMIT = 200 * 1024;
 
 struct NetDev {
 	uint32_t nDev;          /* device neurons, multiple of 32 */
 	uint32_t nWords;        /* nDev / 32 */
-	uint32_t rowStride;     /* rows per source: max(maxDelay, 1) */
 	uint32_t slots;         /* current slots: maxDelay + 1 (cycle t uses slot t mod slots) */
 	int acc32;              /* int32 accumulators (proven not to overflow), else int64 */
 	uint32_t ringMask;      /* firing-ring cycles - 1 */
 	uint32_t fbits;         /* fractional bits of the Q(31-f).f weights */
 	int deliver;            /* 0 when no delay is deliverable (max delay 64) */
 
-	/* forward connectivity: row r = source * rowStride + delay - 1; the rows
-	 * of one source are contiguous, so [rowStart[s*rowStride],
-	 * rowStart[(s+1)*rowStride]) is all of its synapses in delay order */
-	const uint64_t* rowStart;      /* [nDev * rowStride + 1] */
+	/* ownership: block b of the step kernel owns neurons
+	 * [b * ownWarps * 32, (b + 1) * ownWarps * 32) */
+	uint32_t blocks;
+	uint32_t ownWarps;
+	int smemAcc;            /* current slots of the owned neurons in shared memory */
+
+	/* forward connectivity, partitioned by target owner: region b =
+	 * [regionBase[b], regionBase[b+1]); within it the synapses of source s
+	 * are [segOff[s * blocks + b], segOff[(s + 1) * blocks + b]), sorted by
+	 * delay */
 	uint2* fcm;                    /* {target << 6 | (delay - 1), int32 weight} */
+	const uint64_t* regionBase;    /* [blocks + 1] */
+	const uint32_t* segOff;        /* [(nDev + 1) * blocks] */
 	const uint32_t* outDegree;     /* [nDev] synapses per source */
 
 	void* acc;                     /* [slots][nDev][2] E, I current of a future cycle (int32 or int64) */
@@ -64,22 +79,22 @@ struct NetDev {
 	float* ext;                    /* [nDev] external current, cleared after use */
 	uint32_t* fstim;               /* [nWords] firing stimulus, cleared after use */
 
-	/* per-block work lists of the step kernel: [blocks][9 * listCap] */
-	uint32_t* lists;
-	uint32_t fireChunks;           /* 128-synapse chunks per source (max out-degree) */
+	/* per-cycle lists by cycle parity and block, [2][blocks][ownWarps * 32],
+	 * with their lengths [2][blocks]: fired sources (device indices) and the
+	 * reverse-matrix ranges {first, count} of post-spiking targets */
+	uint32_t* firedList;
+	uint32_t* firedCnt;
+	uint2* postList;
+	uint32_t* postCnt;
 
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
 	uint32_t stdpChunks;           /* 128-synapse chunks per target (max in-degree) */
-	const uint64_t* rcmStart;      /* [nDev + 1] */
+	const uint32_t* rcmStart;      /* [nDev + 1] (fewer than 2^32 synapses) */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
 	const uint32_t* rcmForward;    /* index into fcm, ascending within a target */
 	int32_t* rcmAcc;
-	/* [nDev][windows + 1]: first synapse of each target in each forward
-	 * window of APPLY_WINDOW synapses (applyStdp works window by window) */
-	const uint32_t* rcmWindow;
-	uint32_t windows;
 
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;
@@ -123,10 +138,10 @@ struct CycleArgs {
 	int ngroups;
 	uint64_t firstCycle;
 	uint32_t cycles;
-	uint32_t listCap;                    /* entries per per-block work list */
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
-	/* optional phase timestamps (%globaltimer ns), [cycle][block][4]: phase
-	 * start, update done, push and STDP done, barrier passed */
+	/* optional phase timestamps (%globaltimer ns), [cycles + 1][block][5]:
+	 * phase start, urgent gather done, last update warp done (0 when the
+	 * block updates nothing), all work done, barrier passed */
 	unsigned long long* trace;
 };
 
@@ -153,13 +168,14 @@ int noallocScratch(int device, uint32_t** ptr);
 void launchStimulus(const NetDev& net, const StimDev& stim, void* stream);
 /* Stimulus from the allocation-free scratch (layout in kernels.cu). */
 void launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, uint32_t ni, void* stream);
-/* Cooperative launch of k_cycles over `blocks` blocks (from cyclesGrid). */
-void launchCycles(const CycleArgs& args, unsigned blocks, void* stream);
-/* The co-resident grid (one block per SM) and the per-block list capacity
- * (the most neurons one block updates in a cycle). */
-void cyclesGrid(uint32_t totalWarps, unsigned* blocks, uint32_t* listCap);
-void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t nrcm, uint64_t cycleNow,
-		void* stream);
+/* Cooperative launch of k_cycles (grid and shared memory from args.net). */
+void launchCycles(const CycleArgs& args, void* stream);
+/* The step kernel's grid (one block per SM, at most MAX_BLOCKS; 0 when the
+ * kernel cannot be resident), the warps each block owns, and whether the
+ * owned current slots fit in shared memory (`slots` slots of 8-byte int32 E/I
+ * pairs; int64 sums use global memory). */
+void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownWarps, bool* smemAcc);
+void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow, void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);

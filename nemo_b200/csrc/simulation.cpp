@@ -205,31 +205,18 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 synapses per simulation");
 	}
 
-	/* ---- forward matrix: rows (source, delay), insertion order within a row ---- */
-	const uint32_t Ds = std::max<uint32_t>(m_maxDelay, 1);
-	const size_t nrows = size_t(m_nDev) * Ds;
-	std::vector<uint64_t> rowStart(nrows + 1, 0);
+	/* ---- device: the step kernel's plan decides the forward layout ---- */
+	if(conf.cudaDevice >= 0) {
+		NEMO_CUDA(cudaSetDevice(conf.cudaDevice));
+	}
 	std::vector<uint32_t> dsrc(S), dtgt(S);
+	std::vector<int32_t> wfx(S);
+	std::vector<uint32_t> outDegree(m_nDev, 0);
 	for(size_t s = 0; s < S; ++s) {
 		dsrc[s] = map(net.src[s]);
 		dtgt[s] = map(net.tgt[s]);
-		rowStart[size_t(dsrc[s]) * Ds + net.dly[s] - 1 + 1]++;
-	}
-	for(size_t r = 0; r < nrows; ++r) rowStart[r + 1] += rowStart[r];
-	std::vector<uint2> fcm(S);
-	std::vector<uint32_t> fcmPos(S);
-	std::vector<uint32_t> synAt(S);   /* synapse at each forward position */
-	std::vector<uint32_t> outDegree(m_nDev, 0);
-	{
-		std::vector<uint64_t> fill(rowStart.begin(), rowStart.end() - 1);
-		for(size_t s = 0; s < S; ++s) {
-			size_t r = size_t(dsrc[s]) * Ds + net.dly[s] - 1;
-			uint64_t pos = fill[r]++;
-			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(toFix(net.wgt[s], m_fbits)));
-			fcmPos[s] = uint32_t(pos);
-			synAt[pos] = uint32_t(s);
-			outDegree[dsrc[s]]++;
-		}
+		wfx[s] = toFix(net.wgt[s], m_fbits);
+		outDegree[dsrc[s]]++;
 	}
 	/* deliverable delays: the reference masks the history with
 	 * ~(~0 << maxDelay), a shift evaluated modulo 64 on x86-64
@@ -238,7 +225,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	const bool deliver = S > 0 && m_maxDelay < 64;
 	/* current slots: arrivals for cycle c go to slot c mod (maxDelay + 1);
 	 * a slot is drained at its cycle before any spike for the cycle one
-	 * revolution later can be pushed */
+	 * revolution later can be added */
 	const uint32_t slots = deliver ? m_maxDelay + 1 : 1;
 
 	/* int32 accumulators are exact when no slot can leave the int32 range:
@@ -249,7 +236,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	{
 		std::vector<int64_t> pos(m_nDev, 0), neg(m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
-			int64_t w = int32_t(fcm[fcmPos[s]].y);
+			int64_t w = wfx[s];
 			if(m_stdpOn && net.plastic[s]) {
 				if(w > 0) w = std::max<int64_t>(w, m_rule.maxE);
 				else if(w < 0) w = std::min<int64_t>(w, m_rule.maxI);
@@ -262,10 +249,64 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		}
 	}
 
+	uint32_t ownWarps = 1;
+	bool smemAcc = false;
+	cyclesPlan(m_nDev / 32, slots, acc32, &m_blocks, &ownWarps, &smemAcc);
+	NEMO_CUDA(cudaGetLastError());
+	if(m_blocks == 0) {
+		fail(NEMO_CUDA_INVOCATION_ERROR, "The step kernel cannot be resident on this device");
+	}
+	const uint32_t B = m_blocks;
+	const uint32_t ownN = ownWarps * 32;
+
+	/* ---- forward matrix partitioned by target owner: region b holds, source
+	 * by source, the synapses whose target block b owns; within a (source,
+	 * region) segment by delay, then insertion order ---- */
+	std::vector<uint64_t> regionBase(size_t(B) + 1, 0);
+	std::vector<uint32_t> segOff((size_t(m_nDev) + 1) * B, 0);
+	std::vector<uint2> fcm(S);
+	std::vector<uint32_t> fcmPos(S);
+	std::vector<uint32_t> synAt(S);   /* synapse at each forward position */
+	{
+		/* cursor[b][s]: count, then next free offset within region b */
+		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
+		for(size_t s = 0; s < S; ++s) {
+			cursor[size_t(dtgt[s] / ownN) * m_nDev + dsrc[s]]++;
+		}
+		for(uint32_t b = 0; b < B; ++b) {
+			uint32_t* c = &cursor[size_t(b) * m_nDev];
+			uint64_t run = 0;
+			for(uint32_t src = 0; src < m_nDev; ++src) {
+				segOff[size_t(src) * B + b] = uint32_t(run);
+				uint32_t k = c[src];
+				c[src] = uint32_t(run);
+				run += k;
+			}
+			segOff[size_t(m_nDev) * B + b] = uint32_t(run);
+			regionBase[b + 1] = regionBase[b] + run;
+		}
+		/* filled in order of delay (stable), so that every segment is sorted
+		 * by delay and its delay-1 synapses are a prefix */
+		std::vector<uint32_t> byDelay(S);
+		{
+			std::vector<uint64_t> at(66, 0);
+			for(size_t s = 0; s < S; ++s) at[net.dly[s] + 1]++;
+			for(size_t d = 1; d < at.size(); ++d) at[d] += at[d - 1];
+			for(size_t s = 0; s < S; ++s) byDelay[at[net.dly[s]]++] = uint32_t(s);
+		}
+		for(size_t k = 0; k < S; ++k) {
+			const size_t s = byDelay[k];
+			const uint32_t b = dtgt[s] / ownN;
+			const uint64_t pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
+			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(wfx[s]));
+			fcmPos[s] = uint32_t(pos);
+			synAt[pos] = uint32_t(s);
+		}
+	}
+
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
-	std::vector<uint64_t> rcmStart;
-	std::vector<uint32_t> rcmSrcDelay, rcmForward, rcmWindow;
-	m_windows = 1;
+	std::vector<uint32_t> rcmStart;
+	std::vector<uint32_t> rcmSrcDelay, rcmForward;
 	uint64_t maxIn = 0;
 	if(m_stdpOn) {
 		rcmStart.assign(size_t(m_nDev) + 1, 0);
@@ -279,36 +320,19 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		rcmForward.resize(m_nrcm);
 		/* filled in forward order, so each target's synapses are sorted by
 		 * their position in the forward matrix */
-		std::vector<uint64_t> fill(rcmStart.begin(), rcmStart.end() - 1);
+		std::vector<uint32_t> fill(rcmStart.begin(), rcmStart.end() - 1);
 		for(size_t pos = 0; pos < S; ++pos) {
 			size_t s = synAt[pos];
 			if(!net.plastic[s]) continue;
-			uint64_t j = fill[dtgt[s]]++;
+			uint32_t j = fill[dtgt[s]]++;
 			rcmSrcDelay[j] = (dsrc[s] << 6) | (net.dly[s] - 1);
 			rcmForward[j] = uint32_t(pos);
 		}
-		/* applyStdp works through the forward matrix in windows small enough
-		 * to stay in L2; rcmWindow[t][k] is the first of target t's synapses
-		 * at forward position >= k * APPLY_WINDOW */
-		m_windows = uint32_t((S + APPLY_WINDOW - 1) / APPLY_WINDOW);
-		if(m_windows == 0) m_windows = 1;
-		const uint32_t K = m_windows;
-		rcmWindow.assign(size_t(m_nDev) * (K + 1), 0);
-		for(uint32_t t = 0; t < m_nDev; ++t) {
-			uint64_t base = rcmStart[t], len = rcmStart[t + 1] - base, j = 0;
-			for(uint32_t k = 0; k <= K; ++k) {
-				while(j < len && rcmForward[base + j] < uint64_t(k) * APPLY_WINDOW) j++;
-				rcmWindow[size_t(t) * (K + 1) + k] = uint32_t(k == K ? len : j);
-			}
-		}
 	}
-	/* 128-synapse work items per post-spiking target / per fired source */
+	/* 128-synapse STDP work items per post-spiking target */
 	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + 127) / 128);
-	uint64_t maxOut = 0;
-	for(uint32_t n = 0; n < m_nDev; ++n) maxOut = std::max<uint64_t>(maxOut, outDegree[n]);
-	const uint64_t fireChunks = std::max<uint64_t>(1, (maxOut + 127) / 128);
-	if(uint64_t(m_nDev) * std::max(stdpChunks, fireChunks) >= (uint64_t(1) << 32)) {
-		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 synapses per neuron");
+	if(uint64_t(m_nDev) * stdpChunks >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 plastic synapses per neuron");
 	}
 
 	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
@@ -323,9 +347,6 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	}
 
 	/* ---- device ---- */
-	if(conf.cudaDevice >= 0) {
-		NEMO_CUDA(cudaSetDevice(conf.cudaDevice));
-	}
 	cudaStream_t stream;
 	NEMO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
 	m_stream = stream;
@@ -338,14 +359,17 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 
 	m_net.nDev = m_nDev;
 	m_net.nWords = m_nDev / 32;
-	m_net.rowStride = Ds;
 	m_net.slots = slots;
 	m_net.acc32 = acc32 ? 1 : 0;
 	m_net.ringMask = m_ring - 1;
 	m_net.fbits = m_fbits;
 	m_net.deliver = deliver ? 1 : 0;
-	m_net.rowStart = (const uint64_t*) put(rowStart.data(), rowStart.size() * 8);
+	m_net.blocks = B;
+	m_net.ownWarps = ownWarps;
+	m_net.smemAcc = smemAcc ? 1 : 0;
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
+	m_net.regionBase = (const uint64_t*) put(regionBase.data(), regionBase.size() * 8);
+	m_net.segOff = (const uint32_t*) put(segOff.data(), segOff.size() * 4);
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
 	m_net.acc = alloc(size_t(slots) * m_nDev * (acc32 ? 8 : 16));
 	m_net.rf = (uint64_t*) alloc(size_t(2) * m_nDev * 8);
@@ -356,25 +380,18 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
 	m_net.stats = (unsigned long long*) alloc(4 * 8);
 	m_net.barrier = (unsigned*) alloc(4 * 4);
+	m_net.firedList = (uint32_t*) alloc(size_t(2) * B * ownN * 4);
+	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
+	m_net.postList = (uint2*) alloc(size_t(2) * B * ownN * 8);
+	m_net.postCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	m_net.stdp = m_stdpOn ? 1 : 0;
 	m_net.stdpChunks = uint32_t(stdpChunks);
-	m_net.fireChunks = uint32_t(fireChunks);
-	{
-		uint32_t totalWarps = 0;
-		for(const Group& g : m_groups) totalWarps += (g.count + 31) / 32;
-		uint32_t cap;
-		cyclesGrid(totalWarps, &m_blocks, &cap);
-		m_args.listCap = cap;
-		m_net.lists = (uint32_t*) alloc(size_t(m_blocks) * cap * 9 * 4);
-	}
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
-		m_net.rcmStart = (const uint64_t*) put(rcmStart.data(), rcmStart.size() * 8);
+		m_net.rcmStart = (const uint32_t*) put(rcmStart.data(), rcmStart.size() * 4);
 		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
 		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
 		m_net.rcmAcc = (int32_t*) alloc(size_t(m_nrcm) * 4);
-		m_net.rcmWindow = (const uint32_t*) put(rcmWindow.data(), rcmWindow.size() * 4);
-		m_net.windows = m_windows;
 	}
 
 	/* per-neuron RNG seeds by simulation index (src/nemo/RNG.cpp:39-62):
@@ -469,7 +486,7 @@ Simulation::launchBlock(uint64_t first, unsigned cycles)
 	for(int gi = 0; gi < a.ngroups; ++gi) {
 		a.groups[gi].timerBase = uint32_t(m_timerBase);
 	}
-	launchCycles(a, m_blocks, m_stream);
+	launchCycles(a, m_stream);
 	NEMO_CUDA(cudaGetLastError());
 }
 
@@ -723,7 +740,7 @@ Simulation::applyStdp(float reward)
 		fail(NEMO_INVALID_INPUT, msg.str());
 	}
 	if(m_nrcm) {
-		launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_cycle, m_stream);
+		launchApplyStdp(m_net, m_rule, fx, m_cycle, m_stream);
 	}
 	m_fcmHostValid = false;
 }
@@ -957,7 +974,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 		launchBlock(m_cycle, cyclesPerStep);
 		m_cycle += cyclesPerStep;
 		if(apply && m_nrcm) {
-			launchApplyStdp(m_net, m_rule, fx, m_nrcm, m_cycle, m_stream);
+			launchApplyStdp(m_net, m_rule, fx, m_cycle, m_stream);
 		}
 	}
 	NEMO_CUDA(cudaEventRecord(e1, stream));
@@ -993,7 +1010,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	m_cycle += cycles;
 	NEMO_CUDA(cudaEventRecord(e1, stream));
 	if(m_stdpOn && m_nrcm) {
-		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_nrcm, m_cycle, m_stream);
+		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_cycle, m_stream);
 		m_fcmHostValid = false;
 	}
 	NEMO_CUDA(cudaEventRecord(e2, stream));
@@ -1021,13 +1038,14 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 }
 
 void
-Simulation::trace(unsigned cycles, double out[8])
+Simulation::trace(unsigned cycles, double out[10])
 {
 	if(cycles == 0) {
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");
 	}
 	cudaStream_t stream = STREAM(m_stream);
-	size_t words = size_t(cycles + 1) * m_blocks * 4;
+	const unsigned S = 5;
+	size_t words = size_t(cycles + 1) * m_blocks * S;
 	unsigned long long* dTrace;
 	NEMO_CUDA(cudaMalloc(&dTrace, words * 8));
 	NEMO_CUDA(cudaMemsetAsync(dTrace, 0, words * 8, stream));
@@ -1036,7 +1054,7 @@ Simulation::trace(unsigned cycles, double out[8])
 	a.cycles = cycles;
 	a.trace = dTrace;
 	for(int gi = 0; gi < a.ngroups; ++gi) a.groups[gi].timerBase = uint32_t(m_timerBase);
-	launchCycles(a, m_blocks, m_stream);
+	launchCycles(a, m_stream);
 	NEMO_CUDA(cudaGetLastError());
 	m_cycle += cycles;
 	m_stateDirty = true;
@@ -1046,32 +1064,38 @@ Simulation::trace(unsigned cycles, double out[8])
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	cudaFree(dTrace);
 	checkDeviceError();
-	double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+	double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 	for(unsigned k = 0; k < cycles; ++k) {
-		double minT0 = 1e300, maxT3 = 0, maxU = 0, sumU = 0, maxW = 0, sumW = 0, maxT2 = 0, minT2 = 1e300, sumT3 = 0;
+		double minT0 = 1e300, maxT4 = 0, maxG = 0, sumG = 0, maxU = 0, sumU = 0, maxW = 0, sumW = 0,
+				maxT3 = 0, minT3 = 1e300, sumT4 = 0;
 		for(unsigned b = 0; b < m_blocks; ++b) {
-			const unsigned long long* r = &h[(size_t(k) * m_blocks + b) * 4];
-			double t0 = double(r[0]), t1 = double(r[1]), t2 = double(r[2]), t3 = double(r[3]);
+			const unsigned long long* r = &h[(size_t(k) * m_blocks + b) * S];
+			double t0 = double(r[0]), t1 = double(r[1]), t2 = double(r[2]), t3 = double(r[3]), t4 = double(r[4]);
+			if(r[2] == 0) t2 = t1;   /* the block updates nothing */
 			minT0 = std::min(minT0, t0);
+			maxT4 = std::max(maxT4, t4);
+			maxG = std::max(maxG, t1 - t0);
+			sumG += t1 - t0;
+			maxU = std::max(maxU, t2 - t1);
+			sumU += t2 - t1;
+			maxW = std::max(maxW, t3 - t1);
+			sumW += t3 - t1;
 			maxT3 = std::max(maxT3, t3);
-			maxU = std::max(maxU, t1 - t0);
-			sumU += t1 - t0;
-			maxW = std::max(maxW, t2 - t1);
-			sumW += t2 - t1;
-			maxT2 = std::max(maxT2, t2);
-			minT2 = std::min(minT2, t2);
-			sumT3 += t3;
+			minT3 = std::min(minT3, t3);
+			sumT4 += t4;
 		}
-		acc[0] += maxT3 - minT0;
-		acc[1] += maxU;
-		acc[2] += sumU / m_blocks;
-		acc[3] += maxW;
-		acc[4] += sumW / m_blocks;
-		acc[5] += maxT2 - minT0;
-		acc[6] += sumT3 / m_blocks - maxT2;
-		acc[7] += maxT2 - minT2;
+		acc[0] += maxT4 - minT0;
+		acc[1] += maxG;
+		acc[2] += sumG / m_blocks;
+		acc[3] += maxU;
+		acc[4] += sumU / m_blocks;
+		acc[5] += maxT3 - minT0;
+		acc[6] += sumT4 / m_blocks - maxT3;
+		acc[7] += maxT3 - minT3;
+		acc[8] += maxW;
+		acc[9] += sumW / m_blocks;
 	}
-	for(int i = 0; i < 8; ++i) out[i] = acc[i] / cycles;
+	for(int i = 0; i < 10; ++i) out[i] = acc[i] / cycles;
 }
 
 uint64_t

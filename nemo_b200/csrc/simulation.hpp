@@ -91,10 +91,11 @@ public:
 
 	/* Phase timing of one traced persistent launch of `cycles` cycles, means
 	 * over cycles in ns: [0] phase (first start to last barrier exit),
-	 * [1] max / [2] mean block update time, [3] max / [4] mean block push +
-	 * STDP time, [5] first start to last block done, [6] last arrival to
-	 * mean barrier exit, [7] spread of block arrivals. */
-	void trace(unsigned cycles, double out[8]);
+	 * [1] max / [2] mean block urgent gather, [3] max / [4] mean block
+	 * update, [5] first start to last block done, [6] last arrival to mean
+	 * barrier exit, [7] spread of block arrivals, [8] max / [9] mean block
+	 * update with the overlapped deferred gather and STDP. */
+	void trace(unsigned cycles, double out[10]);
 
 private:
 	struct Group {
@@ -140,7 +141,6 @@ private:
 	NetDev m_net;
 	CycleArgs m_args;
 	unsigned m_blocks;          /* grid of the persistent step kernel */
-	uint32_t m_windows;         /* forward-matrix windows of applyStdp */
 	bool m_stdpOn;
 	StdpRule m_rule;
 	StdpFunction m_stdpFn;
