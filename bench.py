@@ -311,12 +311,13 @@ def run_b200(args):
 
     roof = roofline(sim, lib, wl)
     clk = clocks.summary()
-    tr = (ctypes.c_double * 10)()
-    lib.dll.nemo_b200_trace.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double * 10]
+    tr = (ctypes.c_double * 14)()
+    lib.dll.nemo_b200_trace.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double * 14]
     lib.call("nemo_b200_trace", sim.handle, CYCLES_PER_STEP, tr)
-    phase_ns = dict(zip(["phase", "urgent_gather_max", "urgent_gather_mean", "update_max", "update_mean",
-                         "to_last_arrival", "barrier_release", "arrival_spread", "overlapped_max",
-                         "overlapped_mean"], [round(x, 1) for x in tr]))
+    phase_ns = dict(zip(["phase", "update_max", "update_mean", "work_max", "work_mean",
+                         "to_last_arrival", "barrier_release", "arrival_spread", "after_update_max",
+                         "after_update_mean", "gather_unit", "stdp_unit", "gather_units_per_block",
+                         "stdp_units_per_block"], [round(x, 1) for x in tr]))
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -89,13 +89,14 @@ nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float re
 
 /* Phase timing of the step kernel over `cycles` cycles (one traced launch;
  * the cycles are simulated). Means over cycles, in ns: out[0] whole phase,
- * out[1] / out[2] slowest / mean block urgent (delay-1) spike gather,
- * out[3] / out[4] slowest / mean block neuron update, out[5] phase start to
- * the last block's arrival at the grid barrier, out[6] last arrival to
- * barrier exit, out[7] spread of the blocks' arrivals, out[8] / out[9]
- * slowest / mean block update together with the overlapped deferred gather
- * and STDP accumulation. */
-nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[10]);
+ * out[1] / out[2] slowest / mean block neuron update (with the delay-1
+ * push), out[3] / out[4] slowest / mean block work of the phase, out[5]
+ * phase start to the last block's arrival at the grid barrier, out[6] last
+ * arrival to barrier exit, out[7] spread of the blocks' arrivals, out[8] /
+ * out[9] slowest / mean block work left after its update, out[10] /
+ * out[11] mean duration of one gather / STDP work unit of a warp, out[12] /
+ * out[13] such units per block and cycle. */
+nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[14]);
 
 /* Diagnostics: the device noise transform of two RNG words per sample,
  * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the

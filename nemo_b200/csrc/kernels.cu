@@ -22,6 +22,8 @@ namespace {
 
 const unsigned FULL = 0xffffffffu;
 const unsigned BLOCK = 1024;
+/* words per block and cycle of the optional phase trace (kernels.hpp) */
+const unsigned TRACE_WORDS = 9;
 
 /* 64-bit shifts by a count that may reach 64, evaluated like the x86-64
  * shift the reference runs on (count modulo 64). */
@@ -77,30 +79,6 @@ __device__ __forceinline__ float nrand(uint4& s, const uint32_t* sinTab, const u
 	return nrandWords(u1, u2, sinTab, logTab);
 }
 
-/* Read and clear neuron n's E/I sums for the current cycle's slot. With
- * int32 accumulators the host has proven that no sum can leave the int32
- * range, so the value equals the int64 sum and needs no saturation. */
-__device__ __forceinline__ void takeCurrents(const NetDev& net, uint32_t slot, uint32_t n, float& E, float& I)
-{
-	if(net.acc32) {
-		int2* acc = reinterpret_cast<int2*>(net.acc) + size_t(slot) * net.nDev;
-		int2 a = acc[n];
-		if(a.x | a.y) {
-			acc[n] = make_int2(0, 0);
-		}
-		E = wfxToFloat(a.x, net.fbits);
-		I = wfxToFloat(a.y, net.fbits);
-	} else {
-		longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
-		longlong2 a = acc[n];
-		if(a.x | a.y) {
-			acc[n] = make_longlong2(0, 0);
-		}
-		E = wfxToFloat(a.x, net.fbits);
-		I = wfxToFloat(a.y, net.fbits);
-	}
-}
-
 /* Add a weight into the E (w >= 0) or I half of a current slot */
 __device__ __forceinline__ void addCurrent(const NetDev& net, uint32_t slot, uint32_t target, int half, long long w)
 {
@@ -112,6 +90,111 @@ __device__ __forceinline__ void addCurrent(const NetDev& net, uint32_t slot, uin
 	}
 }
 
+/* Read and clear the raw E/I sums of neuron n in current slot `slot` */
+__device__ __forceinline__ void takeSlot(const NetDev& net, uint32_t slot, uint32_t n, long long& e, long long& i)
+{
+	if(net.acc32) {
+		int2* acc = reinterpret_cast<int2*>(net.acc) + size_t(slot) * net.nDev;
+		const int2 a = acc[n];
+		if(a.x | a.y) acc[n] = make_int2(0, 0);
+		e = a.x;
+		i = a.y;
+	} else {
+		longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
+		const longlong2 a = acc[n];
+		if(a.x | a.y) acc[n] = make_longlong2(0, 0);
+		e = a.x;
+		i = a.y;
+	}
+}
+
+/* Add raw E/I sums into neuron n's slot (single writer) */
+__device__ __forceinline__ void addSlot(const NetDev& net, uint32_t slot, uint32_t n, long long e, long long i)
+{
+	if(net.acc32) {
+		int2* acc = reinterpret_cast<int2*>(net.acc) + size_t(slot) * net.nDev;
+		const int2 a = acc[n];
+		acc[n] = make_int2(a.x + int(e), a.y + int(i));
+	} else {
+		longlong2* acc = reinterpret_cast<longlong2*>(net.acc) + size_t(slot) * net.nDev;
+		const longlong2 a = acc[n];
+		acc[n] = make_longlong2(a.x + e, a.y + i);
+	}
+}
+
+/* Read and clear neuron n's delay-1 inbox of cycle parity p */
+__device__ __forceinline__ void takeInbox(const NetDev& net, uint32_t p, uint32_t n, long long& e, long long& i)
+{
+	if(net.acc32) {
+		int2* box = reinterpret_cast<int2*>(net.inbox) + size_t(p) * net.nDev;
+		const int2 a = box[n];
+		if(a.x | a.y) box[n] = make_int2(0, 0);
+		e = a.x;
+		i = a.y;
+	} else {
+		longlong2* box = reinterpret_cast<longlong2*>(net.inbox) + size_t(p) * net.nDev;
+		const longlong2 a = box[n];
+		if(a.x | a.y) box[n] = make_longlong2(0, 0);
+		e = a.x;
+		i = a.y;
+	}
+}
+
+/* Delay-1 synapses of the warp's fired neurons (lane ranges d1 of the
+ * delay-1 part of the forward matrix, empty for lanes that did not fire) into
+ * their targets' inbox of parity p, by fire-and-forget reductions: the
+ * arrivals for the next cycle. The ranges are concatenated over the lanes
+ * and worked off two records per lane at a time. Returns the number of
+ * synapses added (warp total, on every lane). */
+__device__ __forceinline__ uint32_t pushDelayOne(const NetDev& net, uint32_t firedMask, uint2 d1, uint32_t p,
+		uint32_t lane)
+{
+	const uint32_t cnt = d1.y - d1.x;
+	uint32_t incl = cnt;
+#pragma unroll
+	for(int d = 1; d < 32; d <<= 1) {
+		const uint32_t x = __shfl_up_sync(FULL, incl, d);
+		if(lane >= uint32_t(d)) incl += x;
+	}
+	const uint32_t total = __shfl_sync(FULL, incl, 31);
+	const uint32_t excl = incl - cnt;
+	const uint2* recs = net.fcm + net.d1Base;
+	for(uint32_t base = 0; base < total; base += 64u) {
+		uint32_t pos[2] = {0u, 0u};
+		/* the record of each index: in the range of the fired lane that
+		 * holds it */
+		for(uint32_t m = firedMask; m; m &= m - 1) {
+			const uint32_t L = uint32_t(__ffs(int(m)) - 1);
+			const uint32_t eL = __shfl_sync(FULL, excl, L);
+			const uint32_t cL = __shfl_sync(FULL, cnt, L);
+			const uint32_t sL = __shfl_sync(FULL, d1.x, L);
+#pragma unroll
+			for(int h = 0; h < 2; ++h) {
+				const uint32_t idx = base + uint32_t(h) * 32u + lane;
+				if(idx >= eL && idx < eL + cL) pos[h] = sL + (idx - eL);
+			}
+		}
+		uint2 r[2];
+#pragma unroll
+		for(int h = 0; h < 2; ++h) {
+			r[h] = base + uint32_t(h) * 32u + lane < total ? __ldg(&recs[pos[h]]) : make_uint2(0u, 0u);
+		}
+#pragma unroll
+		for(int h = 0; h < 2; ++h) {
+			if(base + uint32_t(h) * 32u + lane < total) {
+				const int32_t w = int32_t(r[h].y);
+				const size_t idx = (size_t(p) * net.nDev + (r[h].x >> 6)) * 2 + (w < 0 ? 1 : 0);
+				if(net.acc32) {
+					atomicAdd(reinterpret_cast<unsigned*>(net.inbox) + idx, (unsigned) w);
+				} else {
+					atomicAdd(reinterpret_cast<unsigned long long*>(net.inbox) + idx, (unsigned long long) (long long) w);
+				}
+			}
+		}
+	}
+	return total;
+}
+
 __device__ __forceinline__ float takeExternal(const NetDev& net, uint32_t n)
 {
 	float x = net.ext[n];
@@ -119,19 +202,6 @@ __device__ __forceinline__ float takeExternal(const NetDev& net, uint32_t n)
 		net.ext[n] = 0.0f;
 	}
 	return x;
-}
-
-/* Per-warp firing-stimulus word of this warp's 32 neurons, cleared after use */
-__device__ __forceinline__ uint32_t takeStimWord(const NetDev& net, uint32_t n, uint32_t lane)
-{
-	uint32_t w = 0;
-	if(lane == 0) {
-		w = net.fstim[n >> 5];
-		if(w) {
-			net.fstim[n >> 5] = 0;
-		}
-	}
-	return __shfl_sync(FULL, w, 0);
 }
 
 /* ---------------- neuron models (one neuron per thread) ---------------- */
@@ -142,18 +212,19 @@ __device__ __forceinline__ uint32_t takeStimWord(const NetDev& net, uint32_t n, 
 
 /* Izhikevich (src/nemo/cpu/plugins/Izhikevich.cpp:53-97). Parameters a, b, c,
  * d, sigma; state u, v. The v update evaluates its bracket in double (double
- * literals in the reference), the u update in float. */
+ * literals in the reference), the u update in float. `noise` is the cycle's
+ * normal deviate (drawNoise), used when sigma is not 0. */
 __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		float E, float I, bool stim)
+		float E, float I, bool stim, float noise)
 {
 	const size_t c = g.count;
 	const float X = net.ext[n];
-	const float sigma = g.param[4 * c + i];
-	uint4 s = g.rng[i];
-	const float a = g.param[0 * c + i];
-	const float b = g.param[1 * c + i];
-	const float pc = g.param[2 * c + i];
-	const float pd = g.param[3 * c + i];
+	/* parameters do not change during a launch: read-only loads */
+	const float sigma = __ldg(&g.param[4 * c + i]);
+	const float a = __ldg(&g.param[0 * c + i]);
+	const float b = __ldg(&g.param[1 * c + i]);
+	const float pc = __ldg(&g.param[2 * c + i]);
+	const float pd = __ldg(&g.param[3 * c + i]);
 	float u = g.state[0 * c + i];
 	float v = g.state[1 * c + i];
 	if(X != 0.0f) {
@@ -161,8 +232,7 @@ __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDe
 	}
 	float In = __fadd_rn(__fadd_rn(E, I), X);
 	if(sigma != 0.0f) {
-		In = __fadd_rn(In, __fmul_rn(sigma, nrand(s, net.sinTab, net.logTab)));
-		g.rng[i] = s;
+		In = __fadd_rn(In, __fmul_rn(sigma, noise));
 	}
 	bool fired = false;
 	for(int k = 0; k < 4; ++k) {
@@ -183,6 +253,21 @@ __device__ __forceinline__ bool modelIzhikevich(const NetDev& net, const GroupDe
 	g.state[0 * c + i] = u;
 	g.state[1 * c + i] = v;
 	return fired;
+}
+
+/* The Izhikevich thalamic noise of one cycle (Izhikevich.cpp:62-64): a
+ * normal deviate drawn from the neuron's generator when its sigma is not 0
+ * (the generator advances only then); 0 otherwise. */
+__device__ __forceinline__ float drawNoise(const NetDev& net, const GroupDev& g, uint32_t i)
+{
+	const float sigma = __ldg(&g.param[4 * size_t(g.count) + i]);
+	float nz = 0.0f;
+	if(sigma != 0.0f) {
+		uint4 s = g.rng[i];
+		nz = nrand(s, net.sinTab, net.logTab);
+		g.rng[i] = s;
+	}
+	return nz;
 }
 
 /* IF_curr_exp (src/nemo/cpu/plugins/IF_curr_exp.cpp:74-121). Parameters in
@@ -432,11 +517,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t B = gridDim.x;
 	const uint32_t b = blockIdx.x;
 	const size_t nDev = net.nDev;
-	const uint32_t ownN = net.ownWarps * 32u;
-	const uint32_t ownBase = b * ownN;
-	const uint32_t totalWarps = A.groupWarp[A.ngroups];
-	const uint32_t firstWarp = b * net.ownWarps;
-	const uint32_t myWarps = firstWarp < totalWarps ? min(net.ownWarps, totalWarps - firstWarp) : 0u;
+	const uint32_t ownN = net.ownWarps * 32u;       /* list and slot stride per block */
+	const uint32_t firstWarp = ownFirst(b, net.ownQ, net.ownR);
+	const uint32_t myWarps = net.ownQ + (b < net.ownR ? 1u : 0u);
+	const uint32_t myN = myWarps * 32u;
+	const uint32_t ownBase = firstWarp * 32u;
+	const uint32_t updWarps = min(myWarps, warpsPerBlock);
 	const size_t listStride = size_t(B) * ownN;  /* one parity of the lists */
 	int2* acc32 = reinterpret_cast<int2*>(net.acc);
 	const uint2* region = net.fcm + net.regionBase[b];
@@ -446,7 +532,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		for(uint32_t x = tid; x < total; x += blockDim.x) {
 			const uint32_t s = x / ownN, l = x - s * ownN;
 			const size_t n = size_t(ownBase) + l;
-			sAcc[x] = n < nDev ? acc32[size_t(s) * nDev + n] : make_int2(0, 0);
+			sAcc[x] = l < myN ? acc32[size_t(s) * nDev + n] : make_int2(0, 0);
 		}
 	}
 
@@ -475,40 +561,20 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			if(warp == 1 && net.stdp) warpPrefix(net.postCnt + par * B, B, sPreP, lane);
 		}
 		__syncthreads();
-		unsigned long long* trace = A.trace ? A.trace + (size_t(k) * B + b) * 5u : nullptr;
+		unsigned long long* trace = A.trace ? A.trace + (size_t(k) * B + b) * TRACE_WORDS : nullptr;
 		if(trace && tid == 0) trace[0] = globalTimer();
 
-		if(doPrev && net.deliver) {
-			/* ---- urgent gather of cycle t-1: the delay-1 synapses (a
-			 * prefix of every segment) feed the update of cycle t ---- */
-			const uint32_t F = sPreF[B];
-			const uint32_t* flist = net.firedList + ((t - 1u) & 1u) * listStride;
-			uint32_t pushed = 0;
-			for(uint32_t j = tid; j < F; j += blockDim.x) {
-				const uint32_t bb = findList(sPreF, B, j);
-				const uint32_t s = flist[size_t(bb) * ownN + (j - sPreF[bb])];
-				const uint32_t beg = net.segOff[size_t(s) * B + b];
-				const uint32_t end = net.segOff[size_t(s + 1u) * B + b];
-				for(uint32_t q = beg; q < end; ++q) {
-					const uint2 r = region[q];
-					if(r.x & 63u) break;
-					gatherAdd<SMEM>(net, sAcc, ownN, ownBase, slotT, r);
-					++pushed;
-				}
-			}
-			pushed = __reduce_add_sync(FULL, pushed);
-			if(lane == 0 && pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
-		}
-		__syncthreads();
-		if(trace && tid == 0) trace[1] = globalTimer();
-
-		/* ---- neuron update of cycle t for the owned neurons ---- */
-		if(doUpdate) {
+		/* ---- neuron update of cycle t for the owned neurons, by the first
+		 * updWarps warps; the other warps start on the deferred work below
+		 * at once. The current of cycle t is its slot plus the delay-1
+		 * inbox filled when the sources fired ---- */
+		if(warp < updWarps && doUpdate) {
 			const uint32_t par = t & 1u;
 			const uint64_t* rfIn = net.rf + (t & 1u) * nDev;
 			uint64_t* rfOut = net.rf + ((t + 1u) & 1u) * nDev;
 			uint32_t* firedOut = net.firedList + par * listStride + size_t(b) * ownN;
 			uint2* postOut = net.postList + par * listStride + size_t(b) * ownN;
+			uint32_t pushed = 0;
 			for(uint32_t lw = warp; lw < myWarps; lw += warpsPerBlock) {
 				const uint32_t dw = firstWarp + lw;
 				int gi = 0;
@@ -517,33 +583,51 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const uint32_t n = dw * 32u + lane;
 				const uint32_t i = n - G.devBase;
 				const bool valid = i < G.count;
-				const uint32_t stimWord = takeStimWord(net, n, lane);
+				/* the firing-stimulus word is cleared after the model has
+				 * issued its loads, so that nothing orders them behind it */
+				uint32_t stimWord = lane == 0 ? net.fstim[dw] : 0u;
+				stimWord = __shfl_sync(FULL, stimWord, 0);
 				/* operands needed after the update, loaded with its own */
 				const uint64_t rfPrev = valid ? rfIn[n] : 0ull;
-				const uint32_t deg = valid ? net.outDegree[n] : 0u;
+				const uint32_t deg = valid ? __ldg(&net.outDegree[n]) : 0u;
 				uint2 rcm = make_uint2(0u, 0u);
-				if(valid && net.stdp) rcm = make_uint2(net.rcmStart[n], net.rcmStart[n + 1]);
-				float E, I;
+				if(valid && net.stdp) rcm = make_uint2(__ldg(&net.rcmStart[n]), __ldg(&net.rcmStart[n + 1]));
+				uint2 d1 = make_uint2(0u, 0u);
+				if(valid && net.deliver) d1 = make_uint2(__ldg(&net.d1Start[n]), __ldg(&net.d1Start[n + 1]));
+				long long e, in;
+				takeInbox(net, par, n, e, in);
 				if(SMEM) {
 					int2* cell = &sAcc[slotT * ownN + lw * 32u + lane];
 					const int2 a = *cell;
 					*cell = make_int2(0, 0);
-					E = wfxToFloat(a.x, net.fbits);
-					I = wfxToFloat(a.y, net.fbits);
+					e += a.x;
+					in += a.y;
 				} else {
-					takeCurrents(net, slotT, n, E, I);
+					long long se, si;
+					takeSlot(net, slotT, n, se, si);
+					e += se;
+					in += si;
 				}
+				const float E = wfxToFloat(e, net.fbits);
+				const float I = wfxToFloat(in, net.fbits);
 				bool fired = false;
 				if(valid) {
 					const bool stim = (stimWord >> lane) & 1u;
 					switch(G.kind) {
-						case 0: fired = modelIzhikevich(net, G, i, n, E, I, stim); break;
+						case 0: {
+							/* the first cycle of a launch draws its noise here;
+							 * later ones use the draw made in the phase before */
+							const float nz = k == 0 ? drawNoise(net, G, i) : net.noise[par * nDev + n];
+							fired = modelIzhikevich(net, G, i, n, E, I, stim, nz);
+							break;
+						}
 						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
 						case 2: fired = modelQif(net, G, i, n, E, I, stim); break;
 						case 4: fired = modelPoisson(net, G, i, n, E, I, stim); break;
 						default: fired = modelInput(net, G, i, n, E, I, stim); break;
 					}
 				}
+				if(lane == 0 && stimWord) net.fstim[dw] = 0u;
 				const uint64_t rfNew = (rfPrev << 1) | uint64_t(fired);
 				if(valid) {
 					rfOut[n] = rfNew;
@@ -551,16 +635,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const uint32_t word = __ballot_sync(FULL, fired);
 				if(lane == 0) {
 					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
-				}
-				if(word) {
-					uint32_t base = 0;
-					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
-					base = __shfl_sync(FULL, base, 0);
-					if(fired) {
-						firedOut[base + __popc(word & lt)] = n;
-					}
-					const uint32_t ev = __reduce_add_sync(FULL, fired ? deg : 0u);
-					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
 				}
 				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
@@ -575,14 +649,36 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						}
 					}
 				}
+				if(word) {
+					uint32_t base = 0;
+					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
+					base = __shfl_sync(FULL, base, 0);
+					if(fired) {
+						firedOut[base + __popc(word & lt)] = n;
+					}
+					const uint32_t ev = __reduce_add_sync(FULL, fired ? deg : 0u);
+					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
+					if(net.deliver) {
+						pushed += pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
+					}
+				}
+				/* in the first phase the noise of the next cycle is drawn by
+				 * the warp that just advanced the generator (later phases
+				 * draw it in work units below) */
+				if(k == 0 && k + 1 < A.cycles && G.kind == 0 && valid) {
+					net.noise[(par ^ 1u) * nDev + n] = drawNoise(net, G, i);
+				}
 			}
-			if(trace && lane == 0 && warp < myWarps) atomicMax(&trace[2], globalTimer());
+			pushed = __reduce_add_sync(FULL, pushed);
+			if(lane == 0 && pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
+			if(trace && lane == 0) atomicMax(&trace[2], globalTimer());
 		}
 
-		/* ---- overlapped with the update: the deferred gather of cycle t-1
-		 * (delays >= 2, into slots of cycles > t) and the STDP accumulation
-		 * of cycle t-1, as units handed out by a block counter so that warps
-		 * without neurons to update start at once. Units [0, G): 32 fired
+		/* ---- overlapped with the update: the gather of cycle t-1 (the
+		 * regions hold delays >= 2 only, which go into slots of cycles > t;
+		 * delay 1 went to the inbox when the sources fired) and the STDP accumulation of cycle t-1, as units
+		 * handed out by a block counter so that warps without neurons to
+		 * update start at once. Units [0, G): 32 fired
 		 * sources each; units [G, G + S): this block's share of the grid's
 		 * 128-synapse STDP items (item u * B + b) ---- */
 		if(doPrev) {
@@ -593,6 +689,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const uint32_t chunks = net.stdpChunks;
 			const uint32_t items = P * chunks;
 			const uint32_t Sb = items > b ? (items - b + B - 1u) / B : 0u;
+			/* units [G, G + NW): the next cycle's noise of one owned neuron
+			 * warp each (from the second phase of a launch on) */
+			const uint32_t NW = (k + 1u < A.cycles) ? myWarps : 0u;
 			const uint32_t* flist = net.firedList + par * listStride;
 			const uint2* plist = net.postList + par * listStride;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
@@ -603,37 +702,71 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				uint32_t u = 0;
 				if(lane == 0) u = atomicAdd(&sWork, 1u);
 				u = __shfl_sync(FULL, u, 0);
-				if(u >= G + Sb) break;
+				if(u >= G + NW + Sb) break;
+				const unsigned long long u0 = trace ? globalTimer() : 0ull;
 				if(u < G) {
+					/* 32 fired sources, one per lane; their segments of this
+					 * block's region are worked off as one concatenation so
+					 * that a warp's loads fall on few lines */
 					const uint32_t j = u * 32u + lane;
+					uint32_t beg = 0, cnt = 0;
 					if(j < F) {
 						const uint32_t bb = findList(sPreF, B, j);
 						const uint32_t s = flist[size_t(bb) * ownN + (j - sPreF[bb])];
-						const uint32_t beg = net.segOff[size_t(s) * B + b];
-						const uint32_t end = net.segOff[size_t(s + 1u) * B + b];
-						for(uint32_t q = beg; q < end; q += 4u) {
-							uint2 r[4];
+						const uint32_t* row = net.segOff + size_t(b) * (nDev + 1u) + s;
+						beg = row[0];
+						cnt = row[1] - beg;
+					}
+					uint32_t incl = cnt;
 #pragma unroll
-							for(int x = 0; x < 4; ++x) {
-								r[x] = q + x < end ? region[q + x] : make_uint2(0u, 0u);
+					for(int d = 1; d < 32; d <<= 1) {
+						const uint32_t x = __shfl_up_sync(FULL, incl, d);
+						if(lane >= uint32_t(d)) incl += x;
+					}
+					const uint32_t total = __shfl_sync(FULL, incl, 31);
+					const uint32_t excl = incl - cnt;
+					pushed += lane == 0 ? total : 0u;
+					for(uint32_t base = 0; base < total; base += 128u) {
+						uint2 r[4];
+#pragma unroll
+						for(int x = 0; x < 4; ++x) {
+							const uint32_t idx = base + uint32_t(x) * 32u + lane;
+							/* the lane whose range holds idx: the last with excl <= idx */
+							uint32_t lo = 0;
+#pragma unroll
+							for(uint32_t step = 16; step; step >>= 1) {
+								const uint32_t e = __shfl_sync(FULL, excl, lo + step);
+								if(e <= idx) lo += step;
 							}
+							const uint32_t eL = __shfl_sync(FULL, excl, lo);
+							const uint32_t bL = __shfl_sync(FULL, beg, lo);
+							r[x] = idx < total ? region[bL + (idx - eL)] : make_uint2(0u, 0u);
+						}
 #pragma unroll
-							for(int x = 0; x < 4; ++x) {
-								/* delay 1 was added by the urgent gather */
-								if(q + x < end && (r[x].x & 63u)) {
-									uint32_t slot = slotPrev + (r[x].x & 63u) + 1u;
-									slot = slot >= net.slots ? slot - net.slots : slot;
-									gatherAdd<SMEM>(net, sAcc, ownN, ownBase, slot, r[x]);
-									++pushed;
-								}
+						for(int x = 0; x < 4; ++x) {
+							if(base + uint32_t(x) * 32u + lane < total) {
+								uint32_t slot = slotPrev + (r[x].x & 63u) + 1u;
+								slot = slot >= net.slots ? slot - net.slots : slot;
+								gatherAdd<SMEM>(net, sAcc, ownN, ownBase, slot, r[x]);
 							}
 						}
+					}
+				} else if(u < G + NW) {
+					const uint32_t lw = u - G;
+					const uint32_t dw = firstWarp + lw;
+					int gi = 0;
+					while(dw >= A.groupWarp[gi + 1]) ++gi;
+					const GroupDev& Gr = A.groups[gi];
+					const uint32_t n = dw * 32u + lane;
+					const uint32_t i = n - Gr.devBase;
+					if(Gr.kind == 0 && i < Gr.count) {
+						net.noise[((t + 1u) & 1u) * nDev + n] = drawNoise(net, Gr, i);
 					}
 				} else {
 					/* STDP (ConnectivityMatrix.cpp:224-258): targets that
 					 * fired P cycles before cycle t-1; every accumulator has
 					 * one writer */
-					const uint32_t it = (u - G) * B + b;
+					const uint32_t it = (u - G - NW) * B + b;
 					const uint32_t tg = it / chunks;
 					const uint32_t off = (it - tg * chunks) * 128u;
 					const uint32_t bb = findList(sPreP, B, tg);
@@ -668,6 +801,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						}
 					}
 				}
+				if(trace) {
+					__syncwarp();
+					if(lane == 0) {
+						atomicAdd(&trace[u < G ? 5 : 6], globalTimer() - u0);
+						atomicAdd(&trace[u < G ? 7 : 8], 1ull);
+					}
+				}
 			}
 			pushed = __reduce_add_sync(FULL, pushed);
 			if(lane == 0) {
@@ -700,13 +840,33 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		if(trace && tid == 0) trace[4] = globalTimer();
 	}
 
+	/* the delay-1 arrivals for the cycle after the launch go into its slot,
+	 * so that between launches every spike fired is in the current slots */
+	{
+		__syncthreads();
+		const uint64_t tEnd = A.firstCycle + A.cycles;
+		const uint32_t slotEnd = uint32_t(tEnd % net.slots);
+		for(uint32_t l = tid; l < myN; l += blockDim.x) {
+			const uint32_t n = ownBase + l;
+			long long e, in;
+			takeInbox(net, uint32_t(tEnd) & 1u, n, e, in);
+			if(e | in) {
+				if(SMEM) {
+					int2* cell = &sAcc[slotEnd * ownN + l];
+					*cell = make_int2(cell->x + int(e), cell->y + int(in));
+				} else {
+					addSlot(net, slotEnd, n, e, in);
+				}
+			}
+		}
+	}
 	if(SMEM) {
 		__syncthreads();
 		const uint32_t total = net.slots * ownN;
 		for(uint32_t x = tid; x < total; x += blockDim.x) {
 			const uint32_t s = x / ownN, l = x - s * ownN;
 			const size_t n = size_t(ownBase) + l;
-			if(n < nDev) acc32[size_t(s) * nDev + n] = sAcc[x];
+			if(l < myN) acc32[size_t(s) * nDev + n] = sAcc[x];
 		}
 	}
 }
@@ -926,15 +1086,16 @@ launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, u
 }
 
 /* The step kernel's plan: one 1024-thread block per SM (its registers allow
- * no more), each owning ceil(warps / blocks) neuron warps; the owned current
- * slots go to shared memory when they are int32 and fit. */
+ * no more), the neuron warps split as evenly as possible over the blocks; the
+ * owned current slots go to shared memory when they are int32 and fit. */
 void
-cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownWarps, bool* smemAcc)
+cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
+		bool* smemAcc)
 {
 	uint32_t B = uint32_t(smCount());
 	if(B > MAX_BLOCKS) B = MAX_BLOCKS;
-	uint32_t own = (totalWarps + B - 1) / B;
-	if(own == 0) own = 1;
+	const uint32_t q = totalWarps / B, r = totalWarps % B;
+	const uint32_t own = q + (r ? 1u : 0u);
 	const uint64_t bytes = uint64_t(slots) * own * 32u * 8u;
 	const bool smem = acc32 && bytes <= SMEM_ACC_LIMIT;
 	int perSm = 0;
@@ -947,7 +1108,8 @@ cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, ui
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false>, BLOCK, 0);
 	}
 	*blocks = perSm >= 1 ? B : 0u;
-	*ownWarps = own;
+	*ownQ = q;
+	*ownR = r;
 	*smemAcc = smem;
 }
 

@@ -12,23 +12,24 @@
  *
  * The step path is one persistent cooperative kernel (k_cycles) over one
  * block per SM, with one grid barrier per cycle. Block b owns a contiguous
- * range of ownWarps x 32 neurons: it updates them, and it alone adds spikes
+ * range of 32-neuron warps (ownerOf below): it updates them, and it alone adds spikes
  * into their current slots, which it keeps in shared memory for the whole
  * launch (or in global memory when they do not fit). The forward matrix is
- * partitioned to match: region b holds, source by source, the synapses whose
- * target block b owns, each (source, region) segment sorted by delay. Phase t:
- *   - urgent gather: every block reads the fired sources of cycle t-1 (all
- *     blocks' lists) and, for each, the delay-1 prefix of its segment of
- *     region b, adding each weight into slot t mod Q of the target (E or I
- *     by sign);
- *   - neuron update of cycle t from slot t mod Q: firing history, bitmap,
- *     the fired and post-spiking lists of cycle t; overlapped with
- *   - the deferred gather of cycle t-1 (delays >= 2, into slots (t-1+d)
- *     mod Q) and the STDP accumulation of cycle t-1 over all blocks'
+ * partitioned to match: region b holds, source by source, the synapses of
+ * delay >= 2 whose target block b owns; the delay-1 synapses follow, grouped
+ * by source. Phase t:
+ *   - neuron update of cycle t from slot t mod Q plus the delay-1 inbox of
+ *     cycle t: firing history, bitmap, the fired and post-spiking lists of
+ *     cycle t; each fired neuron's delay-1 synapses are added at once into
+ *     the inbox of cycle t+1 (global reductions; 5% of the synapses for
+ *     delays U{1..20}); overlapped with
+ *   - the gather of cycle t-1: every block reads the fired sources of cycle
+ *     t-1 (all blocks' lists) and, for each, its segment of region b, adding
+ *     each weight of delay d >= 2 into slot (t-1+d) mod Q of the target (E or
+ *     I by sign), and the STDP accumulation of cycle t-1 over all blocks'
  *     post-spiking targets, dealt out over the grid in 128-synapse items.
- *     Together the two gathers are the reference's deliverSpikes at cycle
- *     t-1+d (src/nemo/cpu/Simulation.cpp:259-308), done one cycle after the
- *     firing;
+ *     Together the inbox and the gather are the reference's deliverSpikes at
+ *     cycle t0+d (src/nemo/cpu/Simulation.cpp:259-308);
  *   - grid barrier.
  * A final phase gathers and learns for the last cycle, so that between
  * launches every spike fired is in the current slots. Integer sums are exact
@@ -56,20 +57,27 @@ struct NetDev {
 	uint32_t fbits;         /* fractional bits of the Q(31-f).f weights */
 	int deliver;            /* 0 when no delay is deliverable (max delay 64) */
 
-	/* ownership: block b of the step kernel owns neurons
-	 * [b * ownWarps * 32, (b + 1) * ownWarps * 32) */
+	/* ownership: with q = warps / blocks and r = warps % blocks, block b owns
+	 * the q + (b < r) neuron warps from b * q + min(b, r) (ownFirst); ownWarps
+	 * = q + (r > 0) is the most any block owns */
 	uint32_t blocks;
 	uint32_t ownWarps;
+	uint32_t ownQ;
+	uint32_t ownR;
 	int smemAcc;            /* current slots of the owned neurons in shared memory */
 
-	/* forward connectivity, partitioned by target owner: region b =
-	 * [regionBase[b], regionBase[b+1]); within it the synapses of source s
-	 * are [segOff[s * blocks + b], segOff[(s + 1) * blocks + b]), sorted by
-	 * delay */
+	/* forward connectivity. Delays >= 2, partitioned by target owner:
+	 * region b = [regionBase[b], regionBase[b+1]); within it the synapses of
+	 * source s are [segOff[b][s], segOff[b][s + 1]) (rows of nDev + 1, so
+	 * that a segment's two ends share a line).
+	 * Delay 1, by source: [d1Base + d1Start[s], d1Base + d1Start[s+1]) */
 	uint2* fcm;                    /* {target << 6 | (delay - 1), int32 weight} */
 	const uint64_t* regionBase;    /* [blocks + 1] */
-	const uint32_t* segOff;        /* [(nDev + 1) * blocks] */
+	const uint32_t* segOff;        /* [blocks][nDev + 1] */
 	const uint32_t* outDegree;     /* [nDev] synapses per source */
+	const uint32_t* d1Start;       /* [nDev + 1] */
+	uint64_t d1Base;
+	void* inbox;                   /* [2][nDev][2] delay-1 arrivals by cycle parity (as acc) */
 
 	void* acc;                     /* [slots][nDev][2] E, I current of a future cycle (int32 or int64) */
 	uint64_t* rf;                  /* [2][nDev] firing history, bit 0 = last cycle */
@@ -77,6 +85,7 @@ struct NetDev {
 	unsigned long long* eventsRing;/* [ring] synaptic events (fired x out-degree) */
 	uint32_t* firedCountRing;      /* [ring] */
 	float* ext;                    /* [nDev] external current, cleared after use */
+	float* noise;                  /* [2][nDev] Izhikevich noise of the next cycle, by cycle parity */
 	uint32_t* fstim;               /* [nWords] firing stimulus, cleared after use */
 
 	/* per-cycle lists by cycle parity and block, [2][blocks][ownWarps * 32],
@@ -139,9 +148,10 @@ struct CycleArgs {
 	uint64_t firstCycle;
 	uint32_t cycles;
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
-	/* optional phase timestamps (%globaltimer ns), [cycles + 1][block][5]:
-	 * phase start, urgent gather done, last update warp done (0 when the
-	 * block updates nothing), all work done, barrier passed */
+	/* optional phase trace (%globaltimer ns), [cycles + 1][block][9]: phase
+	 * start, (unused), last update warp done (0 when the block updates
+	 * nothing), all work done, barrier passed; then the summed durations of
+	 * the block's gather units and STDP units, and their counts */
 	unsigned long long* trace;
 };
 
@@ -168,13 +178,29 @@ int noallocScratch(int device, uint32_t** ptr);
 void launchStimulus(const NetDev& net, const StimDev& stim, void* stream);
 /* Stimulus from the allocation-free scratch (layout in kernels.cu). */
 void launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, uint32_t ni, void* stream);
+#ifdef __CUDACC__
+#define NEMO_HD __host__ __device__
+#else
+#define NEMO_HD
+#endif
+
+/* First neuron warp owned by block b, and the block owning neuron warp w */
+NEMO_HD inline uint32_t ownFirst(uint32_t b, uint32_t q, uint32_t r) { return b * q + (b < r ? b : r); }
+NEMO_HD inline uint32_t ownerOf(uint32_t w, uint32_t q, uint32_t r)
+{
+	const uint32_t big = r * (q + 1u);
+	return w < big ? w / (q + 1u) : r + (w - big) / q;
+}
+
 /* Cooperative launch of k_cycles (grid and shared memory from args.net). */
 void launchCycles(const CycleArgs& args, void* stream);
 /* The step kernel's grid (one block per SM, at most MAX_BLOCKS; 0 when the
- * kernel cannot be resident), the warps each block owns, and whether the
- * owned current slots fit in shared memory (`slots` slots of 8-byte int32 E/I
- * pairs; int64 sums use global memory). */
-void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownWarps, bool* smemAcc);
+ * kernel cannot be resident), the split of the neuron warps over its blocks
+ * (q, r: see NetDev), and whether the owned current slots fit in shared
+ * memory (`slots` slots of 8-byte int32 E/I pairs; int64 sums use global
+ * memory). */
+void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
+		bool* smemAcc);
 void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow, void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);

@@ -249,9 +249,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		}
 	}
 
-	uint32_t ownWarps = 1;
+	uint32_t ownQ = 0, ownR = 0;
 	bool smemAcc = false;
-	cyclesPlan(m_nDev / 32, slots, acc32, &m_blocks, &ownWarps, &smemAcc);
+	cyclesPlan(m_nDev / 32, slots, acc32, &m_blocks, &ownQ, &ownR, &smemAcc);
+	const uint32_t ownWarps = ownQ + (ownR ? 1u : 0u);
 	NEMO_CUDA(cudaGetLastError());
 	if(m_blocks == 0) {
 		fail(NEMO_CUDA_INVOCATION_ERROR, "The step kernel cannot be resident on this device");
@@ -259,11 +260,13 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	const uint32_t B = m_blocks;
 	const uint32_t ownN = ownWarps * 32;
 
-	/* ---- forward matrix partitioned by target owner: region b holds, source
-	 * by source, the synapses whose target block b owns; within a (source,
-	 * region) segment by delay, then insertion order ---- */
+	/* ---- forward matrix: the synapses of delay >= 2 partitioned by target
+	 * owner (region b holds, source by source, those whose target block b
+	 * owns, in insertion order within a segment), then the delay-1
+	 * synapses grouped by source (pushed at firing) ---- */
 	std::vector<uint64_t> regionBase(size_t(B) + 1, 0);
 	std::vector<uint32_t> segOff((size_t(m_nDev) + 1) * B, 0);
+	std::vector<uint32_t> d1Start(size_t(m_nDev) + 1, 0);
 	std::vector<uint2> fcm(S);
 	std::vector<uint32_t> fcmPos(S);
 	std::vector<uint32_t> synAt(S);   /* synapse at each forward position */
@@ -271,33 +274,32 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		/* cursor[b][s]: count, then next free offset within region b */
 		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
-			cursor[size_t(dtgt[s] / ownN) * m_nDev + dsrc[s]]++;
+			if(net.dly[s] == 1) d1Start[dsrc[s] + 1]++;
+			else cursor[size_t(ownerOf(dtgt[s] / 32, ownQ, ownR)) * m_nDev + dsrc[s]]++;
 		}
 		for(uint32_t b = 0; b < B; ++b) {
 			uint32_t* c = &cursor[size_t(b) * m_nDev];
 			uint64_t run = 0;
 			for(uint32_t src = 0; src < m_nDev; ++src) {
-				segOff[size_t(src) * B + b] = uint32_t(run);
+				segOff[size_t(b) * (m_nDev + 1) + src] = uint32_t(run);
 				uint32_t k = c[src];
 				c[src] = uint32_t(run);
 				run += k;
 			}
-			segOff[size_t(m_nDev) * B + b] = uint32_t(run);
+			segOff[size_t(b) * (m_nDev + 1) + m_nDev] = uint32_t(run);
 			regionBase[b + 1] = regionBase[b] + run;
 		}
-		/* filled in order of delay (stable), so that every segment is sorted
-		 * by delay and its delay-1 synapses are a prefix */
-		std::vector<uint32_t> byDelay(S);
-		{
-			std::vector<uint64_t> at(66, 0);
-			for(size_t s = 0; s < S; ++s) at[net.dly[s] + 1]++;
-			for(size_t d = 1; d < at.size(); ++d) at[d] += at[d - 1];
-			for(size_t s = 0; s < S; ++s) byDelay[at[net.dly[s]]++] = uint32_t(s);
-		}
-		for(size_t k = 0; k < S; ++k) {
-			const size_t s = byDelay[k];
-			const uint32_t b = dtgt[s] / ownN;
-			const uint64_t pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
+		for(uint32_t n = 0; n < m_nDev; ++n) d1Start[n + 1] += d1Start[n];
+		std::vector<uint32_t> d1Fill(d1Start.begin(), d1Start.end() - 1);
+		const uint64_t d1Base = regionBase[B];
+		for(size_t s = 0; s < S; ++s) {
+			uint64_t pos;
+			if(net.dly[s] == 1) {
+				pos = d1Base + d1Fill[dsrc[s]]++;
+			} else {
+				const uint32_t b = ownerOf(dtgt[s] / 32, ownQ, ownR);
+				pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
+			}
 			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(wfx[s]));
 			fcmPos[s] = uint32_t(pos);
 			synAt[pos] = uint32_t(s);
@@ -366,17 +368,23 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.deliver = deliver ? 1 : 0;
 	m_net.blocks = B;
 	m_net.ownWarps = ownWarps;
+	m_net.ownQ = ownQ;
+	m_net.ownR = ownR;
 	m_net.smemAcc = smemAcc ? 1 : 0;
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
 	m_net.regionBase = (const uint64_t*) put(regionBase.data(), regionBase.size() * 8);
 	m_net.segOff = (const uint32_t*) put(segOff.data(), segOff.size() * 4);
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
+	m_net.d1Start = (const uint32_t*) put(d1Start.data(), d1Start.size() * 4);
+	m_net.d1Base = regionBase[B];
+	m_net.inbox = alloc(size_t(2) * m_nDev * (acc32 ? 8 : 16));
 	m_net.acc = alloc(size_t(slots) * m_nDev * (acc32 ? 8 : 16));
 	m_net.rf = (uint64_t*) alloc(size_t(2) * m_nDev * 8);
 	m_net.firedRing = (uint32_t*) alloc(size_t(m_ring) * m_net.nWords * 4);
 	m_net.eventsRing = (unsigned long long*) alloc(size_t(m_ring) * 8);
 	m_net.firedCountRing = (uint32_t*) alloc(size_t(m_ring) * 4);
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
+	m_net.noise = (float*) alloc(size_t(2) * m_nDev * 4);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
 	m_net.stats = (unsigned long long*) alloc(4 * 8);
 	m_net.barrier = (unsigned*) alloc(4 * 4);
@@ -1038,13 +1046,13 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 }
 
 void
-Simulation::trace(unsigned cycles, double out[10])
+Simulation::trace(unsigned cycles, double out[14])
 {
 	if(cycles == 0) {
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");
 	}
 	cudaStream_t stream = STREAM(m_stream);
-	const unsigned S = 5;
+	const unsigned S = 9;
 	size_t words = size_t(cycles + 1) * m_blocks * S;
 	unsigned long long* dTrace;
 	NEMO_CUDA(cudaMalloc(&dTrace, words * 8));
@@ -1064,38 +1072,47 @@ Simulation::trace(unsigned cycles, double out[10])
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	cudaFree(dTrace);
 	checkDeviceError();
-	double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+	double acc[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+	double gNs = 0, gN = 0, sNs = 0, sN = 0;
 	for(unsigned k = 0; k < cycles; ++k) {
-		double minT0 = 1e300, maxT4 = 0, maxG = 0, sumG = 0, maxU = 0, sumU = 0, maxW = 0, sumW = 0,
+		double minT0 = 1e300, maxT4 = 0, maxU = 0, sumU = 0, maxA = 0, sumA = 0, maxR = 0, sumR = 0,
 				maxT3 = 0, minT3 = 1e300, sumT4 = 0;
 		for(unsigned b = 0; b < m_blocks; ++b) {
 			const unsigned long long* r = &h[(size_t(k) * m_blocks + b) * S];
-			double t0 = double(r[0]), t1 = double(r[1]), t2 = double(r[2]), t3 = double(r[3]), t4 = double(r[4]);
-			if(r[2] == 0) t2 = t1;   /* the block updates nothing */
+			double t0 = double(r[0]), t2 = double(r[2]), t3 = double(r[3]), t4 = double(r[4]);
+			if(r[2] == 0) t2 = t0;   /* the block updates nothing */
 			minT0 = std::min(minT0, t0);
 			maxT4 = std::max(maxT4, t4);
-			maxG = std::max(maxG, t1 - t0);
-			sumG += t1 - t0;
-			maxU = std::max(maxU, t2 - t1);
-			sumU += t2 - t1;
-			maxW = std::max(maxW, t3 - t1);
-			sumW += t3 - t1;
+			maxU = std::max(maxU, t2 - t0);
+			sumU += t2 - t0;
+			maxA = std::max(maxA, t3 - t0);
+			sumA += t3 - t0;
+			maxR = std::max(maxR, t3 - t2);
+			sumR += t3 - t2;
 			maxT3 = std::max(maxT3, t3);
 			minT3 = std::min(minT3, t3);
 			sumT4 += t4;
+			gNs += double(r[5]);
+			sNs += double(r[6]);
+			gN += double(r[7]);
+			sN += double(r[8]);
 		}
 		acc[0] += maxT4 - minT0;
-		acc[1] += maxG;
-		acc[2] += sumG / m_blocks;
-		acc[3] += maxU;
-		acc[4] += sumU / m_blocks;
+		acc[1] += maxU;
+		acc[2] += sumU / m_blocks;
+		acc[3] += maxA;
+		acc[4] += sumA / m_blocks;
 		acc[5] += maxT3 - minT0;
 		acc[6] += sumT4 / m_blocks - maxT3;
 		acc[7] += maxT3 - minT3;
-		acc[8] += maxW;
-		acc[9] += sumW / m_blocks;
+		acc[8] += maxR;
+		acc[9] += sumR / m_blocks;
 	}
 	for(int i = 0; i < 10; ++i) out[i] = acc[i] / cycles;
+	out[10] = gN ? gNs / gN : 0.0;
+	out[11] = sN ? sNs / sN : 0.0;
+	out[12] = gN / (double(cycles) * m_blocks);
+	out[13] = sN / (double(cycles) * m_blocks);
 }
 
 uint64_t

@@ -90,12 +90,13 @@ public:
 	void readStats(uint64_t out[4]);
 
 	/* Phase timing of one traced persistent launch of `cycles` cycles, means
-	 * over cycles in ns: [0] phase (first start to last barrier exit),
-	 * [1] max / [2] mean block urgent gather, [3] max / [4] mean block
-	 * update, [5] first start to last block done, [6] last arrival to mean
-	 * barrier exit, [7] spread of block arrivals, [8] max / [9] mean block
-	 * update with the overlapped deferred gather and STDP. */
-	void trace(unsigned cycles, double out[10]);
+	 * over cycles in ns: [0] phase, [1] max / [2] mean block update with the
+	 * delay-1 push, [3] max / [4] mean block work, [5] first start to last
+	 * block done, [6] last arrival to mean barrier exit, [7] spread of block
+	 * arrivals, [8] max / [9] mean block work after its update, [10] / [11]
+	 * mean duration of a gather / STDP unit, [12] / [13] such units per block
+	 * and cycle. */
+	void trace(unsigned cycles, double out[14]);
 
 private:
 	struct Group {
