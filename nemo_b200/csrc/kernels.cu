@@ -495,7 +495,10 @@ __device__ __forceinline__ void gatherAdd(const NetDev& net, int2* sAcc, uint32_
 	}
 }
 
-/* k_cycles: see kernels.hpp for the phase structure. SMEM: the owned current
+/* k_cycles: see kernels.hpp for the phase structure. The forward regions and
+ * the reverse-matrix arrays are streamed with evict-first loads and stores
+ * (__ldcs / __stcs), so that they do not push the randomly read firing
+ * history, segment offsets and noise tables out of L2. SMEM: the owned current
  * slots live in dynamic shared memory as int32 E/I pairs,
  * sAcc[slot * ownN + local]; otherwise every access goes to net.acc. */
 template<bool SMEM>
@@ -659,7 +662,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t ev = __reduce_add_sync(FULL, fired ? deg : 0u);
 					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
 					if(net.deliver) {
-						pushed += pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
+						const uint32_t np = pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
+						pushed += lane == 0 ? np : 0u;   /* warp total, counted once */
 					}
 				}
 				/* in the first phase the noise of the next cycle is drawn by
@@ -740,7 +744,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							}
 							const uint32_t eL = __shfl_sync(FULL, excl, lo);
 							const uint32_t bL = __shfl_sync(FULL, beg, lo);
-							r[x] = idx < total ? region[bL + (idx - eL)] : make_uint2(0u, 0u);
+							r[x] = idx < total ? __ldcs(&region[bL + (idx - eL)]) : make_uint2(0u, 0u);
 						}
 #pragma unroll
 						for(int x = 0; x < 4; ++x) {
@@ -779,7 +783,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 #pragma unroll
 						for(int x = 0; x < 4; ++x) {
 							const uint32_t jj = lane + 32u * x;
-							sd[x] = jj < cnt ? net.rcmSrcDelay[b0 + jj] : 0u;
+							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
 						}
 						uint64_t pre[4];
 						int32_t old[4];
@@ -787,7 +791,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						for(int x = 0; x < 4; ++x) {
 							const uint32_t jj = lane + 32u * x;
 							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
-							old[x] = jj < cnt ? net.rcmAcc[b0 + jj] : 0;
+							old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
 						}
 #pragma unroll
 						for(int x = 0; x < 4; ++x) {
@@ -795,7 +799,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							if(jj < cnt) {
 								const int32_t dw = weightChange(pre[x], A.rule);
 								if(dw != 0) {
-									net.rcmAcc[b0 + jj] = int32_t(uint32_t(old[x]) + uint32_t(dw));
+									__stcs(&net.rcmAcc[b0 + jj], int32_t(uint32_t(old[x]) + uint32_t(dw)));
 								}
 							}
 						}
@@ -955,45 +959,47 @@ __device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule
 		}
 	}
 	if(acc) {
-		net.rcmAcc[j] = 0;
+		__stcs(&net.rcmAcc[j], 0);
 	}
 }
 
-/* Items (target, 128-synapse chunk of its plastic synapses) in target order
- * over a grid-stride loop: the items in flight at any moment are consecutive,
- * so they rewrite only the few forward-matrix regions that own those targets
- * (each target's synapses lie in its owner's region, sorted by position),
- * which stay in L2 while they are rewritten. */
+/* Items (target, 128-synapse chunk of its plastic synapses) of the targets
+ * [t0, t1) over a grid-stride loop. The host launches one such kernel per
+ * group of consecutive owner blocks whose forward regions together fit
+ * comfortably in L2 (APPLY_GROUP_SYNAPSES): a target's plastic synapses all
+ * lie in its owner's region (or the delay-1 part), so every forward record a
+ * launch rewrites is loaded from DRAM once and reused from L2 by the other
+ * targets that share its sector. */
 __global__ void __launch_bounds__(256)
-k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow)
+k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint32_t t0, uint32_t t1)
 {
 	const uint64_t* rfNow = net.rf + size_t(cycleNow & 1u) * net.nDev;
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-	const uint32_t chunks = net.stdpChunks;
-	const uint64_t items = uint64_t(net.nDev) * chunks;
+	const uint32_t chunks = net.applyChunks;
+	const uint64_t items = uint64_t(t1 - t0) * chunks;
 	for(uint64_t it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nwarps) {
-		const uint32_t t = uint32_t(it / chunks);
-		const uint32_t c = uint32_t(it - uint64_t(t) * chunks);
-		const uint32_t b0 = net.rcmStart[t] + c * 128u;
+		const uint32_t t = t0 + uint32_t(it / chunks);
+		const uint32_t c = uint32_t(it % chunks);
+		const uint32_t b0 = net.rcmStart[t] + c * (32u * APPLY_PER_LANE);
 		const uint32_t e = net.rcmStart[t + 1];
 		if(b0 >= e) continue;
 		const uint32_t j = b0 + lane;
-		uint32_t f[4];
-		int32_t a[4];
+		uint32_t f[APPLY_PER_LANE];
+		int32_t a[APPLY_PER_LANE];
 #pragma unroll
-		for(int u = 0; u < 4; ++u) {
+		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			const uint32_t jj = j + 32u * u;
-			f[u] = jj < e ? net.rcmForward[jj] : 0u;
-			a[u] = jj < e ? net.rcmAcc[jj] : 0;
+			f[u] = jj < e ? __ldcs(&net.rcmForward[jj]) : 0u;
+			a[u] = jj < e ? __ldcs(&net.rcmAcc[jj]) : 0;
 		}
-		uint2 syn[4];
+		uint2 syn[APPLY_PER_LANE];
 #pragma unroll
-		for(int u = 0; u < 4; ++u) {
+		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			syn[u] = j + 32u * u < e ? net.fcm[f[u]] : make_uint2(0u, 0u);
 		}
 #pragma unroll
-		for(int u = 0; u < 4; ++u) {
+		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			const uint32_t jj = j + 32u * u;
 			if(jj < e) applyOne(net, rule, reward, cycleNow, rfNow, jj, f[u], a[u], syn[u]);
 		}
@@ -1128,15 +1134,32 @@ launchCycles(const CycleArgs& args, void* stream)
 	}
 }
 
-void
-launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow, void* stream)
+/* resident 256-thread blocks of k_apply_stdp per SM (one wave of the grid) */
+static uint32_t
+applyBlocksPerSm()
 {
-	/* one 128-synapse item per warp at a time, 64 warps per SM */
-	const uint64_t items = uint64_t(net.nDev) * net.stdpChunks;
-	uint64_t blocks = (items * 32 + 255) / 256;
-	const uint64_t cap = uint64_t(smCount()) * 8;
-	if(blocks > cap) blocks = cap;
-	k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow);
+	static int perSm = 0;
+	if(perSm == 0) {
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_apply_stdp, 256, 0);
+		if(perSm <= 0) perSm = 1;
+	}
+	return uint32_t(perSm);
+}
+
+void
+launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
+		const uint32_t* groupTargets, uint32_t groups, void* stream)
+{
+	for(uint32_t g = 0; g < groups; ++g) {
+		const uint32_t t0 = groupTargets[g], t1 = groupTargets[g + 1];
+		if(t1 <= t0) continue;
+		/* one item (32 x APPLY_PER_LANE synapses) per warp at a time */
+		const uint64_t items = uint64_t(t1 - t0) * net.applyChunks;
+		uint64_t blocks = (items * 32 + 255) / 256;
+		const uint64_t cap = uint64_t(smCount()) * applyBlocksPerSm();
+		if(blocks > cap) blocks = cap;
+		k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow, t0, t1);
+	}
 }
 
 void

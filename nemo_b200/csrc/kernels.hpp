@@ -45,6 +45,11 @@ const int MAX_GROUPS = 8;
 
 /* most blocks of the step kernel (static shared prefix arrays) */
 const uint32_t MAX_BLOCKS = 256;
+/* forward synapses per applyStdp launch: consecutive owner blocks are grouped
+ * until their regions hold this many (128 MB of records) */
+const uint64_t APPLY_GROUP_SYNAPSES = uint64_t(1) << 24;
+/* plastic synapses per lane in one applyStdp work item */
+const uint32_t APPLY_PER_LANE = 4;
 /* shared memory the step kernel may use for current slots */
 const uint32_t SMEM_ACC_LIMIT = 200 * 1024;
 
@@ -100,6 +105,7 @@ struct NetDev {
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
 	uint32_t stdpChunks;           /* 128-synapse chunks per target (max in-degree) */
+	uint32_t applyChunks;          /* (32 x APPLY_PER_LANE)-synapse chunks per target */
 	const uint32_t* rcmStart;      /* [nDev + 1] (fewer than 2^32 synapses) */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
 	const uint32_t* rcmForward;    /* index into fcm, ascending within a target */
@@ -201,7 +207,10 @@ void launchCycles(const CycleArgs& args, void* stream);
  * memory). */
 void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
 		bool* smemAcc);
-void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow, void* stream);
+/* applyStdp over target groups [groupTargets[g], groupTargets[g+1]), one
+ * launch per group (groups of owner blocks, see APPLY_GROUP_SYNAPSES) */
+void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
+		const uint32_t* groupTargets, uint32_t groups, void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);

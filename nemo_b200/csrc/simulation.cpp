@@ -306,6 +306,16 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		}
 	}
 
+	/* applyStdp launches: consecutive owner blocks grouped until their
+	 * regions hold APPLY_GROUP_SYNAPSES synapses, as target ranges */
+	m_applyGroups.assign(1, 0u);
+	for(uint32_t b = 0; b < B;) {
+		uint32_t e = b + 1;
+		while(e < B && regionBase[e + 1] - regionBase[b] <= APPLY_GROUP_SYNAPSES) ++e;
+		m_applyGroups.push_back(std::min(ownFirst(e, ownQ, ownR) * 32u, m_nDev));
+		b = e;
+	}
+
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
 	std::vector<uint32_t> rcmStart;
 	std::vector<uint32_t> rcmSrcDelay, rcmForward;
@@ -394,6 +404,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.postCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	m_net.stdp = m_stdpOn ? 1 : 0;
 	m_net.stdpChunks = uint32_t(stdpChunks);
+	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
 		m_net.rcmStart = (const uint32_t*) put(rcmStart.data(), rcmStart.size() * 4);
@@ -748,7 +759,7 @@ Simulation::applyStdp(float reward)
 		fail(NEMO_INVALID_INPUT, msg.str());
 	}
 	if(m_nrcm) {
-		launchApplyStdp(m_net, m_rule, fx, m_cycle, m_stream);
+		launchApplyStdp(m_net, m_rule, fx, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
 	}
 	m_fcmHostValid = false;
 }
@@ -982,7 +993,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 		launchBlock(m_cycle, cyclesPerStep);
 		m_cycle += cyclesPerStep;
 		if(apply && m_nrcm) {
-			launchApplyStdp(m_net, m_rule, fx, m_cycle, m_stream);
+			launchApplyStdp(m_net, m_rule, fx, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
 		}
 	}
 	NEMO_CUDA(cudaEventRecord(e1, stream));
@@ -1018,7 +1029,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	m_cycle += cycles;
 	NEMO_CUDA(cudaEventRecord(e1, stream));
 	if(m_stdpOn && m_nrcm) {
-		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_cycle, m_stream);
+		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
 		m_fcmHostValid = false;
 	}
 	NEMO_CUDA(cudaEventRecord(e2, stream));

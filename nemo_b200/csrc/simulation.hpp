@@ -142,6 +142,7 @@ private:
 	NetDev m_net;
 	CycleArgs m_args;
 	unsigned m_blocks;          /* grid of the persistent step kernel */
+	std::vector<uint32_t> m_applyGroups;  /* applyStdp launch target ranges (prefix) */
 	bool m_stdpOn;
 	StdpRule m_rule;
 	StdpFunction m_stdpFn;

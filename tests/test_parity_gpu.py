@@ -145,8 +145,8 @@ def test_mixed_models_with_stimulus(oracle_lib):
 
 
 def test_device_resident_run_matches_steps(oracle_lib):
-    """nemo_b200_run (CUDA graph of many cycles) gives the same trace as
-    stepping the oracle cycle by cycle."""
+    """nemo_b200_run (one persistent launch of many cycles) gives the same
+    trace as stepping the oracle cycle by cycle."""
     spec = netgen.izhikevich_random(1500, 100, dmax=20, seed=6, stdp=True)
     pre, post = netgen.standard_stdp()
     (_, g), (_, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 1.0, 0.0, -1.0)))
@@ -177,3 +177,24 @@ def test_device_resident_run_matches_steps(oracle_lib):
         g.apply_stdp(1.0)
         o.apply_stdp(1.0)
     assert np.array_equal(g.step(), o.step())
+
+
+@pytest.mark.parametrize("dmax", [1, 5, 20])
+def test_every_event_delivered_once(dmax):
+    """The kernel's own counters: over a device-resident run every synaptic
+    event (fired neuron x out-degree) is added into a current exactly once,
+    through the delay-1 inbox or the gather, for delays including 1."""
+    spec = netgen.izhikevich_random(3000, 200, dmax=dmax, seed=12, stdp=True)
+    lib = Library()
+    net = spec.build(Network(lib))
+    conf = Configuration(lib)
+    pre, post = netgen.standard_stdp()
+    conf.set_stdp_function(pre, post, 0.0, 1.0, 0.0, -1.0)
+    sim = Simulation(net, conf)
+    out = (ctypes.c_double * 4)()
+    lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                              ctypes.c_float, ctypes.c_double * 4]
+    lib.call("nemo_b200_timed_steps", sim.handle, 3, 100, 1, ctypes.c_float(1.0), out)
+    fired, events, delivered = out[1], out[2], out[3]
+    assert fired > 0
+    assert delivered == events
