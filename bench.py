@@ -202,13 +202,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def load_traffic(kernel, workload_name):
+    """DRAM bytes per launch of `kernel` on the workload, from the committed
+    ncu summary (a 1-pass dram__bytes_read.sum + dram__bytes_write.sum
+    capture of a full-size launch); None when there is none."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic_%s.md" % workload_name)
     if not os.path.exists(path):
         return None
-    t = json.load(open(path)).get(kernel)
-    return t
+    for line in open(path):
+        f = line.split()
+        if len(f) == 4 and f[0] == "traffic" and f[1] == kernel and f[2] == workload_name:
+            return float(f[3])
+    return None
 
 
 def roofline(sim, lib, wl):
@@ -239,7 +244,7 @@ def roofline(sim, lib, wl):
     dom = max(table, key=lambda k: table[k]["share"])
     d = table[dom]
     roof = {"kernel": dom, "bound": "hbm", "achieved": round(d["gbs"], 1), "peak": peak, "unit": "GB/s",
-            "frac": round(d["gbs"] / peak, 4), "peak_source": peak_kind, "traffic": load_traffic(dom),
+            "frac": round(d["gbs"] / peak, 4), "peak_source": peak_kind, "traffic": load_traffic(dom, wl["name"]),
             "bytes_per_launch": d["bytes_per_launch"], "ms_per_launch": d["ms_per_launch"],
             "per_kernel": {k: {kk: (round(vv, 5) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                            for k, v in table.items()},
