@@ -109,6 +109,17 @@ nemo_status_t nemo_b200_nrand_probe(nemo_simulation_t sim, const uint32_t u1[], 
  * host glibc (0 when the device reproduces the reference bit for bit). */
 nemo_status_t nemo_b200_libm_check(nemo_simulation_t sim, uint64_t* mismatches);
 
+/* Diagnostics: evaluate the device expf of the Hodgkin-Huxley model on every
+ * float in [-104, 89] (the range where expf is neither 0 nor infinity) and
+ * count the results that differ from the host glibc (0 when the device
+ * reproduces it bit for bit). */
+nemo_status_t nemo_b200_expf_check(nemo_simulation_t sim, uint64_t* mismatches);
+
+/* The host-built table of inputs on which glibc expf rounds differently from
+ * the device candidate: its size and its boundary distance (built or loaded
+ * from the cache on first use; no device needed). */
+nemo_status_t nemo_b200_expf_exceptions(size_t* count, double* tau);
+
 /* Path of the glibc correction-table cache file used by this process. */
 const char* nemo_b200_libm_cache_path(void);
 

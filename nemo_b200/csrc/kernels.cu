@@ -347,6 +347,78 @@ __device__ __forceinline__ bool modelQif(const NetDev& net, const GroupDev& g, u
 	return fired;
 }
 
+__device__ __forceinline__ float expfMatch(const NetDev& net, float x)
+{
+	return libm::expf_match(x, net.expKeys, net.expValues, net.expCount, net.expKfac);
+}
+
+/* Hodgkin-Huxley (src/nemo/cpu/plugins/HH.cpp:14-137): state v, n, m, h, dir;
+ * no parameters. The currents act as conductances towards the reversal
+ * potentials 0 and -70 mV. 999 Euler substeps of 0.001 ms ((int)(1/0.001f)
+ * in float), six glibc-matching expf per substep; fires on the first
+ * substep whose voltage change turns negative above -45 mV, from the 10th
+ * cycle after the timer reset on. */
+__device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
+		float Excit, float Inhib, bool stim, uint32_t cycle)
+{
+	const size_t c = g.count;
+	float* S = g.state;
+	const float Exter = net.ext[n];
+	float v = S[0 * c + i];
+	float nn = S[1 * c + i];
+	float m = S[2 * c + i];
+	float h = S[3 * c + i];
+	float dir = S[4 * c + i];
+	if(Exter != 0.0f) {
+		net.ext[n] = 0.0f;
+	}
+	const float dt = 0.001f;
+	const float gNa = 120.0f, gK = 36.0f, gL = 0.3f;
+	const float ENa = __fsub_rn(115.0f, 65.0f);
+	const float EK = __fsub_rn(-12.0f, 65.0f);
+	const float EL = __fsub_rn(10.6f, 65.0f);
+	const float C = 1.0f, RevE = 0.0f, RevI = -70.0f;
+	const int incMax = int(__fdiv_rn(1.0f, dt));
+	bool fired = false;
+	for(int t = 0; t < incMax; ++t) {
+		const float vr = __fadd_rn(v, 65.0f);
+		const float I = __fadd_rn(__fadd_rn(__fmul_rn(Excit, __fsub_rn(RevE, v)),
+					__fmul_rn(Inhib, __fdiv_rn(__fsub_rn(RevI, v), -1.0f))), Exter);
+		const float alphan = __fdiv_rn(__fsub_rn(0.1f, __fmul_rn(0.01f, vr)),
+				__fsub_rn(expfMatch(net, __fsub_rn(1.0f, __fmul_rn(0.1f, vr))), 1.0f));
+		const float alpham = __fdiv_rn(__fsub_rn(2.5f, __fmul_rn(0.1f, vr)),
+				__fsub_rn(expfMatch(net, __fsub_rn(2.5f, __fmul_rn(0.1f, vr))), 1.0f));
+		const float alphah = __fmul_rn(0.07f, expfMatch(net, __fdiv_rn(-vr, 20.0f)));
+		const float betan = __fmul_rn(0.125f, expfMatch(net, __fdiv_rn(-vr, 80.0f)));
+		const float betam = __fmul_rn(4.0f, expfMatch(net, __fdiv_rn(-vr, 18.0f)));
+		const float betah = __fdiv_rn(1.0f, __fadd_rn(expfMatch(net, __fsub_rn(3.0f, __fmul_rn(0.1f, vr))), 1.0f));
+		m = __fadd_rn(m, __fmul_rn(dt, __fsub_rn(__fmul_rn(alpham, __fsub_rn(1.0f, m)), __fmul_rn(betam, m))));
+		nn = __fadd_rn(nn, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphan, __fsub_rn(1.0f, nn)), __fmul_rn(betan, nn))));
+		h = __fadd_rn(h, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphah, __fsub_rn(1.0f, h)), __fmul_rn(betah, h))));
+		const float m3 = __fmul_rn(__fmul_rn(m, m), m);
+		const float n4 = __fmul_rn(__fmul_rn(__fmul_rn(nn, nn), nn), nn);
+		const float Ik = __fadd_rn(__fadd_rn(
+					__fmul_rn(__fmul_rn(__fmul_rn(gNa, m3), h), __fsub_rn(v, ENa)),
+					__fmul_rn(__fmul_rn(gK, n4), __fsub_rn(v, EK))),
+				__fmul_rn(gL, __fsub_rn(v, EL)));
+		const float newv = __fadd_rn(v, __fdiv_rn(__fmul_rn(dt, __fadd_rn(-Ik, I)), C));
+		const float newDir = __fsub_rn(newv, v);
+		const float change = ((dir < 0.0f) | (newv < -45.0f)) ? 0.0f : newDir;
+		dir = newDir;
+		if(!fired && cycle >= 10u) {
+			fired = double(change) < -0.000000001;
+		}
+		v = newv;
+	}
+	fired = fired || stim;
+	S[0 * c + i] = v;
+	S[1 * c + i] = nn;
+	S[2 * c + i] = m;
+	S[3 * c + i] = h;
+	S[4 * c + i] = dir;
+	return fired;
+}
+
 /* PoissonSource (src/nemo/cpu/plugins/PoissonSource.cpp:21-29). The
  * currents (drained by the caller, as every neuron's slot must be) and the
  * external current (cleared) are unused. */
@@ -626,6 +698,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						}
 						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
 						case 2: fired = modelQif(net, G, i, n, E, I, stim); break;
+						case 3: fired = modelHH(net, G, i, n, E, I, stim, t - G.timerBase); break;
 						case 4: fired = modelPoisson(net, G, i, n, E, I, stim); break;
 						default: fired = modelInput(net, G, i, n, E, I, stim); break;
 					}
@@ -1029,6 +1102,16 @@ k_libm_eval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t
 	}
 }
 
+/* the device expf of the floats with bits [first, first + n) (diagnostics) */
+__global__ void
+k_exp_eval(uint32_t first, uint32_t n, float* out, NetDev net)
+{
+	const uint32_t stride = gridDim.x * blockDim.x;
+	for(uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
+		out[k] = expfMatch(net, libm::u2f(first + k));
+	}
+}
+
 int g_smCount = 0;
 
 } // namespace
@@ -1168,6 +1251,13 @@ launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 {
 	if(n == 0) return;
 	k_nrand_probe<<<uint32_t((n + 255) / 256), 256, 0, S(stream)>>>(u1, u2, out, n, sinTab, logTab);
+}
+
+void
+launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* stream)
+{
+	if(n == 0) return;
+	k_exp_eval<<<smCount() * 8, 256, 0, S(stream)>>>(first, n, out, net);
 }
 
 void

@@ -114,6 +114,12 @@ struct NetDev {
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;
 	const uint32_t* logTab;
+	/* expf exceptions (libm_tables.hpp ExpExceptions): sorted input bits,
+	 * glibc results, count, and 0.5 - tau */
+	const uint32_t* expKeys;
+	const uint32_t* expValues;
+	uint32_t expCount;
+	double expKfac;
 
 	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
 	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */
@@ -214,6 +220,8 @@ void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, ui
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);
+/* device expf (glibc-matching) of the floats with bits [first, first + n) */
+void launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* stream);
 int smCount();
 
 } // namespace nemo_b200

@@ -200,6 +200,88 @@ LIBM_HD float log_argument(float fu) {
 LIBM_HD float sin_candidate(float a) { return float(sin_candidate_d(double(a))); }
 LIBM_HD float log_candidate(float y) { return float(log_candidate_d(y)); }
 
+/* exp(x) of a float x, evaluated in double with explicitly rounded
+ * operations (identical on host and device): x = k ln2 + r with the
+ * Cody-Waite split of ln2 (|r| <= ln2/2), e^r by its Taylor series to degree
+ * 13 in Horner form, scaled by 2^k. Beyond the float range: 0 below -104,
+ * infinity above 89; NaN stays NaN. */
+LIBM_HD double exp_candidate_d(float xf) {
+	if(!(xf == xf)) return double(xf);
+	if(xf > 89.0f) return u2d(0x7FF0000000000000ull);
+	if(xf < -104.0f) return 0.0;
+	const double invln2 = 1.4426950408889634;
+	const double ln2_hi = 6.93147180369123816490e-01;  /* 0x3FE62E42FEE00000 */
+	const double ln2_lo = 1.90821492927058770002e-10;
+	const double x = double(xf);
+	const double t = D_MUL(x, invln2);
+#ifdef __CUDA_ARCH__
+	const int k = __double2int_rn(t);
+#else
+	const int k = int(nearbyint(t));
+#endif
+	const double kd = double(k);
+	const double r = D_SUB(D_SUB(x, D_MUL(kd, ln2_hi)), D_MUL(kd, ln2_lo));
+	double p = 1.6059043836821613e-10;           /* 1/13! */
+	p = D_ADD(D_MUL(p, r), 2.08767569878681e-09);   /* 1/12! */
+	p = D_ADD(D_MUL(p, r), 2.505210838544172e-08);  /* 1/11! */
+	p = D_ADD(D_MUL(p, r), 2.755731922398589e-07);  /* 1/10! */
+	p = D_ADD(D_MUL(p, r), 2.7557319223985893e-06); /* 1/9! */
+	p = D_ADD(D_MUL(p, r), 2.48015873015873e-05);   /* 1/8! */
+	p = D_ADD(D_MUL(p, r), 0.0001984126984126984);  /* 1/7! */
+	p = D_ADD(D_MUL(p, r), 0.001388888888888889);   /* 1/6! */
+	p = D_ADD(D_MUL(p, r), 0.008333333333333333);   /* 1/5! */
+	p = D_ADD(D_MUL(p, r), 0.041666666666666664);   /* 1/4! */
+	p = D_ADD(D_MUL(p, r), 0.16666666666666666);    /* 1/3! */
+	p = D_ADD(D_MUL(p, r), 0.5);
+	p = D_ADD(D_MUL(p, r), 1.0);
+	p = D_ADD(D_MUL(p, r), 1.0);
+	return D_MUL(p, u2d(uint64_t(1023 + k) << 52));
+}
+
+/* How far the double candidate c lies from the float rounding boundary, in
+ * units of the float spacing at float(c): 0.5 - |c - float(c)| / spacing,
+ * i.e. 0 on a midpoint and 0.5 on a float. Infinity and NaN give 1. */
+LIBM_HD double exp_boundary(double c) {
+	const float r = float(c);
+	const uint32_t rb = f2u(r);
+	if((rb & 0x7F800000u) == 0x7F800000u) return 1.0;
+	const float nb = u2f(double(r) < c ? rb + 1u : (rb == 0u ? 1u : rb - 1u));
+	const double spacing = double(nb) > double(r) ? D_SUB(double(nb), double(r)) : D_SUB(double(r), double(nb));
+	const double off = c > double(r) ? D_SUB(c, double(r)) : D_SUB(double(r), c);
+	return D_SUB(0.5, D_DIV(off, spacing));
+}
+
+/* Whether the candidate c lies within (0.5 - kfac) spacings of the float
+ * rounding boundary (kfac = 0.5 - tau, tau from the exception table); the
+ * division-free form of exp_boundary(c) <= tau. */
+LIBM_HD bool exp_near_boundary(double c, double kfac) {
+	const float r = float(c);
+	const uint32_t rb = f2u(r);
+	if((rb & 0x7F800000u) == 0x7F800000u) return false;
+	const float nb = u2f(double(r) < c ? rb + 1u : (rb == 0u ? 1u : rb - 1u));
+	const double spacing = double(nb) > double(r) ? D_SUB(double(nb), double(r)) : D_SUB(double(r), double(nb));
+	const double off = c > double(r) ? D_SUB(c, double(r)) : D_SUB(double(r), c);
+	return off >= D_MUL(kfac, spacing);
+}
+
+/* glibc expf: the rounded candidate, or the exception table's value for an
+ * input on which glibc rounds the other way (keys sorted) */
+LIBM_HD float expf_match(float x, const uint32_t* keys, const uint32_t* values, uint32_t count, double kfac) {
+	const double c = exp_candidate_d(x);
+	float r = float(c);
+	if(count && exp_near_boundary(c, kfac)) {
+		const uint32_t key = f2u(x);
+		uint32_t lo = 0, hi = count;
+		while(lo < hi) {
+			const uint32_t mid = (lo + hi) >> 1;
+			if(keys[mid] < key) lo = mid + 1;
+			else hi = mid;
+		}
+		if(lo < count && keys[lo] == key) r = u2f(values[lo]);
+	}
+	return r;
+}
+
 LIBM_HD float apply_code(float cand, uint32_t code) {
 	uint32_t b = f2u(cand);
 	b += (code == 1u) ? 1u : 0u;

@@ -14,6 +14,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -178,6 +179,143 @@ std::string
 libmCachePath()
 {
 	return cachePath();
+}
+
+/* ---- expf exceptions (the HH plugin's exp, src/nemo/cpu/plugins/HH.cpp:92-98) ---- */
+
+static const uint32_t EXP_MAGIC = 0x4e4d4558u; /* "NMEX" */
+static const uint32_t EXP_VERSION = 1u;
+
+static std::string
+expCachePath()
+{
+	std::string p = cachePath();
+	size_t slash = p.rfind('/');
+	std::string dir = slash == std::string::npos ? std::string(".") : p.substr(0, slash);
+	return dir + "/expf_exceptions_v1_glibc-" + gnu_get_libc_version() + ".bin";
+}
+
+struct ExpPart {
+	std::vector<uint32_t> keys, values;
+	double tau = 0.0;
+	unsigned long bad = 0;
+};
+
+static void
+buildExpRange(uint32_t lo, uint32_t hi, unsigned stride, unsigned offset, ExpPart* out)
+{
+	for(uint64_t u = uint64_t(lo) + offset; u <= hi; u += stride) {
+		const float x = u2f(uint32_t(u));
+		volatile float g = expf(x);
+		const double c = exp_candidate_d(x);
+		const float r = float(c);
+		if(f2u(g) != f2u(r)) {
+			const int64_t d = int64_t(f2u(g)) - int64_t(f2u(r));
+			if(d != 1 && d != -1) out->bad++;
+			out->keys.push_back(uint32_t(u));
+			out->values.push_back(f2u(g));
+			out->tau = std::max(out->tau, exp_boundary(c));
+		}
+	}
+}
+
+static ExpExceptions
+buildExpExceptions()
+{
+	unsigned nthreads = std::max(1u, std::thread::hardware_concurrency());
+	std::vector<ExpPart> parts(2 * nthreads);
+	std::vector<std::thread> pool;
+	const uint32_t posHi = f2u(89.0f), negLo = 0x80000000u, negHi = f2u(-104.0f);
+	for(unsigned i = 0; i < nthreads; ++i) {
+		pool.emplace_back(buildExpRange, 0u, posHi, nthreads, i, &parts[i]);
+		pool.emplace_back(buildExpRange, negLo, negHi, nthreads, i, &parts[nthreads + i]);
+	}
+	for(auto& th : pool) th.join();
+	ExpExceptions e;
+	std::vector<std::pair<uint32_t, uint32_t>> all;
+	unsigned long bad = 0;
+	for(const ExpPart& p : parts) {
+		for(size_t k = 0; k < p.keys.size(); ++k) all.emplace_back(p.keys[k], p.values[k]);
+		e.tau = std::max(e.tau, p.tau);
+		bad += p.bad;
+	}
+	/* margin for the division-free test on the device (exp_near_boundary) */
+	e.tau += 1e-6;
+	if(bad) {
+		fail(NEMO_LOGIC_ERROR, "expf exceptions: " + std::to_string(bad)
+				+ " inputs differ from glibc by more than one unit in the last place");
+	}
+	std::sort(all.begin(), all.end());
+	for(const auto& kv : all) {
+		e.keys.push_back(kv.first);
+		e.values.push_back(kv.second);
+	}
+	return e;
+}
+
+static bool
+loadExpCache(const std::string& path, ExpExceptions& e)
+{
+	FILE* f = fopen(path.c_str(), "rb");
+	if(!f) return false;
+	uint32_t hdr[3] = {0, 0, 0};
+	char ver[32] = {0};
+	double tau = 0;
+	bool ok = fread(hdr, sizeof(hdr), 1, f) == 1 && fread(ver, sizeof(ver), 1, f) == 1
+		&& fread(&tau, sizeof(tau), 1, f) == 1
+		&& hdr[0] == EXP_MAGIC && hdr[1] == EXP_VERSION
+		&& strncmp(ver, gnu_get_libc_version(), sizeof(ver)) == 0;
+	if(ok) {
+		e.keys.resize(hdr[2]);
+		e.values.resize(hdr[2]);
+		e.tau = tau;
+		ok = fread(e.keys.data(), 4, hdr[2], f) == hdr[2] && fread(e.values.data(), 4, hdr[2], f) == hdr[2];
+	}
+	fclose(f);
+	return ok;
+}
+
+static void
+saveExpCache(const std::string& path, const ExpExceptions& e)
+{
+	size_t slash = path.rfind('/');
+	if(slash != std::string::npos) {
+		mkdir(path.substr(0, slash).c_str(), 0755);
+	}
+	std::string tmp = path + ".tmp." + std::to_string(getpid());
+	FILE* f = fopen(tmp.c_str(), "wb");
+	if(!f) return;
+	const uint32_t n = uint32_t(e.keys.size());
+	uint32_t hdr[3] = {EXP_MAGIC, EXP_VERSION, n};
+	char ver[32] = {0};
+	strncpy(ver, gnu_get_libc_version(), sizeof(ver) - 1);
+	bool ok = fwrite(hdr, sizeof(hdr), 1, f) == 1 && fwrite(ver, sizeof(ver), 1, f) == 1
+		&& fwrite(&e.tau, sizeof(e.tau), 1, f) == 1
+		&& fwrite(e.keys.data(), 4, n, f) == n && fwrite(e.values.data(), 4, n, f) == n;
+	ok = (fclose(f) == 0) && ok;
+	if(ok) {
+		rename(tmp.c_str(), path.c_str());
+	} else {
+		remove(tmp.c_str());
+	}
+}
+
+const ExpExceptions&
+expExceptions()
+{
+	static std::mutex lock;
+	static ExpExceptions table;
+	static bool ready = false;
+	std::lock_guard<std::mutex> guard(lock);
+	if(!ready) {
+		std::string path = expCachePath();
+		if(!loadExpCache(path, table)) {
+			table = buildExpExceptions();
+			saveExpCache(path, table);
+		}
+		ready = true;
+	}
+	return table;
 }
 
 } // namespace nemo_b200

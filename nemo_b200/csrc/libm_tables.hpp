@@ -21,6 +21,21 @@ LibmTables buildLibmTables();
 
 std::string libmCachePath();
 
+/* The inputs on which host glibc expf differs from the rounded device
+ * candidate libm::exp_candidate_d (all finite floats in [-104, 89]; outside
+ * that range both give 0 or infinity), sorted by input bits, with glibc's
+ * results, and the largest libm::exp_boundary of their candidates: an input
+ * whose candidate lies farther from the rounding boundary is never an
+ * exception. */
+struct ExpExceptions {
+	std::vector<uint32_t> keys;
+	std::vector<uint32_t> values;
+	double tau = 0.0;
+};
+
+/* Process-wide table: loaded from the cache file or built (all cores). */
+const ExpExceptions& expExceptions();
+
 } // namespace nemo_b200
 
 #endif

@@ -346,6 +346,22 @@ nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[14])
 }
 
 nemo_status_t
+nemo_b200_expf_check(nemo_simulation_t s, uint64_t* mismatches)
+{
+	RETURN_CALL(*mismatches = s->sim.expfCheck());
+}
+
+nemo_status_t
+nemo_b200_expf_exceptions(size_t* count, double* tau)
+{
+	RETURN_CALL({
+		const nemo_b200::ExpExceptions& e = nemo_b200::expExceptions();
+		if(count) *count = e.keys.size();
+		if(tau) *tau = e.tau;
+	});
+}
+
+nemo_status_t
 nemo_b200_libm_check(nemo_simulation_t s, uint64_t* mismatches)
 {
 	RETURN_CALL(*mismatches = s->sim.libmCheck());

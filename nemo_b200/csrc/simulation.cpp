@@ -108,7 +108,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	for(const NeuronGroup& ng : net.groups) {
 		uint32_t n = uint32_t(ng.gidx.size());
 		if(n == 0) continue;
-		if(ng.type.kind == MODEL_COUNT || ng.type.kind == MODEL_HH) {
+		if(ng.type.kind == MODEL_COUNT) {
 			fail(NEMO_API_UNSUPPORTED, "The B200 backend has no kernel for neuron model " + ng.type.name);
 		}
 		Group g;
@@ -428,6 +428,15 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		}
 		g.dRng = (uint4*) put(seeds.data(), seeds.size() * 16);
 		needTables = needTables || g.type.kind == MODEL_IZHIKEVICH;
+	}
+	bool needExp = false;
+	for(const Group& g : m_groups) needExp = needExp || g.type.kind == MODEL_HH;
+	if(needExp) {
+		const ExpExceptions& e = expExceptions();
+		m_net.expKeys = (const uint32_t*) put(e.keys.data(), e.keys.size() * 4);
+		m_net.expValues = (const uint32_t*) put(e.values.data(), e.values.size() * 4);
+		m_net.expCount = uint32_t(e.keys.size());
+		m_net.expKfac = 0.5 - e.tau;
 	}
 	if(needTables) {
 		const LibmTables& t = libmTables();
@@ -1124,6 +1133,58 @@ Simulation::trace(unsigned cycles, double out[14])
 	out[11] = sN ? sNs / sN : 0.0;
 	out[12] = gN / (double(cycles) * m_blocks);
 	out[13] = sN / (double(cycles) * m_blocks);
+}
+
+/* Every float in [-104, 89] through the device expf, compared with host
+ * glibc expf, in chunks of 2^26 inputs. */
+uint64_t
+Simulation::expfCheck()
+{
+	const ExpExceptions& e = expExceptions();
+	cudaStream_t stream = STREAM(m_stream);
+	NetDev net = m_net;
+	uint32_t *keys = nullptr, *vals = nullptr;
+	float* dout = nullptr;
+	const uint32_t CHUNK = 1u << 26;
+	NEMO_CUDA(cudaMalloc(&keys, e.keys.size() * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&vals, e.values.size() * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&dout, size_t(CHUNK) * 4));
+	NEMO_CUDA(cudaMemcpyAsync(keys, e.keys.data(), e.keys.size() * 4, cudaMemcpyHostToDevice, stream));
+	NEMO_CUDA(cudaMemcpyAsync(vals, e.values.data(), e.values.size() * 4, cudaMemcpyHostToDevice, stream));
+	net.expKeys = keys;
+	net.expValues = vals;
+	net.expCount = uint32_t(e.keys.size());
+	net.expKfac = 0.5 - e.tau;
+	std::vector<float> h(CHUNK);
+	uint64_t bad = 0;
+	const uint32_t ranges[2][2] = {{0u, libm::f2u(89.0f)}, {0x80000000u, libm::f2u(-104.0f)}};
+	unsigned nth = std::max(1u, std::thread::hardware_concurrency());
+	for(const auto& rg : ranges) {
+		for(uint64_t first = rg[0]; first <= rg[1]; first += CHUNK) {
+			const uint32_t n = uint32_t(std::min<uint64_t>(CHUNK, uint64_t(rg[1]) - first + 1));
+			launchExpEval(uint32_t(first), n, dout, net, m_stream);
+			NEMO_CUDA(cudaMemcpyAsync(h.data(), dout, size_t(n) * 4, cudaMemcpyDeviceToHost, stream));
+			NEMO_CUDA(cudaStreamSynchronize(stream));
+			std::vector<uint64_t> part(nth, 0);
+			std::vector<std::thread> pool;
+			for(unsigned w = 0; w < nth; ++w) {
+				pool.emplace_back([&, w]() {
+					uint64_t b = 0;
+					for(uint32_t k = w; k < n; k += nth) {
+						volatile float g = expf(libm::u2f(uint32_t(first) + k));
+						if(libm::f2u(g) != libm::f2u(h[k])) b++;
+					}
+					part[w] = b;
+				});
+			}
+			for(auto& th : pool) th.join();
+			for(uint64_t b : part) bad += b;
+		}
+	}
+	cudaFree(keys);
+	cudaFree(vals);
+	cudaFree(dout);
+	return bad;
 }
 
 uint64_t

@@ -74,6 +74,10 @@ public:
 	 * the results that differ from host glibc (tests; expected 0). */
 	uint64_t libmCheck();
 
+	/* Evaluate the device expf of the HH model on every float in [-104, 89]
+	 * and count the results that differ from host glibc (tests; expected 0). */
+	uint64_t expfCheck();
+
 	/* Device-timed throughput loop: `steps` x (one persistent launch of
 	 * `cyclesPerStep` cycles, then applyStdp(reward) if apply), bracketed by
 	 * CUDA events on the simulation's stream. out: [0] device ms, [1] neurons

@@ -105,3 +105,16 @@ def test_simulation_without_gpu_fails_loudly():
     net = netgen.ring(64).build(Network(gpu))
     with pytest.raises(NemoError, match="CUDA"):
         Simulation(net, Configuration(gpu))
+
+
+def test_expf_exception_table_is_small():
+    """The host-built table of inputs where glibc expf rounds differently from
+    the device candidate: about 1e-4 of the 2.2e9 floats in [-104, 89], all
+    close to a rounding boundary."""
+    import ctypes
+    from nemo_b200.nemo import PRODUCT_LIBRARY
+    lib = ctypes.CDLL(PRODUCT_LIBRARY)
+    count, tau = ctypes.c_size_t(), ctypes.c_double()
+    assert lib.nemo_b200_expf_exceptions(ctypes.byref(count), ctypes.byref(tau)) == 0
+    assert 0 < count.value < 2_000_000
+    assert 0.0 < tau.value < 0.01

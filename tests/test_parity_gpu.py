@@ -110,11 +110,57 @@ def test_stdp_network_weights(oracle_lib):
             assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid)
 
 
-def test_mixed_models_with_stimulus(oracle_lib):
-    """Izhikevich, IF_curr_exp, QIF, PoissonSource and Input populations with
-    random firing and current stimulus every cycle."""
+def test_expf_exhaustive():
+    """The Hodgkin-Huxley model's device expf reproduces host glibc expf on
+    every float in [-104, 89]."""
+    lib = Library()
+    net = netgen.ring(32).build(Network(lib))
+    sim = Simulation(net, Configuration(lib))
+    mism = ctypes.c_uint64(99)
+    lib.dll.nemo_b200_expf_check.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+    lib.call("nemo_b200_expf_check", sim.handle, ctypes.byref(mism))
+    assert mism.value == 0
+
+
+def _hh_network(n, m, seed):
+    rng = np.random.default_rng(seed)
     f32 = np.float32
-    spec = netgen.mixed_plugins(n_iz=700, n_lif=500, n_qif=300, n_hh=0, m=60, dmax=10, seed=5)
+    vals = [-65.0, 0.3177, 0.0529, 0.5961, 0.0]
+    spec = netgen.NetSpec([netgen.Population("HH", np.arange(n, dtype=np.uint32),
+                                             [np.full(n, x, f32) for x in vals])])
+    spec.source = np.repeat(np.arange(n, dtype=np.uint32), m)
+    spec.target = rng.integers(0, n, n * m, dtype=np.uint32)
+    spec.delay = rng.integers(1, 6, n * m, dtype=np.uint32)
+    spec.weight = (rng.random(n * m, dtype=f32) * f32(0.3)).astype(f32)
+    spec.plastic = np.zeros(n * m, np.uint8)
+    return spec
+
+
+def test_hodgkin_huxley_network(oracle_lib):
+    """A network of Hodgkin-Huxley neurons alone (simulation index base 0,
+    where the reference plugin is well defined) driven by current stimulus:
+    identical firing every cycle and identical v, n, m, h, dir bits."""
+    n = 160
+    spec = _hh_network(n, 20, seed=8)
+    (_, g), (_, o) = _pair(spec, oracle_lib)
+    rng = np.random.default_rng(1)
+    total = 0
+    for c in range(60):
+        ii = np.nonzero(rng.random(n) < 0.3)[0]
+        istim = [(int(i), float(rng.uniform(5, 25))) for i in ii]
+        a, b = g.step(istim=istim), o.step(istim=istim)
+        assert np.array_equal(a, b), "cycle %d" % c
+        total += a.size
+    assert total > 0
+    for var in range(5):
+        assert np.array_equal(_state_bits(g, spec, var), _state_bits(o, spec, var)), var
+
+
+def test_mixed_models_with_stimulus(oracle_lib):
+    """Izhikevich, IF_curr_exp, QIF, Hodgkin-Huxley, PoissonSource and Input
+    populations with random firing and current stimulus every cycle."""
+    f32 = np.float32
+    spec = netgen.mixed_plugins(n_iz=700, n_lif=500, n_qif=300, n_hh=60, m=60, dmax=10, seed=5)
     rng = np.random.default_rng(3)
     npois, ninp = 100, 50
     base = spec.neuron_count
@@ -130,7 +176,7 @@ def test_mixed_models_with_stimulus(oracle_lib):
     spec.weight = np.concatenate([spec.weight, rng.random(extra_src.size, dtype=f32) * f32(2)])
     spec.plastic = np.concatenate([spec.plastic, np.zeros(extra_src.size, np.uint8)])
     (_, g), (_, o) = _pair(spec, oracle_lib)
-    for c in range(400):
+    for c in range(150):
         fstim = np.nonzero(rng.random(n) < 0.01)[0]
         ii = np.nonzero(rng.random(n) < 0.02)[0]
         istim = [(int(i), float(rng.normal(5, 5))) for i in ii]
