@@ -71,6 +71,48 @@ nemo_status_t nemo_b200_step_noalloc(nemo_simulation_t sim,
 		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
 		unsigned fired[], size_t fired_capacity, size_t* fired_count);
 
+/* Cumulative device counters since the simulation was created: out[0]
+ * synapses delivered, out[1] STDP synapse visits, out[2] neurons fired,
+ * out[3] synaptic events (fired neurons x out-degree). */
+nemo_status_t nemo_b200_counters(nemo_simulation_t sim, uint64_t out[4]);
+
+/* ---- batches: many independent networks in one simulation ----
+ *
+ * nemo_b200_new_batch builds one simulation from `count` networks that stay
+ * independent (trials, parameter sweeps): they advance together in the same
+ * persistent step kernel, and each gives exactly the firing it gives when
+ * simulated alone (its own random seeds, its own neuron indices).
+ * nemo_step / nemo_b200_run / nemo_b200_run_graph advance all instances; a
+ * fired list of nemo_step holds the instances' neurons shifted by the
+ * instance's base index (instances in order), so use
+ * nemo_b200_batch_fired_at to read them per instance. Returns NULL on error
+ * (nemo_strerror). */
+nemo_simulation_t nemo_b200_new_batch(nemo_network_t nets[], size_t count, nemo_configuration_t conf);
+
+/* Number of networks of a batch (1 for an ordinary simulation). */
+nemo_status_t nemo_b200_batch_instances(nemo_simulation_t sim, size_t* count);
+
+/* Fired neurons of every instance in `cycle` (one of the last 1024): each
+ * instance's own neuron indices in its simulation order, instance after
+ * instance; instance j's are fired[offsets[j] .. offsets[j+1]). Both arrays
+ * belong to the simulation and stay valid until the next call. */
+nemo_status_t nemo_b200_batch_fired_at(nemo_simulation_t sim, uint64_t cycle,
+		const unsigned* fired[], const size_t* offsets[]);
+
+/* Run `cycles` cycles (<= 1024) as a CUDA graph of persistent launches of at
+ * most `cycles_per_launch` cycles each (0: one launch); the graph is captured
+ * on the first call with given sizes and replayed afterwards. *used_graph
+ * (may be NULL) is 0 when the device refused the capture and the launches
+ * ran directly. Same results as nemo_b200_run. */
+nemo_status_t nemo_b200_run_graph(nemo_simulation_t sim, unsigned cycles, unsigned cycles_per_launch,
+		int* used_graph);
+
+/* Choose the step kernel's threads per partition (1024, 512 or 256; the
+ * partitions stay) by timing `trial_cycles` cycles with each, keeping the
+ * fastest. The 3 x trial_cycles cycles are simulated like any others.
+ * ms[k] (may be NULL): device ms per cycle of each size. */
+nemo_status_t nemo_b200_autotune(nemo_simulation_t sim, unsigned trial_cycles, unsigned* threads, double ms[3]);
+
 /* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`
  * cycles in one persistent launch, then applyStdp(reward) when apply_stdp != 0),
  * bracketed by CUDA events on the simulation's stream. out[0] = device ms,

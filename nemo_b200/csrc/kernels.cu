@@ -21,7 +21,6 @@ namespace nemo_b200 {
 namespace {
 
 const unsigned FULL = 0xffffffffu;
-const unsigned BLOCK = 1024;
 /* words per block and cycle of the optional phase trace (kernels.hpp) */
 const unsigned TRACE_WORDS = 9;
 
@@ -573,8 +572,8 @@ __device__ __forceinline__ void gatherAdd(const NetDev& net, int2* sAcc, uint32_
  * history, segment offsets and noise tables out of L2. SMEM: the owned current
  * slots live in dynamic shared memory as int32 E/I pairs,
  * sAcc[slot * ownN + local]; otherwise every access goes to net.acc. */
-template<bool SMEM>
-__global__ void __launch_bounds__(BLOCK, 1)
+template<bool SMEM, unsigned T>
+__global__ void __launch_bounds__(T, 1)
 k_cycles(const __grid_constant__ CycleArgs A)
 {
 	extern __shared__ int2 sAcc[];
@@ -602,6 +601,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	int2* acc32 = reinterpret_cast<int2*>(net.acc);
 	const uint2* region = net.fcm + net.regionBase[b];
 
+	/* the first cycle: a kernel parameter, or (for launches replayed from a
+	 * CUDA graph) a device counter that block 0 advances at the end */
+	const uint64_t first = A.cycleCounter ? *A.cycleCounter : A.firstCycle;
+
 	if(SMEM) {
 		const uint32_t total = net.slots * ownN;
 		for(uint32_t x = tid; x < total; x += blockDim.x) {
@@ -612,7 +615,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	}
 
 	for(uint32_t k = 0; k <= A.cycles; ++k) {
-		const uint64_t t64 = A.firstCycle + k;
+		const uint64_t t64 = first + k;
 		const uint32_t t = uint32_t(t64);
 		const bool doUpdate = k < A.cycles;
 		const bool doPrev = k > 0;     /* gather and learn for cycle t-1 */
@@ -921,7 +924,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	 * so that between launches every spike fired is in the current slots */
 	{
 		__syncthreads();
-		const uint64_t tEnd = A.firstCycle + A.cycles;
+		const uint64_t tEnd = first + A.cycles;
 		const uint32_t slotEnd = uint32_t(tEnd % net.slots);
 		for(uint32_t l = tid; l < myN; l += blockDim.x) {
 			const uint32_t n = ownBase + l;
@@ -945,6 +948,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const size_t n = size_t(ownBase) + l;
 			if(l < myN) acc32[size_t(s) * nDev + n] = sAcc[x];
 		}
+	}
+	if(A.cycleCounter && b == 0 && tid == 0) {
+		*A.cycleCounter = first + A.cycles;
 	}
 }
 
@@ -1187,19 +1193,39 @@ cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, ui
 	const uint32_t own = q + (r ? 1u : 0u);
 	const uint64_t bytes = uint64_t(slots) * own * 32u * 8u;
 	const bool smem = acc32 && bytes <= SMEM_ACC_LIMIT;
+	/* the attribute is per device and shared by all simulations: set it to
+	 * the largest size any of them uses */
+	cudaFuncSetAttribute(k_cycles<true, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
 	int perSm = 0;
 	if(smem) {
-		/* the attribute is per device and shared by all simulations: set it
-		 * to the largest size any of them uses */
-		cudaFuncSetAttribute(k_cycles<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<true>, BLOCK, size_t(bytes));
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<true, 1024>, 1024, size_t(bytes));
 	} else {
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false>, BLOCK, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false, 1024>, 1024, 0);
 	}
 	*blocks = perSm >= 1 ? B : 0u;
 	*ownQ = q;
 	*ownR = r;
 	*smemAcc = smem;
+}
+
+template<bool SMEM>
+static cudaError_t
+launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
+{
+	const NetDev& net = args.net;
+	switch(net.threads) {
+		case 256:
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 256>, dim3(net.blocks), dim3(256), params,
+					bytes, stream);
+		case 512:
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 512>, dim3(net.blocks), dim3(512), params,
+					bytes, stream);
+		default:
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 1024>, dim3(net.blocks), dim3(1024), params,
+					bytes, stream);
+	}
 }
 
 void
@@ -1209,11 +1235,9 @@ launchCycles(const CycleArgs& args, void* stream)
 	const NetDev& net = args.net;
 	if(net.smemAcc) {
 		const size_t bytes = size_t(net.slots) * net.ownWarps * 32u * 8u;
-		cudaLaunchCooperativeKernel((const void*) k_cycles<true>, dim3(net.blocks), dim3(BLOCK), params, bytes,
-				S(stream));
+		launchCyclesT<true>(args, params, bytes, S(stream));
 	} else {
-		cudaLaunchCooperativeKernel((const void*) k_cycles<false>, dim3(net.blocks), dim3(BLOCK), params, 0,
-				S(stream));
+		launchCyclesT<false>(args, params, 0, S(stream));
 	}
 }
 

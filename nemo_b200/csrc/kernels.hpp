@@ -66,6 +66,7 @@ struct NetDev {
 	 * the q + (b < r) neuron warps from b * q + min(b, r) (ownFirst); ownWarps
 	 * = q + (r > 0) is the most any block owns */
 	uint32_t blocks;
+	uint32_t threads;       /* threads per block of the step kernel: 1024, 512 or 256 */
 	uint32_t ownWarps;
 	uint32_t ownQ;
 	uint32_t ownR;
@@ -160,6 +161,9 @@ struct CycleArgs {
 	uint64_t firstCycle;
 	uint32_t cycles;
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
+	/* when set, the first cycle is read from here instead of firstCycle and
+	 * advanced by the launch (launches replayed from a CUDA graph) */
+	uint64_t* cycleCounter;
 	/* optional phase trace (%globaltimer ns), [cycles + 1][block][9]: phase
 	 * start, (unused), last update warp done (0 when the block updates
 	 * nothing), all work done, barrier passed; then the summed durations of
@@ -204,7 +208,8 @@ NEMO_HD inline uint32_t ownerOf(uint32_t w, uint32_t q, uint32_t r)
 	return w < big ? w / (q + 1u) : r + (w - big) / q;
 }
 
-/* Cooperative launch of k_cycles (grid and shared memory from args.net). */
+/* Cooperative launch of k_cycles (grid, block size and shared memory from
+ * args.net). */
 void launchCycles(const CycleArgs& args, void* stream);
 /* The step kernel's grid (one block per SM, at most MAX_BLOCKS; 0 when the
  * kernel cannot be resident), the split of the neuron warps over its blocks

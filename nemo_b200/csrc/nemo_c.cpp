@@ -225,6 +225,30 @@ nemo_new_simulation(nemo_network_t n, nemo_configuration_t c)
 
 void nemo_delete_simulation(nemo_simulation_t s) { delete s; }
 
+nemo_simulation_t
+nemo_b200_new_batch(nemo_network_t nets[], size_t count, nemo_configuration_t c)
+{
+	try {
+		if(count == 0) {
+			fail(NEMO_INVALID_INPUT, "Batch: no networks");
+		}
+		std::vector<const Network*> list(count);
+		for(size_t j = 0; j < count; ++j) list[j] = &nets[j]->net;
+		std::vector<uint32_t> base;
+		Network merged = Network::merge(list, &base);
+		nemo_simulation_class* s = new nemo_simulation_class(merged, c->conf);
+		s->sim.setBatch(std::move(base));
+		return s;
+	} catch(Exception& e) {
+		setResult(e.what(), e.code());
+	} catch(std::exception& e) {
+		setResult(e.what(), NEMO_UNKNOWN_ERROR);
+	} catch(...) {
+		setResult("Unknown error", NEMO_UNKNOWN_ERROR);
+	}
+	return NULL;
+}
+
 nemo_status_t
 nemo_step(nemo_simulation_t s, unsigned fstim_nidx[], size_t fstim_count,
 		unsigned istim_nidx[], float istim_current[], size_t istim_count,
@@ -343,6 +367,47 @@ nemo_status_t
 nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[14])
 {
 	RETURN_CALL(s->sim.trace(cycles, out));
+}
+
+nemo_status_t
+nemo_b200_counters(nemo_simulation_t s, uint64_t out[4])
+{
+	RETURN_CALL(s->sim.readStats(out));
+}
+
+nemo_status_t
+nemo_b200_batch_instances(nemo_simulation_t s, size_t* count)
+{
+	RETURN_CALL(*count = s->sim.instances());
+}
+
+nemo_status_t
+nemo_b200_batch_fired_at(nemo_simulation_t s, uint64_t cycle, const unsigned* fired[], const size_t* offsets[])
+{
+	RETURN_CALL({
+		const std::vector<unsigned>* f;
+		const std::vector<size_t>* o;
+		s->sim.batchFiredAt(cycle, &f, &o);
+		*fired = f->empty() ? NULL : f->data();
+		*offsets = o->data();
+	});
+}
+
+nemo_status_t
+nemo_b200_run_graph(nemo_simulation_t s, unsigned cycles, unsigned cycles_per_launch, int* used_graph)
+{
+	RETURN_CALL(s->sim.runGraph(cycles, cycles_per_launch, used_graph));
+}
+
+nemo_status_t
+nemo_b200_autotune(nemo_simulation_t s, unsigned trial_cycles, unsigned* threads, double ms[3])
+{
+	RETURN_CALL({
+		double t[3];
+		unsigned best = s->sim.autotune(trial_cycles, t);
+		if(threads) *threads = best;
+		if(ms) for(int k = 0; k < 3; ++k) ms[k] = t[k];
+	});
 }
 
 nemo_status_t

@@ -421,6 +421,58 @@ Network::getSynapsesFrom(unsigned source)
 	return m_queried;
 }
 
+/* Instances in order; a type takes the merged group of its name, in order of
+ * first appearance, so each instance keeps its own type order and neuron
+ * order within its neurons. */
+Network
+Network::merge(const std::vector<const Network*>& nets, std::vector<uint32_t>* base)
+{
+	Network m;
+	base->assign(nets.size() + 1, 0u);
+	uint64_t next = 0;
+	for(size_t j = 0; j < nets.size(); ++j) {
+		const Network& n = *nets[j];
+		(*base)[j] = uint32_t(next);
+		uint64_t span = 0;
+		for(const NeuronGroup& g : n.groups) {
+			for(uint32_t gi : g.gidx) span = std::max<uint64_t>(span, uint64_t(gi) + 1);
+		}
+		if(next + span >= (uint64_t(1) << 32)) {
+			fail(NEMO_INVALID_INPUT, "Batch: the networks' neuron indices do not fit in 32 bits together");
+		}
+		const uint32_t off = uint32_t(next);
+		uint32_t local = 0;
+		for(const NeuronGroup& g : n.groups) {
+			const unsigned t = m.addNeuronType(g.type.name);
+			NeuronGroup& mg = m.groups[t];
+			if(m.seedKey.size() < m.groups.size()) m.seedKey.resize(m.groups.size());
+			for(unsigned p = 0; p < g.type.nParam; ++p) {
+				mg.param[p].insert(mg.param[p].end(), g.param[p].begin(), g.param[p].end());
+			}
+			for(unsigned s = 0; s < g.type.nState; ++s) {
+				mg.state[s].insert(mg.state[s].end(), g.state[s].begin(), g.state[s].end());
+			}
+			for(uint32_t gi : g.gidx) {
+				mg.gidx.push_back(gi + off);
+				m.seedKey[t].push_back((uint64_t(j) << 32) | local++);
+			}
+		}
+		const size_t S = n.src.size();
+		for(size_t k = 0; k < S; ++k) {
+			m.src.push_back(n.src[k] + off);
+			m.tgt.push_back(n.tgt[k] + off);
+		}
+		m.dly.insert(m.dly.end(), n.dly.begin(), n.dly.end());
+		m.wgt.insert(m.wgt.end(), n.wgt.begin(), n.wgt.end());
+		m.plastic.insert(m.plastic.end(), n.plastic.begin(), n.plastic.end());
+		m.sid.insert(m.sid.end(), n.sid.begin(), n.sid.end());
+		m.m_maxDelay = std::max(m.m_maxDelay, n.m_maxDelay);
+		next += span;
+	}
+	(*base)[nets.size()] = uint32_t(next);
+	return m;
+}
+
 unsigned
 Network::neuronCount() const
 {

@@ -96,6 +96,14 @@ public:
 	unsigned maxDelay() const { return m_maxDelay; }
 	size_t synapseCount() const { return src.size(); }
 
+	/* A batch: independent networks as one, instance j's user indices
+	 * shifted by base[j] (base has one entry per instance and a final end);
+	 * synapses never cross instances. seedKey[g][i] is (instance << 32) |
+	 * simulation index within the instance for neuron i of group g, so that
+	 * each instance's neurons get the random seeds they would get alone. */
+	static Network merge(const std::vector<const Network*>& nets, std::vector<uint32_t>* base);
+	std::vector<std::vector<uint64_t>> seedKey;
+
 	std::vector<NeuronGroup> groups;
 	std::unordered_map<std::string, unsigned> typeIds;
 	std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> mapper; /* gidx -> (type, index) */

@@ -105,7 +105,9 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	/* ---- neurons: simulation order = type registration order ---- */
 	uint32_t local = 0, devPos = 0;
 	std::vector<const std::vector<uint32_t>*> groupGidx;
-	for(const NeuronGroup& ng : net.groups) {
+	std::vector<const std::vector<uint64_t>*> groupSeedKey;
+	for(size_t ngi = 0; ngi < net.groups.size(); ++ngi) {
+		const NeuronGroup& ng = net.groups[ngi];
 		uint32_t n = uint32_t(ng.gidx.size());
 		if(n == 0) continue;
 		if(ng.type.kind == MODEL_COUNT) {
@@ -129,6 +131,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		}
 		m_groups.push_back(std::move(g));
 		groupGidx.push_back(&ng.gidx);
+		groupSeedKey.push_back(ngi < net.seedKey.size() ? &net.seedKey[ngi] : nullptr);
 		local += n;
 		devPos = uint32_t(roundUp(uint64_t(devPos) + n, 32));
 	}
@@ -377,6 +380,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.fbits = m_fbits;
 	m_net.deliver = deliver ? 1 : 0;
 	m_net.blocks = B;
+	m_net.threads = 1024;
 	m_net.ownWarps = ownWarps;
 	m_net.ownQ = ownQ;
 	m_net.ownR = ownR;
@@ -417,14 +421,43 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	 * outputs 4i..4i+3 of a default-seeded mt19937, reduced to [0, 2^31) by
 	 * Boost's uniform_int (bucket size 2, i.e. >> 1) */
 	std::mt19937 mt;
+	/* a batch seeds each instance as if it were alone: a fresh generator per
+	 * instance, outputs 4i..4i+3 for its simulation index i */
+	std::vector<std::vector<uint4>> instanceSeeds;
+	if(!net.seedKey.empty()) {
+		std::vector<uint32_t> count;
+		for(const auto& keys : net.seedKey) {
+			for(uint64_t key : keys) {
+				const uint32_t j = uint32_t(key >> 32), i = uint32_t(key);
+				if(count.size() <= j) count.resize(j + 1, 0u);
+				count[j] = std::max(count[j], i + 1);
+			}
+		}
+		instanceSeeds.resize(count.size());
+		for(size_t j = 0; j < count.size(); ++j) {
+			std::mt19937 mi;
+			instanceSeeds[j].resize(count[j]);
+			for(uint32_t i = 0; i < count[j]; ++i) {
+				uint32_t a = mi() >> 1, b = mi() >> 1, c = mi() >> 1, d = mi() >> 1;
+				instanceSeeds[j][i] = make_uint4(a, b, c, d);
+			}
+		}
+	}
 	bool needTables = false;
-	for(Group& g : m_groups) {
+	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
+		Group& g = m_groups[gi];
 		g.dParam = (float*) put(g.param.data(), g.param.size() * 4);
 		g.dState = (float*) put(g.state.data(), g.state.size() * 4);
 		std::vector<uint4> seeds(g.count);
+		const std::vector<uint64_t>* keys = groupSeedKey[gi];
 		for(uint32_t i = 0; i < g.count; ++i) {
-			uint32_t a = mt() >> 1, b = mt() >> 1, c = mt() >> 1, d = mt() >> 1;
-			seeds[i] = make_uint4(a, b, c, d);
+			if(keys) {
+				const uint64_t key = (*keys)[i];
+				seeds[i] = instanceSeeds[key >> 32][uint32_t(key)];
+			} else {
+				uint32_t a = mt() >> 1, b = mt() >> 1, c = mt() >> 1, d = mt() >> 1;
+				seeds[i] = make_uint4(a, b, c, d);
+			}
 		}
 		g.dRng = (uint4*) put(seeds.data(), seeds.size() * 16);
 		needTables = needTables || g.type.kind == MODEL_IZHIKEVICH;
@@ -469,6 +502,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 Simulation::~Simulation()
 {
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
+	destroyGraph();
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_hWords) cudaFreeHost(m_hWords);
 	if(m_hStim) cudaFreeHost(m_hStim);
@@ -731,6 +765,142 @@ Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 		if(firedCounts) firedCounts[k] = fc[slot];
 		if(events) events[k] = ev[slot];
 	}
+}
+
+void
+Simulation::batchFiredAt(uint64_t cycle, const std::vector<unsigned>** fired, const std::vector<size_t>** offsets)
+{
+	const std::vector<unsigned>& all = firedAt(cycle);
+	const size_t J = instances();
+	m_batchOffsets.assign(J + 1, 0);
+	m_batchFired.resize(all.size());
+	if(m_batchBase.empty()) {
+		std::copy(all.begin(), all.end(), m_batchFired.begin());
+		m_batchOffsets[1] = all.size();
+	} else {
+		/* stable bucketing by instance keeps each instance's order */
+		std::vector<uint32_t> inst(all.size());
+		for(size_t k = 0; k < all.size(); ++k) {
+			inst[k] = uint32_t(std::upper_bound(m_batchBase.begin(), m_batchBase.end(), all[k]) - m_batchBase.begin() - 1);
+			m_batchOffsets[inst[k] + 1]++;
+		}
+		for(size_t j = 0; j < J; ++j) m_batchOffsets[j + 1] += m_batchOffsets[j];
+		std::vector<size_t> fill(m_batchOffsets.begin(), m_batchOffsets.end() - 1);
+		for(size_t k = 0; k < all.size(); ++k) {
+			m_batchFired[fill[inst[k]]++] = all[k] - m_batchBase[inst[k]];
+		}
+	}
+	*fired = &m_batchFired;
+	*offsets = &m_batchOffsets;
+}
+
+void
+Simulation::destroyGraph()
+{
+	if(m_graphExec) {
+		cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(m_graphExec));
+		m_graphExec = nullptr;
+	}
+}
+
+void
+Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
+{
+	if(cycles == 0) return;
+	if(cycles > m_ring) {
+		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
+	}
+	if(cyclesPerLaunch == 0) cyclesPerLaunch = cycles;
+	cudaStream_t stream = STREAM(m_stream);
+	if(!m_dCycleCounter) {
+		m_dCycleCounter = (uint64_t*) alloc(8);
+	}
+	CycleArgs a = m_args;
+	a.cycleCounter = m_dCycleCounter;
+	for(int gi = 0; gi < a.ngroups; ++gi) a.groups[gi].timerBase = uint32_t(m_timerBase);
+	const uint64_t key[4] = {cycles, cyclesPerLaunch, m_net.threads, m_timerBase};
+	if(m_graphUsable && (!m_graphExec || !std::equal(key, key + 4, m_graphKey))) {
+		destroyGraph();
+		cudaGraph_t graph = nullptr;
+		cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+		if(e == cudaSuccess) {
+			for(unsigned done = 0; done < cycles; done += cyclesPerLaunch) {
+				a.cycles = std::min(cyclesPerLaunch, cycles - done);
+				launchCycles(a, m_stream);
+			}
+			e = cudaStreamEndCapture(stream, &graph);
+		}
+		cudaGraphExec_t exec = nullptr;
+		if(e == cudaSuccess) {
+			e = cudaGraphInstantiate(&exec, graph, 0);
+		}
+		if(graph) cudaGraphDestroy(graph);
+		if(e == cudaSuccess) {
+			m_graphExec = exec;
+			std::copy(key, key + 4, m_graphKey);
+		} else {
+			(void) cudaGetLastError();   /* the capture failed: launch directly from now on */
+			m_graphUsable = false;
+		}
+	}
+	uint64_t counter = m_cycle;
+	NEMO_CUDA(cudaMemcpyAsync(m_dCycleCounter, &counter, 8, cudaMemcpyHostToDevice, stream));
+	if(m_graphUsable && m_graphExec) {
+		NEMO_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(m_graphExec), stream));
+		if(usedGraph) *usedGraph = 1;
+	} else {
+		for(unsigned done = 0; done < cycles; done += cyclesPerLaunch) {
+			a.cycles = std::min(cyclesPerLaunch, cycles - done);
+			launchCycles(a, m_stream);
+			NEMO_CUDA(cudaGetLastError());
+		}
+		if(usedGraph) *usedGraph = 0;
+	}
+	m_cycle += cycles;
+	m_stateDirty = true;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	checkDeviceError();
+}
+
+unsigned
+Simulation::autotune(unsigned trialCycles, double ms[3])
+{
+	if(trialCycles == 0 || trialCycles > m_ring) {
+		fail(NEMO_INVALID_INPUT, "autotune: trial cycles must be in 1.." + std::to_string(m_ring));
+	}
+	cudaStream_t stream = STREAM(m_stream);
+	const unsigned sizes[3] = {1024, 512, 256};
+	unsigned best = sizes[0];
+	double bestMs = 1e300;
+	cudaEvent_t e0, e1;
+	NEMO_CUDA(cudaEventCreate(&e0));
+	NEMO_CUDA(cudaEventCreate(&e1));
+	for(int k = 0; k < 3; ++k) {
+		m_net.threads = sizes[k];
+		m_args.net.threads = sizes[k];
+		NEMO_CUDA(cudaEventRecord(e0, stream));
+		launchBlock(m_cycle, trialCycles);
+		NEMO_CUDA(cudaEventRecord(e1, stream));
+		NEMO_CUDA(cudaEventSynchronize(e1));
+		m_cycle += trialCycles;
+		float t = 0;
+		NEMO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+		ms[k] = double(t) / trialCycles;
+		if(ms[k] < bestMs) {
+			bestMs = ms[k];
+			best = sizes[k];
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	m_net.threads = best;
+	m_args.net.threads = best;
+	m_stateDirty = true;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	checkDeviceError();
+	return best;
 }
 
 void

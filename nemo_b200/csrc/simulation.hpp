@@ -93,6 +93,27 @@ public:
 
 	void readStats(uint64_t out[4]);
 
+	/* ---- batches of independent networks (Network::merge) ---- */
+	void setBatch(std::vector<uint32_t> base) { m_batchBase = std::move(base); }
+	size_t instances() const { return m_batchBase.empty() ? 1 : m_batchBase.size() - 1; }
+	/* Fired neurons of every instance at `cycle` (one of the last cycles):
+	 * instance-local user indices, instance after instance, each in its own
+	 * simulation order, and the offsets of the instances [instances + 1]. */
+	void batchFiredAt(uint64_t cycle, const std::vector<unsigned>** fired, const std::vector<size_t>** offsets);
+
+	/* `cycles` cycles (<= the firing ring) as a CUDA graph of launches of
+	 * at most `cyclesPerLaunch` cycles each, the first cycle of each launch
+	 * read from a device counter; the graph is captured once per (cycles,
+	 * cyclesPerLaunch, block size, timer base) and replayed. *usedGraph = 0
+	 * when the device refused the capture and the launches ran directly. */
+	void runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph);
+
+	/* Time `trialCycles` cycles with each block size of the step kernel
+	 * (1024, 512, 256 threads over the same partitions; the results are the
+	 * same) and keep the fastest. The cycles are simulated (3 x trialCycles
+	 * in all). ms[k]: device ms per cycle of each size. Returns the size. */
+	unsigned autotune(unsigned trialCycles, double ms[3]);
+
 	/* Phase timing of one traced persistent launch of `cycles` cycles, means
 	 * over cycles in ns: [0] phase, [1] max / [2] mean block update with the
 	 * delay-1 push, [3] max / [4] mean block work, [5] first start to last
@@ -180,6 +201,18 @@ private:
 	std::vector<unsigned> m_fired;
 
 	int m_noallocDevice = -1;  /* device of the simulation, found on the first stepNoAlloc */
+
+	/* batch */
+	std::vector<uint32_t> m_batchBase;
+	std::vector<unsigned> m_batchFired;
+	std::vector<size_t> m_batchOffsets;
+
+	/* graph run */
+	void destroyGraph();
+	void* m_graphExec = nullptr;
+	uint64_t* m_dCycleCounter = nullptr;
+	uint64_t m_graphKey[4] = {0, 0, 0, 0};
+	bool m_graphUsable = true;
 };
 
 } // namespace nemo_b200
