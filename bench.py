@@ -254,6 +254,14 @@ def roofline(sim, lib, wl):
     return roof
 
 
+def apply_launches(sim, lib):
+    """Kernel launches of one applyStdp (one per group of owner regions)."""
+    lib.dll.nemo_b200_apply_launches.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]
+    n = ctypes.c_uint()
+    lib.call("nemo_b200_apply_launches", sim.handle, ctypes.byref(n))
+    return n.value
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -286,6 +294,14 @@ def run_b200(args):
     lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_double * 4]
     out = (ctypes.c_double * 4)()
+    # threads per partition of the step kernel, chosen by timing 100-cycle
+    # trials (simulated like any other cycles) after a first warm-up step
+    lib.dll.nemo_b200_autotune.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),
+                                           ctypes.c_double * 3]
+    lib.call("nemo_b200_timed_steps", sim.handle, 1, CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
+    tuned = ctypes.c_uint()
+    tune_ms = (ctypes.c_double * 3)()
+    lib.call("nemo_b200_autotune", sim.handle, CYCLES_PER_STEP, ctypes.byref(tuned), tune_ms)
     # the clock sampler runs through warm-up and the timed region, so that the
     # GPU is under the same load for every sample
     with ClockSampler(local) as clocks:
@@ -342,7 +358,9 @@ def run_b200(args):
                 "steps": e2e_steps_n, "s_per_step": round(e2e_s / e2e_steps_n, 4)},
         "roofline": roof,
         "phase_ns": phase_ns,
-        "gpu_launches": args.steps * 2,
+        "gpu_launches": args.steps * (1 + apply_launches(sim, lib)),
+        "autotune": {"threads": tuned.value, "ms_per_cycle": {"1024": round(tune_ms[0], 5), "512": round(tune_ms[1], 5),
+                                                             "256": round(tune_ms[2], 5)}},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -379,6 +397,105 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args):
+    """The batched form: 256 independent Izhikevich networks (sizes
+    log-uniform in [500, 20000], 100 synapses per neuron, delays U{1..20},
+    per-instance seed and thalamic sigma U(3, 7) / 0.4x for inhibitory
+    neurons) advanced together for 1000 cycles by one persistent kernel
+    replayed from a CUDA graph, block size chosen by the autotuner; against
+    the same networks run one after another with the plain step loop
+    (nemo_step per cycle) and with the device-resident loop."""
+    lib = Library()
+    P = ctypes.POINTER
+    d = lib.dll
+    d.nemo_b200_new_batch.restype = ctypes.c_void_p
+    d.nemo_b200_new_batch.argtypes = [P(ctypes.c_void_p), ctypes.c_size_t, ctypes.c_void_p]
+    d.nemo_b200_run_graph.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, P(ctypes.c_int)]
+    d.nemo_b200_autotune.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint), ctypes.c_double * 3]
+    d.nemo_b200_counters.argtypes = [ctypes.c_void_p, ctypes.c_uint64 * 4]
+    d.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    d.nemo_delete_simulation.argtypes = [ctypes.c_void_p]
+    count, cycles = args.batch_count, 1000
+    sizes = netgen.batched_sizes(count, 500, 20000, seed=3)
+    rng = np.random.default_rng(4)
+    sig = rng.uniform(3.0, 7.0, size=count)
+    specs = [netgen.izhikevich_random(int(n), 100, dmax=20, seed=1000 + j, sigma_exc=float(sig[j]),
+                                      sigma_inh=float(0.4 * sig[j])) for j, n in enumerate(sizes)]
+
+    def counters(handle):
+        c = (ctypes.c_uint64 * 4)()
+        lib.call("nemo_b200_counters", handle, c)
+        return list(c)
+
+    nets = [spec.build(Network(lib)) for spec in specs]
+    conf = Configuration(lib)
+    handles = (ctypes.c_void_p * count)(*[n.handle for n in nets])
+    t0 = time.perf_counter()
+    batch = d.nemo_b200_new_batch(handles, count, conf.handle)
+    if not batch:
+        raise RuntimeError(d.nemo_strerror().decode())
+    build_s = time.perf_counter() - t0
+    del nets
+    threads = ctypes.c_uint()
+    ms = (ctypes.c_double * 3)()
+    lib.call("nemo_b200_run_graph", batch, 100, 100, None)
+    lib.call("nemo_b200_autotune", batch, 100, ctypes.byref(threads), ms)
+    used = ctypes.c_int()
+    lib.call("nemo_b200_run_graph", batch, 100, 100, ctypes.byref(used))   # warm-up, graph capture
+    before = counters(batch)
+    t0 = time.perf_counter()
+    lib.call("nemo_b200_run_graph", batch, cycles, 100, ctypes.byref(used))
+    batched_s = time.perf_counter() - t0
+    events = counters(batch)[3] - before[3]
+    d.nemo_delete_simulation(batch)
+    batched = events / batched_s
+
+    # the same networks one after another
+    plain_s = resident_s = 0.0
+    plain_events = resident_events = 0
+    fptr = P(ctypes.c_uint)()
+    nf = ctypes.c_size_t()
+    for spec in specs:
+        for mode in ("plain", "resident"):
+            net = spec.build(Network(lib))
+            sim = Simulation(net, Configuration(lib))
+            del net
+            b0 = counters(sim.handle)
+            t0 = time.perf_counter()
+            if mode == "plain":
+                for _ in range(cycles):
+                    if d.nemo_step(sim.handle, None, 0, None, None, 0, ctypes.byref(fptr), ctypes.byref(nf)) != 0:
+                        raise RuntimeError(d.nemo_strerror().decode())
+            else:
+                lib.call("nemo_b200_run", sim.handle, cycles, None, None)
+            dt = time.perf_counter() - t0
+            ev = counters(sim.handle)[3] - b0[3]
+            if mode == "plain":
+                plain_s += dt
+                plain_events += ev
+            else:
+                resident_s += dt
+                resident_events += ev
+            del sim
+    line = {
+        "metric": "synaptic events/s (batched form)", "value": round(batched, 1), "unit": UNIT,
+        "n_gpus": 1, "higher_is_better": True, "data": "synthetic (seeded generator)",
+        "config": {"workload": "izhikevich-batch-%d-m100" % count, "instances": count,
+                   "neurons": int(sizes.sum()), "synapses": int(sizes.sum()) * 100, "cycles": cycles,
+                   "sizes": "log-uniform [500, 20000]", "sigma": "U(3,7) exc, 0.4x inh per instance"},
+        "batched": {"seconds": round(batched_s, 4), "events": events, "graph_used": bool(used.value),
+                    "threads_chosen": threads.value, "autotune_ms_per_cycle": [round(x, 5) for x in ms],
+                    "build_s": round(build_s, 2)},
+        "sequential_plain_step_loop": {"events_per_s": round(plain_events / plain_s, 1), "seconds": round(plain_s, 3),
+                                       "events": plain_events},
+        "sequential_device_resident": {"events_per_s": round(resident_events / resident_s, 1),
+                                       "seconds": round(resident_s, 3), "events": resident_events},
+        "speedup_vs_plain_step_loop": round(batched / (plain_events / plain_s), 2),
+        "speedup_vs_device_resident": round(batched / (resident_events / resident_s), 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -389,8 +506,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--batched", action="store_true",
+                    help="measure the batched form (256 networks) instead of the headline workload")
+    ap.add_argument("--batch-count", type=int, default=256)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.batched:
+        run_batched(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)

@@ -71,6 +71,9 @@ nemo_status_t nemo_b200_step_noalloc(nemo_simulation_t sim,
 		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
 		unsigned fired[], size_t fired_capacity, size_t* fired_count);
 
+/* Kernel launches one applyStdp makes (0 without plastic synapses). */
+nemo_status_t nemo_b200_apply_launches(nemo_simulation_t sim, unsigned* launches);
+
 /* Cumulative device counters since the simulation was created: out[0]
  * synapses delivered, out[1] STDP synapse visits, out[2] neurons fired,
  * out[3] synaptic events (fired neurons x out-degree). */
@@ -108,9 +111,9 @@ nemo_status_t nemo_b200_run_graph(nemo_simulation_t sim, unsigned cycles, unsign
 		int* used_graph);
 
 /* Choose the step kernel's threads per partition (1024, 512 or 256; the
- * partitions stay) by timing `trial_cycles` cycles with each, keeping the
- * fastest. The 3 x trial_cycles cycles are simulated like any others.
- * ms[k] (may be NULL): device ms per cycle of each size. */
+ * partitions stay) by timing `trial_cycles` cycles with each, twice, keeping
+ * the fastest. The 6 x trial_cycles cycles are simulated like any others.
+ * ms[k] (may be NULL): the better device ms per cycle of each size. */
 nemo_status_t nemo_b200_autotune(nemo_simulation_t sim, unsigned trial_cycles, unsigned* threads, double ms[3]);
 
 /* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`

@@ -370,6 +370,12 @@ nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[14])
 }
 
 nemo_status_t
+nemo_b200_apply_launches(nemo_simulation_t s, unsigned* launches)
+{
+	RETURN_CALL(*launches = s->sim.applyLaunches());
+}
+
+nemo_status_t
 nemo_b200_counters(nemo_simulation_t s, uint64_t out[4])
 {
 	RETURN_CALL(s->sim.readStats(out));

@@ -92,6 +92,7 @@ public:
 	void profile(unsigned cycles, float reward, double out[10]);
 
 	void readStats(uint64_t out[4]);
+	unsigned applyLaunches() const { return m_stdpOn && m_nrcm ? unsigned(m_applyGroups.size() - 1) : 0u; }
 
 	/* ---- batches of independent networks (Network::merge) ---- */
 	void setBatch(std::vector<uint32_t> base) { m_batchBase = std::move(base); }
@@ -110,8 +111,9 @@ public:
 
 	/* Time `trialCycles` cycles with each block size of the step kernel
 	 * (1024, 512, 256 threads over the same partitions; the results are the
-	 * same) and keep the fastest. The cycles are simulated (3 x trialCycles
-	 * in all). ms[k]: device ms per cycle of each size. Returns the size. */
+	 * same), twice each, and keep the fastest. The cycles are simulated
+	 * (6 x trialCycles in all). ms[k]: the better device ms per cycle of
+	 * each size. Returns the size. */
 	unsigned autotune(unsigned trialCycles, double ms[3]);
 
 	/* Phase timing of one traced persistent launch of `cycles` cycles, means

@@ -72,7 +72,7 @@ class Batch:
         t = ctypes.c_uint()
         ms = (ctypes.c_double * 3)()
         self.lib.call("nemo_b200_autotune", self.handle, trial, ctypes.byref(t), ms)
-        self.cycle += 3 * trial
+        self.cycle += 6 * trial
         return t.value, list(ms)
 
 
