@@ -116,6 +116,56 @@ nemo_status_t nemo_b200_run_graph(nemo_simulation_t sim, unsigned cycles, unsign
  * ms[k] (may be NULL): the better device ms per cycle of each size. */
 nemo_status_t nemo_b200_autotune(nemo_simulation_t sim, unsigned trial_cycles, unsigned* threads, double ms[3]);
 
+/* ---- the differentiable form: discrete LIF network and its BPTT adjoint ----
+ *
+ * A recurrent network of leaky integrate-and-fire neurons (1 ms Euler step,
+ * reset by subtraction) for up to 32 trials at once, and the exact adjoint of
+ * its backpropagation through time with a fast-sigmoid surrogate
+ * 1 / (1 + kappa |u - theta|)^2 standing in for the derivative of the
+ * threshold (the model and the adjoint are written out in
+ * nemo_b200/csrc/lif_bptt.cu). All pointers are device memory; `stream` is a
+ * cudaStream_t (NULL: the default stream). Synapses are listed by target
+ * (rowptr/pre: pre < N a recurrent neuron, whose spike arrives one step
+ * later; pre >= N input channel pre - N, same step), and the recurrent ones
+ * also by source (colptr/post/wpos, wpos the index in pre/w). Return a status;
+ * nemo_b200_lif_error describes a failure. No counterpart in the reference. */
+typedef struct nemo_b200_lif_net {
+	int N;          /* neurons */
+	int C;          /* input channels */
+	int B;          /* trials, 1..32 */
+	int T;          /* steps */
+	int K;          /* steps between checkpoints */
+	int bin_steps;  /* steps per counting bin (T a multiple of it) */
+	float beta;     /* 1 - dt / tau_m */
+	float theta;    /* threshold */
+	float kappa;    /* surrogate slope */
+	const int* rowptr;
+	const int* pre;
+	const int* colptr;
+	const int* post;
+	const int* wpos;
+} nemo_b200_lif_net;
+
+/* Bytes of the work buffer both calls need. */
+size_t nemo_b200_lif_work_bytes(const nemo_b200_lif_net* net);
+
+/* Forward: in_bits [T][C] input spikes (bit b = trial b); outputs s_bits
+ * [T][N] spikes (bit b = trial b), v_ckpt [ceil(T/K)][N][32] checkpoints and
+ * counts [B][T/bin_steps] spikes per trial and bin. relaxed != 0 runs the
+ * relaxed model (spike r(u - theta) = (u - theta) / (1 + kappa |u - theta|),
+ * stored in s_float [T][N][32] instead of s_bits). */
+int nemo_b200_lif_forward(const nemo_b200_lif_net* net, const float* w, const uint32_t* in_bits, int relaxed,
+		uint32_t* s_bits, float* s_float, float* v_ckpt, float* counts, float* work, void* stream);
+
+/* Backward: adds dL/dw into dw (pass zeros) for dL/dcounts dcounts
+ * [B][T/bin_steps], from the forward's s_bits / s_float and v_ckpt, recomputing
+ * each segment of K steps from its checkpoint. */
+int nemo_b200_lif_backward(const nemo_b200_lif_net* net, const float* w, const uint32_t* in_bits, int relaxed,
+		const uint32_t* s_bits, const float* s_float, const float* v_ckpt, const float* dcounts, float* dw,
+		float* work, void* stream);
+
+const char* nemo_b200_lif_error(void);
+
 /* Device-timed throughput loop: `steps` repetitions of (`cycles_per_step`
  * cycles in one persistent launch, then applyStdp(reward) when apply_stdp != 0),
  * bracketed by CUDA events on the simulation's stream. out[0] = device ms,
