@@ -496,6 +496,69 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_bptt(args):
+    """The differentiable form: BPTT gradient steps/s of a recurrent LIF
+    network of 10,000 neurons (tau_m 20 ms, threshold 1, reset by
+    subtraction, 1 ms Euler step), 200 recurrent synapses per neuron
+    (float32 weights ~N(0, 1/sqrt(200))) and 50 synapses per neuron from 500
+    Poisson input channels at 10 Hz; 32 trials of 500 steps; loss: mean
+    squared error between the 10 ms-binned population rate and 20 + 10
+    sin(2 pi 4 t) Hz; gradient w.r.t. all weights through the adjoint kernel
+    (fast-sigmoid surrogate, slope 10, checkpoints every 50 steps)."""
+    import torch
+    from nemo_b200.lif import LIFNetwork, lif_bptt, poisson_bits, rate_loss, sinusoid_target
+    n, fan, chans, infan, steps, trials, binsteps = 10000, 200, 500, 50, 500, 32, 10
+    t0 = time.perf_counter()
+    net = LIFNetwork.random(n, fan, chans, infan, seed=7, checkpoint=50, bin_steps=binsteps, kappa=10.0)
+    w = net.initial_weights(seed=7, scale_in=0.35).requires_grad_(True)
+    bits, _ = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8)
+    target = sinusoid_target(steps // binsteps, binsteps)
+    build_s = time.perf_counter() - t0
+
+    def grad_step():
+        w.grad = None
+        counts = lif_bptt(w, bits, net, trials)
+        loss = rate_loss(counts, n, binsteps, target)
+        loss.backward()
+        return loss, counts
+
+    for _ in range(max(args.warmup, 1)):
+        grad_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k = max(args.steps if args.steps < 100 else 10, 1)
+    e0.record()
+    for _ in range(k):
+        loss, counts = grad_step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    rate = counts.sum().item() / (trials * n * steps / 1000.0)
+    # the forward and the adjoint alone
+    from nemo_b200.lif import lif_backward, lif_forward
+    wd = w.detach()
+    f0, f1, b1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    f0.record()
+    c2, saved = lif_forward(net, wd, bits, trials)
+    f1.record()
+    lif_backward(net, wd, bits, trials, saved, torch.ones_like(c2))
+    b1.record()
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = f0.elapsed_time(f1), f1.elapsed_time(b1)
+    line = {
+        "metric": "BPTT grad steps/s", "value": round(1000.0 / ms, 3), "unit": "grad steps/s", "n_gpus": 1,
+        "steps": k, "warmup": max(args.warmup, 1), "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic (seeded Poisson inputs)",
+        "config": {"workload": "lif-bptt-10k-200", "neurons": n, "recurrent_synapses_per_neuron": fan,
+                   "input_channels": chans, "input_synapses_per_neuron": infan, "trials": trials,
+                   "steps": steps, "checkpoint_every": 50, "surrogate": "1/(1+10|u-theta|)^2"},
+        "loss": round(loss.item(), 3), "mean_rate_hz": round(rate, 3), "build_s": round(build_s, 2),
+        "forward_ms": round(fwd_ms, 3), "backward_ms": round(bwd_ms, 3),
+        "synapse_steps_per_s": round(net.synapses * trials * steps / (ms * 1e-3), 1),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -509,8 +572,12 @@ def main():
     ap.add_argument("--batched", action="store_true",
                     help="measure the batched form (256 networks) instead of the headline workload")
     ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--bptt", action="store_true",
+                    help="measure the differentiable form (BPTT grad steps/s) instead of the headline workload")
     args = ap.parse_args()
-    if args.batched:
+    if args.bptt:
+        run_bptt(args)
+    elif args.batched:
         run_batched(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -75,6 +75,14 @@ __device__ __forceinline__ float presyn(const Net& n, int p, int t, uint32_t lan
 	return float((sBits[size_t(t - 1) * n.N + p] >> lane) & 1u);
 }
 
+/* the spike word (bit b = trial b) of presynaptic unit p at step t */
+__device__ __forceinline__ uint32_t presynWord(const Net& n, int p, int t, const uint32_t* sBits,
+		const uint32_t* inBits)
+{
+	if(p >= n.N) return inBits[size_t(t) * n.C + (p - n.N)];
+	return t == 0 ? 0u : sBits[size_t(t - 1) * n.N + p];
+}
+
 /* One forward step for every neuron (warp per neuron, lane per trial).
  * v: [N][32] state, read and written. RECOMPUTE: store u into uOut (a
  * segment buffer [K][N][32]) instead of the spikes and counts. */
@@ -97,8 +105,9 @@ k_step(Net n, int t, const float* w, const uint32_t* inBits, uint32_t* sBits, fl
 		if(!RECOMPUTE && t % n.K == 0) {
 			vCkpt[size_t(t / n.K) * n.N * 32 + cell] = vPrev;
 		}
-		/* in-synapses in order, 32 at a time: lane L loads synapse base + L,
-		 * then every lane takes them in turn */
+		/* in-synapses in order, 32 at a time: lane L loads synapse base + L
+		 * (and, for spikes as bits, the presynaptic word of all trials), then
+		 * every lane takes them in turn; a word without spikes adds nothing */
 		float I = 0.0f;
 		const int k0 = n.rowptr[i], k1 = n.rowptr[i + 1];
 		for(int base = k0; base < k1; base += 32) {
@@ -106,10 +115,22 @@ k_step(Net n, int t, const float* w, const uint32_t* inBits, uint32_t* sBits, fl
 			const int p = k < k1 ? n.pre[k] : 0;
 			const float wk = k < k1 ? w[k] : 0.0f;
 			const int cnt = min(32, k1 - base);
-			for(int q = 0; q < cnt; ++q) {
-				const int pq = __shfl_sync(FULL, p, q);
-				const float wq = __shfl_sync(FULL, wk, q);
-				I = __fadd_rn(I, __fmul_rn(wq, presyn<RELAXED>(n, pq, t, lane, sBits, sF, inBits)));
+			if(RELAXED) {
+				for(int q = 0; q < cnt; ++q) {
+					const int pq = __shfl_sync(FULL, p, q);
+					const float wq = __shfl_sync(FULL, wk, q);
+					I = __fadd_rn(I, __fmul_rn(wq, presyn<RELAXED>(n, pq, t, lane, sBits, sF, inBits)));
+				}
+			} else {
+				const uint32_t word = k < k1 ? presynWord(n, p, t, sBits, inBits) : 0u;
+				uint32_t nz = __ballot_sync(FULL, word != 0u);
+				while(nz) {
+					const int q = __ffs(int(nz)) - 1;
+					nz &= nz - 1u;
+					const uint32_t wd = __shfl_sync(FULL, word, q);
+					const float wq = __shfl_sync(FULL, wk, q);
+					if((wd >> lane) & 1u) I = __fadd_rn(I, wq);
+				}
 			}
 		}
 		const float u = __fadd_rn(__fmul_rn(n.beta, vPrev), I);
@@ -163,6 +184,7 @@ k_back(Net n, int t, const float* w, const float* uSeg, int segStart, const floa
 				const int i = e < e1 ? n.post[e] : 0;
 				const float we = e < e1 ? w[n.wpos[e]] : 0.0f;
 				const int cnt = min(32, e1 - base);
+#pragma unroll 8
 				for(int q = 0; q < cnt; ++q) {
 					const int iq = __shfl_sync(FULL, i, q);
 					const float wq = __shfl_sync(FULL, we, q);
@@ -195,14 +217,78 @@ k_dw(Net n, int segStart, int segEnd, const float* guSeg, const uint32_t* sBits,
 			const int p = n.pre[k];
 			float acc = 0.0f;
 			for(int t = segStart; t < segEnd; ++t) {
-				const float g = guSeg[(size_t(t - segStart) * n.N + i) * 32 + lane];
-				acc = __fadd_rn(acc, __fmul_rn(g, presyn<RELAXED>(n, p, t, lane, sBits, sF, inBits)));
+				if(RELAXED) {
+					const float g = guSeg[(size_t(t - segStart) * n.N + i) * 32 + lane];
+					acc = __fadd_rn(acc, __fmul_rn(g, presyn<RELAXED>(n, p, t, lane, sBits, sF, inBits)));
+				} else {
+					/* spikes are 0 or 1: add gu where the trial's bit is set */
+					const uint32_t word = presynWord(n, p, t, sBits, inBits);
+					if(word && ((word >> lane) & 1u)) {
+						acc = __fadd_rn(acc, guSeg[(size_t(t - segStart) * n.N + i) * 32 + lane]);
+					}
+				}
 			}
 #pragma unroll
 			for(int d = 16; d; d >>= 1) acc = __fadd_rn(acc, __shfl_xor_sync(FULL, acc, d));
 			if(lane == 0) dw[k] = __fadd_rn(dw[k], acc);
 		}
 	}
+}
+
+/* dL/dw over one segment for spikes as bits: lanes over the neuron's
+ * in-synapses, each lane walking its synapse's presynaptic words along the
+ * segment (words stored source-major, [unit][T], so consecutive steps are
+ * consecutive words) and adding gu[t]_i of every trial whose bit is set. */
+__global__ void __launch_bounds__(THREADS)
+k_dw_bits(Net n, int segStart, int segEnd, const float* guSeg, const uint32_t* sT, const uint32_t* inT, float* dw)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	const int warps = int((gridDim.x * blockDim.x) >> 5);
+	for(int i = int((blockIdx.x * blockDim.x + threadIdx.x) >> 5); i < n.N; i += warps) {
+		const int k0 = n.rowptr[i], k1 = n.rowptr[i + 1];
+		for(int base = k0; base < k1; base += 32) {
+			const int k = base + int(lane);
+			if(k >= k1) continue;
+			const int p = n.pre[k];
+			const bool input = p >= n.N;
+			const uint32_t* words = input ? inT + size_t(p - n.N) * n.T : sT + size_t(p) * n.T;
+			float acc = 0.0f;
+			for(int t = segStart; t < segEnd; ++t) {
+				uint32_t word = input ? words[t] : (t == 0 ? 0u : words[t - 1]);
+				while(word) {
+					const int b = __ffs(int(word)) - 1;
+					word &= word - 1u;
+					acc = __fadd_rn(acc, __ldg(&guSeg[(size_t(t - segStart) * n.N + i) * 32 + b]));
+				}
+			}
+			dw[k] = __fadd_rn(dw[k], acc);
+		}
+	}
+}
+
+/* dst[c][r] = src[r][c] for a rows x cols array of words */
+__global__ void
+k_transpose(const uint32_t* src, uint32_t* dst, int rows, int cols)
+{
+	__shared__ uint32_t tile[32][33];
+	const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+	for(int y = threadIdx.y; y < 32; y += blockDim.y) {
+		const int r = r0 + y, c = c0 + int(threadIdx.x);
+		if(r < rows && c < cols) tile[y][threadIdx.x] = src[size_t(r) * cols + c];
+	}
+	__syncthreads();
+	for(int y = threadIdx.y; y < 32; y += blockDim.y) {
+		const int c = c0 + y, r = r0 + int(threadIdx.x);
+		if(r < rows && c < cols) dst[size_t(c) * rows + r] = tile[threadIdx.x][y];
+	}
+}
+
+static void
+transpose(const uint32_t* src, uint32_t* dst, int rows, int cols, cudaStream_t st)
+{
+	if(rows == 0 || cols == 0) return;
+	dim3 g((cols + 31) / 32, (rows + 31) / 32), b(32, 8);
+	k_transpose<<<g, b, 0, st>>>(src, dst, rows, cols);
 }
 
 static int
@@ -237,12 +323,13 @@ validate(const Net& n)
 
 using namespace nemo_b200;
 
-/* work buffer: v state [N][32], the segment's u and gu [K][N][32], gu of the
- * step after the segment [N][32] */
+/* work buffer: v state [N][32], gu of the step after the segment [N][32],
+ * the segment's u and gu [K][N][32], then the spike and input words
+ * transposed to [unit][T] */
 static size_t
 workFloats(const lif::Net& n)
 {
-	return size_t(n.N) * 32 * (2 + 2 * size_t(n.K));
+	return size_t(n.N) * 32 * (2 + 2 * size_t(n.K)) + (size_t(n.N) + size_t(n.C)) * size_t(n.T);
 }
 
 static std::string g_lifError;
@@ -306,6 +393,12 @@ nemo_b200_lif_backward(const nemo_b200_lif_net* net, const float* w, const uint3
 		float* guNextSeg = work + NS;          /* gu of the first step after the segment */
 		float* uSeg = work + 2 * NS;
 		float* guSeg = uSeg + size_t(n.K) * NS;
+		uint32_t* sT = reinterpret_cast<uint32_t*>(guSeg + size_t(n.K) * NS);
+		uint32_t* inT = sT + size_t(n.N) * n.T;
+		if(!relaxed) {
+			lif::transpose(s_bits, sT, n.T, n.N, st);
+			lif::transpose(in_bits, inT, n.T, n.C, st);
+		}
 		const int g = lif::grid(n.N);
 		const int segments = (n.T + n.K - 1) / n.K;
 		for(int sgi = segments - 1; sgi >= 0; --sgi) {
@@ -330,7 +423,7 @@ nemo_b200_lif_backward(const nemo_b200_lif_net* net, const float* w, const uint3
 			if(relaxed) {
 				lif::k_dw<true><<<g, lif::THREADS, 0, st>>>(n, c0, c1, guSeg, s_bits, s_float, in_bits, dw);
 			} else {
-				lif::k_dw<false><<<g, lif::THREADS, 0, st>>>(n, c0, c1, guSeg, s_bits, s_float, in_bits, dw);
+				lif::k_dw_bits<<<g, lif::THREADS, 0, st>>>(n, c0, c1, guSeg, sT, inT, dw);
 			}
 			NEMO_CUDA(cudaMemcpyAsync(guNextSeg, guSeg, NS * 4, cudaMemcpyDeviceToDevice, st));
 		}
