@@ -415,12 +415,25 @@ def run_batched(args):
     d.nemo_b200_counters.argtypes = [ctypes.c_void_p, ctypes.c_uint64 * 4]
     d.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
     d.nemo_delete_simulation.argtypes = [ctypes.c_void_p]
+    import torch
+    import torch.distributed as dist
+    from nemo_b200.dist import shard_instances
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     count, cycles = args.batch_count, 1000
-    sizes = netgen.batched_sizes(count, 500, 20000, seed=3)
+    sizes_all = netgen.batched_sizes(count, 500, 20000, seed=3)
     rng = np.random.default_rng(4)
     sig = rng.uniform(3.0, 7.0, size=count)
-    specs = [netgen.izhikevich_random(int(n), 100, dmax=20, seed=1000 + j, sigma_exc=float(sig[j]),
-                                      sigma_inh=float(0.4 * sig[j])) for j, n in enumerate(sizes)]
+    # several GPUs: the networks are split over the ranks (strong scaling)
+    mine = shard_instances(sizes_all, world)[rank]
+    sizes = sizes_all[mine]
+    specs = [netgen.izhikevich_random(int(sizes_all[j]), 100, dmax=20, seed=1000 + j, sigma_exc=float(sig[j]),
+                                      sigma_inh=float(0.4 * sig[j])) for j in mine]
+    count = len(mine)
 
     def counters(handle):
         c = (ctypes.c_uint64 * 4)()
@@ -448,6 +461,21 @@ def run_batched(args):
     batched_s = time.perf_counter() - t0
     events = counters(batch)[3] - before[3]
     d.nemo_delete_simulation(batch)
+    if world > 1:
+        t = torch.tensor([batched_s, float(events)], dtype=torch.float64, device="cuda")
+        mx = t[:1].clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        batched_s, events = float(mx[0]), int(t[1])
+        line = {"metric": "synaptic events/s (batched form)", "value": round(events / batched_s, 1), "unit": UNIT,
+                "n_gpus": world, "scaling": "strong", "higher_is_better": True, "data": "synthetic (seeded generator)",
+                "config": {"workload": "izhikevich-batch-%d-m100" % args.batch_count, "cycles": cycles,
+                           "instances_per_rank": "largest first to the least loaded rank"},
+                "batched": {"seconds": round(batched_s, 4), "events": events, "graph_used": bool(used.value)}}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dist.destroy_process_group()
+        return
     batched = events / batched_s
 
     # the same networks one after another
@@ -506,12 +534,21 @@ def run_bptt(args):
     sin(2 pi 4 t) Hz; gradient w.r.t. all weights through the adjoint kernel
     (fast-sigmoid surrogate, slope 10, checkpoints every 50 steps)."""
     import torch
+    import torch.distributed as dist
+    from nemo_b200.dist import dp_grad
     from nemo_b200.lif import LIFNetwork, lif_bptt, poisson_bits, rate_loss, sinusoid_target
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     n, fan, chans, infan, steps, trials, binsteps = 10000, 200, 500, 50, 500, 32, 10
     t0 = time.perf_counter()
     net = LIFNetwork.random(n, fan, chans, infan, seed=7, checkpoint=50, bin_steps=binsteps, kappa=10.0)
     w = net.initial_weights(seed=7, scale_in=0.35).requires_grad_(True)
-    bits, _ = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8)
+    # data parallel over trials: every rank runs 32 trials of its own
+    bits, _ = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8 + 1000 * rank)
     target = sinusoid_target(steps // binsteps, binsteps)
     build_s = time.perf_counter() - t0
 
@@ -520,10 +557,13 @@ def run_bptt(args):
         counts = lif_bptt(w, bits, net, trials)
         loss = rate_loss(counts, n, binsteps, target)
         loss.backward()
+        dp_grad(w.grad, trials, trials * world)   # one all-reduce of the weight gradient
         return loss, counts
 
     for _ in range(max(args.warmup, 1)):
         grad_step()
+    if world > 1:
+        dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     k = max(args.steps if args.steps < 100 else 10, 1)
@@ -533,6 +573,10 @@ def run_bptt(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / k
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t[0])
     rate = counts.sum().item() / (trials * n * steps / 1000.0)
     # the forward and the adjoint alone
     from nemo_b200.lif import lif_backward, lif_forward
@@ -546,7 +590,8 @@ def run_bptt(args):
     torch.cuda.synchronize()
     fwd_ms, bwd_ms = f0.elapsed_time(f1), f1.elapsed_time(b1)
     line = {
-        "metric": "BPTT grad steps/s", "value": round(1000.0 / ms, 3), "unit": "grad steps/s", "n_gpus": 1,
+        "metric": "BPTT grad steps/s", "value": round(1000.0 / ms, 3), "unit": "grad steps/s", "n_gpus": world,
+        "scaling": "weak", "global_trials": trials * world,
         "steps": k, "warmup": max(args.warmup, 1), "ms_per_step": round(ms, 3), "higher_is_better": True,
         "dtype": "f32", "data": "synthetic (seeded Poisson inputs)",
         "config": {"workload": "lif-bptt-10k-200", "neurons": n, "recurrent_synapses_per_neuron": fan,
@@ -554,9 +599,12 @@ def run_bptt(args):
                    "steps": steps, "checkpoint_every": 50, "surrogate": "1/(1+10|u-theta|)^2"},
         "loss": round(loss.item(), 3), "mean_rate_hz": round(rate, 3), "build_s": round(build_s, 2),
         "forward_ms": round(fwd_ms, 3), "backward_ms": round(bwd_ms, 3),
-        "synapse_steps_per_s": round(net.synapses * trials * steps / (ms * 1e-3), 1),
+        "synapse_steps_per_s": round(net.synapses * trials * world * steps / (ms * 1e-3), 1),
     }
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def main():
