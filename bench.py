@@ -607,6 +607,69 @@ def run_bptt(args):
         dist.destroy_process_group()
 
 
+def run_mixed(args):
+    """The mixed-plugin network: 50,000 neurons (20k Izhikevich RS/FS with no
+    noise, 15k IF_curr_exp, 10k QIF, 5k Hodgkin-Huxley), 500 synapses per
+    neuron across all populations, delays U{1..10}, weights 0.3 U (excitatory)
+    / -0.6 U (inhibitory Izhikevich sources); Poisson input at 5 Hz per neuron
+    as firing stimulus through nemo_step, one Bernoulli(0.005) draw per neuron
+    per cycle, seeded. Timed through the C ABI (stimulus copied in, fired list
+    copied out every cycle); the reference CPU restatement on a bounded
+    sample of the same cycles."""
+    lib = Library()
+    spec = netgen.mixed_plugins(seed=2)
+    n = spec.neuron_count
+    cycles = args.mixed_cycles
+    rng = np.random.default_rng(5)
+    stim = [np.nonzero(rng.random(n) < 0.005)[0].astype(np.uint32) for _ in range(cycles)]
+    outdeg = spec.out_degree()
+    P = ctypes.POINTER
+
+    def run(sim_lib, sim, count):
+        fptr = P(ctypes.c_uint)()
+        nf = ctypes.c_size_t()
+        events = 0
+        t0 = time.perf_counter()
+        for c in range(count):
+            f = stim[c]
+            st = sim_lib.dll.nemo_step(sim.handle, f.ctypes.data_as(P(ctypes.c_uint)), f.size, None, None, 0,
+                                       ctypes.byref(fptr), ctypes.byref(nf))
+            if st != 0:
+                raise RuntimeError(sim_lib.dll.nemo_strerror().decode())
+            if nf.value:
+                events += int(outdeg[np.ctypeslib.as_array(fptr, shape=(nf.value,))].sum())
+        return time.perf_counter() - t0, events
+
+    net = spec.build(Network(lib))
+    sim = Simulation(net, Configuration(lib))
+    del net
+    run(lib, sim, min(20, cycles))            # warm-up (the same stimulus is reused below)
+    sim2 = None
+    net = spec.build(Network(lib))
+    sim2 = Simulation(net, Configuration(lib))
+    del net, sim
+    secs, events = run(lib, sim2, cycles)
+    line = {"metric": "synaptic events/s (mixed plugins)", "value": round(events / secs, 1), "unit": UNIT,
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic (seeded generator, seeded Poisson stimulus)",
+            "config": {"workload": "mixed-50k-m500", "neurons": n, "synapses": spec.synapse_count,
+                       "populations": "20k Izhikevich, 15k IF_curr_exp, 10k QIF, 5k HH", "cycles": cycles,
+                       "stimulus": "Bernoulli(0.005) firing stimulus per neuron per cycle"},
+            "sim_ms_per_wall_s": round(cycles / secs, 2), "seconds": round(secs, 3), "events": events}
+    if not args.no_cpu_baseline:
+        ol = Library(oracle_library())
+        net = spec.build(Network(ol))
+        conf = Configuration(ol)
+        conf.set_cpu_backend()
+        osim = Simulation(net, conf)
+        del net
+        k = max(1, min(args.cpu_steps, cycles))
+        osecs, oev = run(ol, osim, k)
+        line["cpu_baseline"] = {"value": round(oev / osecs, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": "first %d cycles, %.1f s" % (k, osecs),
+                                "sim_ms_per_wall_s": round(k / osecs, 3)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -622,8 +685,13 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--bptt", action="store_true",
                     help="measure the differentiable form (BPTT grad steps/s) instead of the headline workload")
+    ap.add_argument("--mixed", action="store_true",
+                    help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
+    ap.add_argument("--mixed-cycles", type=int, default=1000)
     args = ap.parse_args()
-    if args.bptt:
+    if args.mixed:
+        run_mixed(args)
+    elif args.bptt:
         run_bptt(args)
     elif args.batched:
         run_batched(args)

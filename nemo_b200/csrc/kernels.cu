@@ -348,7 +348,33 @@ __device__ __forceinline__ bool modelQif(const NetDev& net, const GroupDev& g, u
 
 __device__ __forceinline__ float expfMatch(const NetDev& net, float x)
 {
-	return libm::expf_match(x, net.expKeys, net.expValues, net.expCount, net.expKfac);
+	return libm::expf_match(x, net.expSlots, net.expBits, net.expProbe, net.expNear);
+}
+
+/* glibc expf of six arguments: the six double candidates first, free of
+ * branches so that their dependency chains interleave, then the table lookup
+ * for the few inputs whose candidate lies near a rounding boundary. */
+__device__ __forceinline__ void expfMatch6(const NetDev& net, const float (&x)[6], float (&y)[6])
+{
+	double c[6];
+#pragma unroll
+	for(int k = 0; k < 6; ++k) {
+		c[k] = libm::exp_candidate_d(x[k]);
+		y[k] = float(c[k]);
+	}
+	unsigned near = 0;
+#pragma unroll
+	for(int k = 0; k < 6; ++k) {
+		near |= libm::exp_midpoint_units(c[k]) <= net.expNear ? 1u << k : 0u;
+	}
+	if(near && net.expProbe) {
+#pragma unroll
+		for(int k = 0; k < 6; ++k) {
+			if(near & (1u << k)) {
+				y[k] = libm::exp_lookup(x[k], y[k], net.expSlots, net.expBits, net.expProbe);
+			}
+		}
+	}
 }
 
 /* Hodgkin-Huxley (src/nemo/cpu/plugins/HH.cpp:14-137): state v, n, m, h, dir;
@@ -376,21 +402,25 @@ __device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, ui
 	const float ENa = __fsub_rn(115.0f, 65.0f);
 	const float EK = __fsub_rn(-12.0f, 65.0f);
 	const float EL = __fsub_rn(10.6f, 65.0f);
-	const float C = 1.0f, RevE = 0.0f, RevI = -70.0f;
+	const float RevE = 0.0f, RevI = -70.0f;
 	const int incMax = int(__fdiv_rn(1.0f, dt));
 	bool fired = false;
 	for(int t = 0; t < incMax; ++t) {
 		const float vr = __fadd_rn(v, 65.0f);
+		/* (RevI - v) / -1 is the exact negation */
 		const float I = __fadd_rn(__fadd_rn(__fmul_rn(Excit, __fsub_rn(RevE, v)),
-					__fmul_rn(Inhib, __fdiv_rn(__fsub_rn(RevI, v), -1.0f))), Exter);
-		const float alphan = __fdiv_rn(__fsub_rn(0.1f, __fmul_rn(0.01f, vr)),
-				__fsub_rn(expfMatch(net, __fsub_rn(1.0f, __fmul_rn(0.1f, vr))), 1.0f));
-		const float alpham = __fdiv_rn(__fsub_rn(2.5f, __fmul_rn(0.1f, vr)),
-				__fsub_rn(expfMatch(net, __fsub_rn(2.5f, __fmul_rn(0.1f, vr))), 1.0f));
-		const float alphah = __fmul_rn(0.07f, expfMatch(net, __fdiv_rn(-vr, 20.0f)));
-		const float betan = __fmul_rn(0.125f, expfMatch(net, __fdiv_rn(-vr, 80.0f)));
-		const float betam = __fmul_rn(4.0f, expfMatch(net, __fdiv_rn(-vr, 18.0f)));
-		const float betah = __fdiv_rn(1.0f, __fadd_rn(expfMatch(net, __fsub_rn(3.0f, __fmul_rn(0.1f, vr))), 1.0f));
+					__fmul_rn(Inhib, -__fsub_rn(RevI, v))), Exter);
+		const float x[6] = {__fsub_rn(1.0f, __fmul_rn(0.1f, vr)), __fsub_rn(2.5f, __fmul_rn(0.1f, vr)),
+			__fdiv_rn(-vr, 20.0f), __fdiv_rn(-vr, 80.0f), __fdiv_rn(-vr, 18.0f),
+			__fsub_rn(3.0f, __fmul_rn(0.1f, vr))};
+		float e[6];
+		expfMatch6(net, x, e);
+		const float alphan = __fdiv_rn(__fsub_rn(0.1f, __fmul_rn(0.01f, vr)), __fsub_rn(e[0], 1.0f));
+		const float alpham = __fdiv_rn(__fsub_rn(2.5f, __fmul_rn(0.1f, vr)), __fsub_rn(e[1], 1.0f));
+		const float alphah = __fmul_rn(0.07f, e[2]);
+		const float betan = __fmul_rn(0.125f, e[3]);
+		const float betam = __fmul_rn(4.0f, e[4]);
+		const float betah = __fdiv_rn(1.0f, __fadd_rn(e[5], 1.0f));
 		m = __fadd_rn(m, __fmul_rn(dt, __fsub_rn(__fmul_rn(alpham, __fsub_rn(1.0f, m)), __fmul_rn(betam, m))));
 		nn = __fadd_rn(nn, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphan, __fsub_rn(1.0f, nn)), __fmul_rn(betan, nn))));
 		h = __fadd_rn(h, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphah, __fsub_rn(1.0f, h)), __fmul_rn(betah, h))));
@@ -400,7 +430,8 @@ __device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, ui
 					__fmul_rn(__fmul_rn(__fmul_rn(gNa, m3), h), __fsub_rn(v, ENa)),
 					__fmul_rn(__fmul_rn(gK, n4), __fsub_rn(v, EK))),
 				__fmul_rn(gL, __fsub_rn(v, EL)));
-		const float newv = __fadd_rn(v, __fdiv_rn(__fmul_rn(dt, __fadd_rn(-Ik, I)), C));
+		/* division by C = 1 is exact */
+		const float newv = __fadd_rn(v, __fmul_rn(dt, __fadd_rn(-Ik, I)));
 		const float newDir = __fsub_rn(newv, v);
 		const float change = ((dir < 0.0f) | (newv < -45.0f)) ? 0.0f : newDir;
 		dir = newDir;

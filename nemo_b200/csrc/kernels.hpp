@@ -115,12 +115,13 @@ struct NetDev {
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;
 	const uint32_t* logTab;
-	/* expf exceptions (libm_tables.hpp ExpExceptions): sorted input bits,
-	 * glibc results, count, and 0.5 - tau */
-	const uint32_t* expKeys;
-	const uint32_t* expValues;
-	uint32_t expCount;
-	double expKfac;
+	/* expf exceptions (libm_tables.hpp ExpExceptions) as the hash of
+	 * libm::exp_lookup: slots, log2 of their count, probe bound (0: no
+	 * table), and the largest libm::exp_midpoint_units of an exception */
+	const uint64_t* expSlots;
+	uint32_t expBits;
+	uint32_t expProbe;
+	uint32_t expNear;
 
 	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
 	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */

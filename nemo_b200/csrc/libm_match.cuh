@@ -43,12 +43,14 @@
 #define D_SUB(a, b) __dsub_rn((a), (b))
 #define D_MUL(a, b) __dmul_rn((a), (b))
 #define D_DIV(a, b) __ddiv_rn((a), (b))
+#define D_FMA(a, b, c) __fma_rn((a), (b), (c))
 #else
 /* Host builds of this header must use -ffp-contract=off. */
 #define D_ADD(a, b) ((a) + (b))
 #define D_SUB(a, b) ((a) - (b))
 #define D_MUL(a, b) ((a) * (b))
 #define D_DIV(a, b) ((a) / (b))
+#define D_FMA(a, b, c) __builtin_fma((a), (b), (c))
 #endif
 
 /* On the device, host-only names are not available; keep the header free of
@@ -201,84 +203,100 @@ LIBM_HD float sin_candidate(float a) { return float(sin_candidate_d(double(a)));
 LIBM_HD float log_candidate(float y) { return float(log_candidate_d(y)); }
 
 /* exp(x) of a float x, evaluated in double with explicitly rounded
- * operations (identical on host and device): x = k ln2 + r with the
- * Cody-Waite split of ln2 (|r| <= ln2/2), e^r by its Taylor series to degree
- * 13 in Horner form, scaled by 2^k. Beyond the float range: 0 below -104,
- * infinity above 89; NaN stays NaN. */
+ * operations, fused multiply-adds included (identical on host and device):
+ * k = round(x / ln2) by adding 1.5 * 2^52 (the fused x * (1/ln2) + 1.5 * 2^52
+ * rounds once, to a double whose last place is 1), r = x - k ln2 with the
+ * Cody-Waite split of ln2 (|r| <= 0.3466), e^r by its Taylor series to degree
+ * 11 (truncation below 7e-15 relative) in Estrin's scheme, scaled by 2^k.
+ * Beyond the float range: 0 below -104, infinity above 89; NaN stays NaN.
+ * The result is branch-free, so that several evaluations interleave. */
 LIBM_HD double exp_candidate_d(float xf) {
-	if(!(xf == xf)) return double(xf);
-	if(xf > 89.0f) return u2d(0x7FF0000000000000ull);
-	if(xf < -104.0f) return 0.0;
-	const double invln2 = 1.4426950408889634;
 	const double ln2_hi = 6.93147180369123816490e-01;  /* 0x3FE62E42FEE00000 */
 	const double ln2_lo = 1.90821492927058770002e-10;
+	const double shift = 6755399441055744.0;            /* 1.5 * 2^52 */
 	const double x = double(xf);
-	const double t = D_MUL(x, invln2);
+	const double t = D_FMA(x, 1.4426950408889634, shift);
+	const double kd = D_SUB(t, shift);
+	const uint32_t k = uint32_t(d2u(t));                /* k mod 2^32 */
+	const double r = D_FMA(-kd, ln2_lo, D_FMA(-kd, ln2_hi, x));
+	/* 1/n! for n = 0..11, rounded to double */
+	const double r2 = D_MUL(r, r);
+	const double a0 = D_FMA(r, 1.0, 1.0);
+	const double a1 = D_FMA(r, 0.16666666666666666, 0.5);
+	const double a2 = D_FMA(r, 0.008333333333333333, 0.041666666666666664);
+	const double a3 = D_FMA(r, 0.0001984126984126984, 0.001388888888888889);
+	const double a4 = D_FMA(r, 2.7557319223985893e-06, 2.48015873015873e-05);
+	const double a5 = D_FMA(r, 2.505210838544172e-08, 2.755731922398589e-07);
+	const double r4 = D_MUL(r2, r2);
+	const double b0 = D_FMA(r2, a1, a0);
+	const double b1 = D_FMA(r2, a3, a2);
+	const double b2 = D_FMA(r2, a5, a4);
+	const double r8 = D_MUL(r4, r4);
+	const double p = D_FMA(r8, b2, D_FMA(r4, b1, b0));
+	/* 2^k is a normal double for every k the range [-104, 89] gives */
+	double res = D_MUL(p, u2d(uint64_t((1023u + k) & 0x7FFu) << 52));
+	res = xf > 89.0f ? u2d(0x7FF0000000000000ull) : res;
+	res = xf < -104.0f ? 0.0 : res;
+	return xf == xf ? res : x;
+}
+
+/* How close the double candidate c lies to a float rounding midpoint: the
+ * distance in units of 2^-29 of the float spacing, read from the low 29 bits
+ * of the double's significand (the part of c below the float spacing; the
+ * midpoint is 2^28). Exact integer arithmetic, for c in the float normal
+ * range [2^-126, 2^128); 0 outside it, so that such candidates always count
+ * as near. */
+LIBM_HD uint32_t exp_midpoint_units(double c) {
+	const uint64_t b = d2u(c);
+	const uint32_t e = uint32_t(b >> 52) & 0x7FFu;
+	if(e < 897u || e > 1150u) return 0u;
+	const int32_t d = int32_t(uint32_t(b) & 0x1FFFFFFFu) - 0x10000000;
+	return uint32_t(d < 0 ? -d : d);
+}
+
+/* The exception table as an open-addressing hash: 2^bits slots of
+ * (glibc result bits << 32 | input bits), linear probing from exp_hash(key);
+ * empty slots hold EXP_EMPTY_KEY, which is no float in [-104, 89]. A probe
+ * sequence never runs longer than `probe` slots (the longest run of occupied
+ * slots plus one), so an absent key meets an empty slot within the bound. */
+#define LIBM_EXP_EMPTY_KEY 0xFFFFFFFFu
+
+LIBM_HD uint32_t exp_hash(uint32_t key, uint32_t bits) {
+	return (key * 0x9E3779B1u) >> (32u - bits);
+}
+
+LIBM_HD uint64_t exp_slot_load(const uint64_t* p) {
 #ifdef __CUDA_ARCH__
-	const int k = __double2int_rn(t);
+	return __ldg((const unsigned long long*) p);
 #else
-	const int k = int(nearbyint(t));
+	return *p;
 #endif
-	const double kd = double(k);
-	const double r = D_SUB(D_SUB(x, D_MUL(kd, ln2_hi)), D_MUL(kd, ln2_lo));
-	double p = 1.6059043836821613e-10;           /* 1/13! */
-	p = D_ADD(D_MUL(p, r), 2.08767569878681e-09);   /* 1/12! */
-	p = D_ADD(D_MUL(p, r), 2.505210838544172e-08);  /* 1/11! */
-	p = D_ADD(D_MUL(p, r), 2.755731922398589e-07);  /* 1/10! */
-	p = D_ADD(D_MUL(p, r), 2.7557319223985893e-06); /* 1/9! */
-	p = D_ADD(D_MUL(p, r), 2.48015873015873e-05);   /* 1/8! */
-	p = D_ADD(D_MUL(p, r), 0.0001984126984126984);  /* 1/7! */
-	p = D_ADD(D_MUL(p, r), 0.001388888888888889);   /* 1/6! */
-	p = D_ADD(D_MUL(p, r), 0.008333333333333333);   /* 1/5! */
-	p = D_ADD(D_MUL(p, r), 0.041666666666666664);   /* 1/4! */
-	p = D_ADD(D_MUL(p, r), 0.16666666666666666);    /* 1/3! */
-	p = D_ADD(D_MUL(p, r), 0.5);
-	p = D_ADD(D_MUL(p, r), 1.0);
-	p = D_ADD(D_MUL(p, r), 1.0);
-	return D_MUL(p, u2d(uint64_t(1023 + k) << 52));
 }
 
-/* How far the double candidate c lies from the float rounding boundary, in
- * units of the float spacing at float(c): 0.5 - |c - float(c)| / spacing,
- * i.e. 0 on a midpoint and 0.5 on a float. Infinity and NaN give 1. */
-LIBM_HD double exp_boundary(double c) {
-	const float r = float(c);
-	const uint32_t rb = f2u(r);
-	if((rb & 0x7F800000u) == 0x7F800000u) return 1.0;
-	const float nb = u2f(double(r) < c ? rb + 1u : (rb == 0u ? 1u : rb - 1u));
-	const double spacing = double(nb) > double(r) ? D_SUB(double(nb), double(r)) : D_SUB(double(r), double(nb));
-	const double off = c > double(r) ? D_SUB(c, double(r)) : D_SUB(double(r), c);
-	return D_SUB(0.5, D_DIV(off, spacing));
-}
-
-/* Whether the candidate c lies within (0.5 - kfac) spacings of the float
- * rounding boundary (kfac = 0.5 - tau, tau from the exception table); the
- * division-free form of exp_boundary(c) <= tau. */
-LIBM_HD bool exp_near_boundary(double c, double kfac) {
-	const float r = float(c);
-	const uint32_t rb = f2u(r);
-	if((rb & 0x7F800000u) == 0x7F800000u) return false;
-	const float nb = u2f(double(r) < c ? rb + 1u : (rb == 0u ? 1u : rb - 1u));
-	const double spacing = double(nb) > double(r) ? D_SUB(double(nb), double(r)) : D_SUB(double(r), double(nb));
-	const double off = c > double(r) ? D_SUB(c, double(r)) : D_SUB(double(r), c);
-	return off >= D_MUL(kfac, spacing);
+/* glibc's result for an input on which glibc rounds the other way from the
+ * candidate; `fallback` (the rounded candidate) when the input is not in the
+ * table. */
+LIBM_HD float exp_lookup(float x, float fallback, const uint64_t* slots, uint32_t bits, uint32_t probe) {
+	const uint32_t key = f2u(x);
+	const uint32_t mask = (1u << bits) - 1u;
+	uint32_t h = exp_hash(key, bits);
+	for(uint32_t k = 0; k < probe; ++k) {
+		const uint64_t e = exp_slot_load(slots + h);
+		const uint32_t ek = uint32_t(e);
+		if(ek == key) return u2f(uint32_t(e >> 32));
+		if(ek == LIBM_EXP_EMPTY_KEY) break;
+		h = (h + 1u) & mask;
+	}
+	return fallback;
 }
 
 /* glibc expf: the rounded candidate, or the exception table's value for an
- * input on which glibc rounds the other way (keys sorted) */
-LIBM_HD float expf_match(float x, const uint32_t* keys, const uint32_t* values, uint32_t count, double kfac) {
+ * input on which glibc rounds the other way (only candidates within
+ * `nearUnits` of a midpoint can be such inputs) */
+LIBM_HD float expf_match(float x, const uint64_t* slots, uint32_t bits, uint32_t probe, uint32_t nearUnits) {
 	const double c = exp_candidate_d(x);
-	float r = float(c);
-	if(count && exp_near_boundary(c, kfac)) {
-		const uint32_t key = f2u(x);
-		uint32_t lo = 0, hi = count;
-		while(lo < hi) {
-			const uint32_t mid = (lo + hi) >> 1;
-			if(keys[mid] < key) lo = mid + 1;
-			else hi = mid;
-		}
-		if(lo < count && keys[lo] == key) r = u2f(values[lo]);
-	}
+	const float r = float(c);
+	if(probe && exp_midpoint_units(c) <= nearUnits) return exp_lookup(x, r, slots, bits, probe);
 	return r;
 }
 

@@ -184,7 +184,7 @@ libmCachePath()
 /* ---- expf exceptions (the HH plugin's exp, src/nemo/cpu/plugins/HH.cpp:92-98) ---- */
 
 static const uint32_t EXP_MAGIC = 0x4e4d4558u; /* "NMEX" */
-static const uint32_t EXP_VERSION = 1u;
+static const uint32_t EXP_VERSION = 2u;
 
 static std::string
 expCachePath()
@@ -192,12 +192,12 @@ expCachePath()
 	std::string p = cachePath();
 	size_t slash = p.rfind('/');
 	std::string dir = slash == std::string::npos ? std::string(".") : p.substr(0, slash);
-	return dir + "/expf_exceptions_v1_glibc-" + gnu_get_libc_version() + ".bin";
+	return dir + "/expf_exceptions_v2_glibc-" + gnu_get_libc_version() + ".bin";
 }
 
 struct ExpPart {
 	std::vector<uint32_t> keys, values;
-	double tau = 0.0;
+	uint32_t nearUnits = 0;
 	unsigned long bad = 0;
 };
 
@@ -214,7 +214,7 @@ buildExpRange(uint32_t lo, uint32_t hi, unsigned stride, unsigned offset, ExpPar
 			if(d != 1 && d != -1) out->bad++;
 			out->keys.push_back(uint32_t(u));
 			out->values.push_back(f2u(g));
-			out->tau = std::max(out->tau, exp_boundary(c));
+			out->nearUnits = std::max(out->nearUnits, exp_midpoint_units(c));
 		}
 	}
 }
@@ -236,11 +236,10 @@ buildExpExceptions()
 	unsigned long bad = 0;
 	for(const ExpPart& p : parts) {
 		for(size_t k = 0; k < p.keys.size(); ++k) all.emplace_back(p.keys[k], p.values[k]);
-		e.tau = std::max(e.tau, p.tau);
+		e.nearUnits = std::max(e.nearUnits, p.nearUnits);
 		bad += p.bad;
 	}
-	/* margin for the division-free test on the device (exp_near_boundary) */
-	e.tau += 1e-6;
+	e.tau = double(e.nearUnits) / double(1u << 29);
 	if(bad) {
 		fail(NEMO_LOGIC_ERROR, "expf exceptions: " + std::to_string(bad)
 				+ " inputs differ from glibc by more than one unit in the last place");
@@ -269,6 +268,7 @@ loadExpCache(const std::string& path, ExpExceptions& e)
 		e.keys.resize(hdr[2]);
 		e.values.resize(hdr[2]);
 		e.tau = tau;
+		e.nearUnits = uint32_t(tau * double(1u << 29) + 0.5);
 		ok = fread(e.keys.data(), 4, hdr[2], f) == hdr[2] && fread(e.values.data(), 4, hdr[2], f) == hdr[2];
 	}
 	fclose(f);
@@ -300,6 +300,44 @@ saveExpCache(const std::string& path, const ExpExceptions& e)
 	}
 }
 
+/* Insert every (key, value) pair by linear probing into a power-of-two table
+ * at most one third full; the probe bound is the longest cyclic run of
+ * occupied slots plus one. */
+static void
+buildExpSlots(ExpExceptions& e)
+{
+	uint32_t bits = 4;
+	while((uint64_t(1) << bits) < 3 * uint64_t(e.keys.size())) ++bits;
+	const uint32_t size = 1u << bits, mask = size - 1u;
+	e.slots.assign(size, uint64_t(LIBM_EXP_EMPTY_KEY));
+	for(size_t k = 0; k < e.keys.size(); ++k) {
+		uint32_t h = libm::exp_hash(e.keys[k], bits);
+		while(uint32_t(e.slots[h]) != LIBM_EXP_EMPTY_KEY) h = (h + 1u) & mask;
+		e.slots[h] = uint64_t(e.values[k]) << 32 | e.keys[k];
+	}
+	/* longest run of occupied slots, wrapping around the end */
+	uint32_t first = 0;
+	while(first < size && uint32_t(e.slots[first]) != LIBM_EXP_EMPTY_KEY) ++first;
+	uint32_t run = 0, longest = 0;
+	for(uint32_t k = 1; k <= size; ++k) {
+		if(uint32_t(e.slots[(first + k) & mask]) != LIBM_EXP_EMPTY_KEY) {
+			longest = std::max(longest, ++run);
+		} else {
+			run = 0;
+		}
+	}
+	e.slotBits = bits;
+	e.slotProbe = longest + 1;
+	/* every pair is found by the device's own lookup, with the same bound */
+	for(size_t k = 0; k < e.keys.size(); ++k) {
+		const float x = u2f(e.keys[k]);
+		const float miss = u2f(e.values[k] ^ 1u);
+		if(f2u(libm::exp_lookup(x, miss, e.slots.data(), bits, e.slotProbe)) != e.values[k]) {
+			fail(NEMO_LOGIC_ERROR, "expf exception hash: key " + std::to_string(e.keys[k]) + " not found");
+		}
+	}
+}
+
 const ExpExceptions&
 expExceptions()
 {
@@ -313,6 +351,7 @@ expExceptions()
 			table = buildExpExceptions();
 			saveExpCache(path, table);
 		}
+		buildExpSlots(table);
 		ready = true;
 	}
 	return table;

@@ -466,10 +466,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	for(const Group& g : m_groups) needExp = needExp || g.type.kind == MODEL_HH;
 	if(needExp) {
 		const ExpExceptions& e = expExceptions();
-		m_net.expKeys = (const uint32_t*) put(e.keys.data(), e.keys.size() * 4);
-		m_net.expValues = (const uint32_t*) put(e.values.data(), e.values.size() * 4);
-		m_net.expCount = uint32_t(e.keys.size());
-		m_net.expKfac = 0.5 - e.tau;
+		m_net.expSlots = (const uint64_t*) put(e.slots.data(), e.slots.size() * 8);
+		m_net.expBits = e.slotBits;
+		m_net.expProbe = e.slotProbe;
+		m_net.expNear = e.nearUnits;
 	}
 	if(needTables) {
 		const LibmTables& t = libmTables();
@@ -1320,18 +1320,16 @@ Simulation::expfCheck()
 	const ExpExceptions& e = expExceptions();
 	cudaStream_t stream = STREAM(m_stream);
 	NetDev net = m_net;
-	uint32_t *keys = nullptr, *vals = nullptr;
+	uint64_t* slots = nullptr;
 	float* dout = nullptr;
 	const uint32_t CHUNK = 1u << 26;
-	NEMO_CUDA(cudaMalloc(&keys, e.keys.size() * 4 + 4));
-	NEMO_CUDA(cudaMalloc(&vals, e.values.size() * 4 + 4));
+	NEMO_CUDA(cudaMalloc(&slots, e.slots.size() * 8));
 	NEMO_CUDA(cudaMalloc(&dout, size_t(CHUNK) * 4));
-	NEMO_CUDA(cudaMemcpyAsync(keys, e.keys.data(), e.keys.size() * 4, cudaMemcpyHostToDevice, stream));
-	NEMO_CUDA(cudaMemcpyAsync(vals, e.values.data(), e.values.size() * 4, cudaMemcpyHostToDevice, stream));
-	net.expKeys = keys;
-	net.expValues = vals;
-	net.expCount = uint32_t(e.keys.size());
-	net.expKfac = 0.5 - e.tau;
+	NEMO_CUDA(cudaMemcpyAsync(slots, e.slots.data(), e.slots.size() * 8, cudaMemcpyHostToDevice, stream));
+	net.expSlots = slots;
+	net.expBits = e.slotBits;
+	net.expProbe = e.slotProbe;
+	net.expNear = e.nearUnits;
 	std::vector<float> h(CHUNK);
 	uint64_t bad = 0;
 	const uint32_t ranges[2][2] = {{0u, libm::f2u(89.0f)}, {0x80000000u, libm::f2u(-104.0f)}};
@@ -1358,8 +1356,7 @@ Simulation::expfCheck()
 			for(uint64_t b : part) bad += b;
 		}
 	}
-	cudaFree(keys);
-	cudaFree(vals);
+	cudaFree(slots);
 	cudaFree(dout);
 	return bad;
 }
