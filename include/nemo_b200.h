@@ -210,6 +210,12 @@ nemo_status_t nemo_b200_libm_check(nemo_simulation_t sim, uint64_t* mismatches);
  * reproduces it bit for bit). */
 nemo_status_t nemo_b200_expf_check(nemo_simulation_t sim, uint64_t* mismatches);
 
+/* Diagnostics: the Hodgkin-Huxley model's divisions of -(v + 65) by 20, 80
+ * and 18 (an FMA-corrected product with the rounded reciprocal) against the
+ * device's correctly rounded division, on every float of magnitude at least
+ * 2^-100 and on the zeros; mismatches[q] per divisor (0 when they agree). */
+nemo_status_t nemo_b200_hh_division_check(uint64_t mismatches[3]);
+
 /* The host-built table of inputs on which glibc expf rounds differently from
  * the device candidate: its size and its boundary distance (built or loaded
  * from the cache on first use; no device needed). */

@@ -351,30 +351,18 @@ __device__ __forceinline__ float expfMatch(const NetDev& net, float x)
 	return libm::expf_match(x, net.expSlots, net.expBits, net.expProbe, net.expNear);
 }
 
-/* glibc expf of six arguments: the six double candidates first, free of
- * branches so that their dependency chains interleave, then the table lookup
- * for the few inputs whose candidate lies near a rounding boundary. */
-__device__ __forceinline__ void expfMatch6(const NetDev& net, const float (&x)[6], float (&y)[6])
+/* -a / d rounded to nearest for the constant divisors d of the HH rates,
+ * from y = RN(1/d): q0 = RN(a y), the exact residual a - q0 d by FMA, and
+ * one correction q0 + r y (Markstein's division step). Equal to __fdiv_rn(a,
+ * d) for every a with |a| >= 2^-100, zero or infinite (checked over all such
+ * floats by nemo_b200_hh_division_check); the HH argument v + 65 is zero or
+ * at least 2^-17 in magnitude, the spacing of floats near -65. */
+__device__ __forceinline__ float hhDivConst(float a, float d, float y)
 {
-	double c[6];
-#pragma unroll
-	for(int k = 0; k < 6; ++k) {
-		c[k] = libm::exp_candidate_d(x[k]);
-		y[k] = float(c[k]);
-	}
-	unsigned near = 0;
-#pragma unroll
-	for(int k = 0; k < 6; ++k) {
-		near |= libm::exp_midpoint_units(c[k]) <= net.expNear ? 1u << k : 0u;
-	}
-	if(near && net.expProbe) {
-#pragma unroll
-		for(int k = 0; k < 6; ++k) {
-			if(near & (1u << k)) {
-				y[k] = libm::exp_lookup(x[k], y[k], net.expSlots, net.expBits, net.expProbe);
-			}
-		}
-	}
+	const float q0 = __fmul_rn(a, y);
+	const float r = __fmaf_rn(-q0, d, a);
+	const float q1 = __fmaf_rn(r, y, q0);
+	return (r == 0.0f || !isfinite(q0)) ? q0 : q1;
 }
 
 /* Hodgkin-Huxley (src/nemo/cpu/plugins/HH.cpp:14-137): state v, n, m, h, dir;
@@ -382,20 +370,36 @@ __device__ __forceinline__ void expfMatch6(const NetDev& net, const float (&x)[6
  * potentials 0 and -70 mV. 999 Euler substeps of 0.001 ms ((int)(1/0.001f)
  * in float), six glibc-matching expf per substep; fires on the first
  * substep whose voltage change turns negative above -45 mV, from the 10th
- * cycle after the timer reset on. */
-__device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
-		float Excit, float Inhib, bool stim, uint32_t cycle)
+ * cycle after the timer reset on.
+ *
+ * Each neuron has eight lanes (device indices devBase + 8 i .. + 7; only the
+ * first is a neuron to the rest of the kernel). In a substep lane s of the
+ * eight evaluates the rate that needs exponential s (alpha_n, alpha_m,
+ * alpha_h, beta_n, beta_m, beta_h) and the six rates are exchanged by
+ * shuffles; every lane then advances the same state with the same
+ * operations. Called by all 32 lanes of a warp; `E`, `I` and the stimulus
+ * are taken from the neuron's first lane. Returns the neuron's firing on all
+ * its lanes. */
+__device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, uint32_t i, float E, float I,
+		uint32_t stimWord, uint32_t cycle, uint32_t lane)
 {
+	const uint32_t lead = lane & ~7u, s = lane & 7u;
+	const bool member = i < g.count;
 	const size_t c = g.count;
 	float* S = g.state;
-	const float Exter = net.ext[n];
-	float v = S[0 * c + i];
-	float nn = S[1 * c + i];
-	float m = S[2 * c + i];
-	float h = S[3 * c + i];
-	float dir = S[4 * c + i];
-	if(Exter != 0.0f) {
-		net.ext[n] = 0.0f;
+	const float Excit = __shfl_sync(FULL, E, lead);
+	const float Inhib = __shfl_sync(FULL, I, lead);
+	const bool stim = (stimWord >> lead) & 1u;
+	const uint32_t nLead = g.devBase + (i << 3);
+	const float Exter = member ? net.ext[nLead] : 0.0f;
+	float v = member ? S[0 * c + i] : -65.0f;
+	float nn = member ? S[1 * c + i] : 0.0f;
+	float m = member ? S[2 * c + i] : 0.0f;
+	float h = member ? S[3 * c + i] : 0.0f;
+	float dir = member ? S[4 * c + i] : 0.0f;
+	__syncwarp();
+	if(member && s == 0u && Exter != 0.0f) {
+		net.ext[nLead] = 0.0f;
 	}
 	const float dt = 0.001f;
 	const float gNa = 120.0f, gK = 36.0f, gL = 0.3f;
@@ -404,23 +408,39 @@ __device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, ui
 	const float EL = __fsub_rn(10.6f, 65.0f);
 	const float RevE = 0.0f, RevI = -70.0f;
 	const int incMax = int(__fdiv_rn(1.0f, dt));
+	/* this lane's exponent: a - 0.1 (v + 65) for s = 0, 1, 5 (a = 1, 2.5,
+	 * 3), -(v + 65) / d for s = 2, 3, 4 (d = 20, 80, 18), none for 6, 7 */
+	const bool argDiv = s >= 2u && s <= 4u;
+	const float argA = s == 0u ? 1.0f : (s == 1u ? 2.5f : 3.0f);
+	const float argD = s == 2u ? 20.0f : (s == 3u ? 80.0f : 18.0f);
+	const float argY = __fdiv_rn(1.0f, argD);
+	/* this lane's rate: num / (e -+ 1) for s = 0, 1, 5, coef * e for 2, 3, 4 */
+	const bool rateDiv = s <= 1u || s == 5u;
+	const float rateCoef = s == 2u ? 0.07f : (s == 3u ? 0.125f : 4.0f);
+	const bool lookup = net.expProbe != 0u;
 	bool fired = false;
 	for(int t = 0; t < incMax; ++t) {
 		const float vr = __fadd_rn(v, 65.0f);
 		/* (RevI - v) / -1 is the exact negation */
 		const float I = __fadd_rn(__fadd_rn(__fmul_rn(Excit, __fsub_rn(RevE, v)),
 					__fmul_rn(Inhib, -__fsub_rn(RevI, v))), Exter);
-		const float x[6] = {__fsub_rn(1.0f, __fmul_rn(0.1f, vr)), __fsub_rn(2.5f, __fmul_rn(0.1f, vr)),
-			__fdiv_rn(-vr, 20.0f), __fdiv_rn(-vr, 80.0f), __fdiv_rn(-vr, 18.0f),
-			__fsub_rn(3.0f, __fmul_rn(0.1f, vr))};
-		float e[6];
-		expfMatch6(net, x, e);
-		const float alphan = __fdiv_rn(__fsub_rn(0.1f, __fmul_rn(0.01f, vr)), __fsub_rn(e[0], 1.0f));
-		const float alpham = __fdiv_rn(__fsub_rn(2.5f, __fmul_rn(0.1f, vr)), __fsub_rn(e[1], 1.0f));
-		const float alphah = __fmul_rn(0.07f, e[2]);
-		const float betan = __fmul_rn(0.125f, e[3]);
-		const float betam = __fmul_rn(4.0f, e[4]);
-		const float betah = __fdiv_rn(1.0f, __fadd_rn(e[5], 1.0f));
+		const float tenth = __fmul_rn(0.1f, vr);
+		float x = argDiv ? hhDivConst(-vr, argD, argY) : __fsub_rn(argA, tenth);
+		x = s < 6u ? x : 0.0f;
+		const double cand = libm::exp_candidate_d(x);
+		float e = float(cand);
+		if(lookup && libm::exp_midpoint_units(cand) <= net.expNear) {
+			e = libm::exp_lookup(x, e, net.expSlots, net.expBits, net.expProbe);
+		}
+		const float num = s == 0u ? __fsub_rn(0.1f, __fmul_rn(0.01f, vr)) : (s == 1u ? __fsub_rn(2.5f, tenth) : 1.0f);
+		const float den = s == 5u ? __fadd_rn(e, 1.0f) : __fsub_rn(e, 1.0f);
+		const float rate = rateDiv ? __fdiv_rn(num, den) : __fmul_rn(rateCoef, e);
+		const float alphan = __shfl_sync(FULL, rate, lead + 0u);
+		const float alpham = __shfl_sync(FULL, rate, lead + 1u);
+		const float alphah = __shfl_sync(FULL, rate, lead + 2u);
+		const float betan = __shfl_sync(FULL, rate, lead + 3u);
+		const float betam = __shfl_sync(FULL, rate, lead + 4u);
+		const float betah = __shfl_sync(FULL, rate, lead + 5u);
 		m = __fadd_rn(m, __fmul_rn(dt, __fsub_rn(__fmul_rn(alpham, __fsub_rn(1.0f, m)), __fmul_rn(betam, m))));
 		nn = __fadd_rn(nn, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphan, __fsub_rn(1.0f, nn)), __fmul_rn(betan, nn))));
 		h = __fadd_rn(h, __fmul_rn(dt, __fsub_rn(__fmul_rn(alphah, __fsub_rn(1.0f, h)), __fmul_rn(betah, h))));
@@ -441,11 +461,13 @@ __device__ __forceinline__ bool modelHH(const NetDev& net, const GroupDev& g, ui
 		v = newv;
 	}
 	fired = fired || stim;
-	S[0 * c + i] = v;
-	S[1 * c + i] = nn;
-	S[2 * c + i] = m;
-	S[3 * c + i] = h;
-	S[4 * c + i] = dir;
+	if(member && s == 0u) {
+		S[0 * c + i] = v;
+		S[1 * c + i] = nn;
+		S[2 * c + i] = m;
+		S[3 * c + i] = h;
+		S[4 * c + i] = dir;
+	}
 	return fired;
 }
 
@@ -690,8 +712,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				while(dw >= A.groupWarp[gi + 1]) ++gi;
 				const GroupDev& G = A.groups[gi];
 				const uint32_t n = dw * 32u + lane;
-				const uint32_t i = n - G.devBase;
-				const bool valid = i < G.count;
+				const uint32_t rel = n - G.devBase;
+				const uint32_t i = rel >> G.shift;
+				/* a neuron at this device index (not one of an HH neuron's
+				 * seven helper lanes) */
+				const bool valid = (rel & ((1u << G.shift) - 1u)) == 0u && i < G.count;
 				/* the firing-stimulus word is cleared after the model has
 				 * issued its loads, so that nothing orders them behind it */
 				uint32_t stimWord = lane == 0 ? net.fstim[dw] : 0u;
@@ -720,7 +745,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const float E = wfxToFloat(e, net.fbits);
 				const float I = wfxToFloat(in, net.fbits);
 				bool fired = false;
-				if(valid) {
+				if(G.kind == 3) {   /* MODEL_HH */
+					/* all lanes: eight per neuron */
+					fired = modelHH(net, G, i, E, I, stimWord, t - G.timerBase, lane) && valid;
+				} else if(valid) {
 					const bool stim = (stimWord >> lane) & 1u;
 					switch(G.kind) {
 						case 0: {
@@ -732,7 +760,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						}
 						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
 						case 2: fired = modelQif(net, G, i, n, E, I, stim); break;
-						case 3: fired = modelHH(net, G, i, n, E, I, stim, t - G.timerBase); break;
 						case 4: fired = modelPoisson(net, G, i, n, E, I, stim); break;
 						default: fired = modelInput(net, G, i, n, E, I, stim); break;
 					}
@@ -1149,6 +1176,28 @@ k_exp_eval(uint32_t first, uint32_t n, float* out, NetDev net)
 	}
 }
 
+/* hhDivConst against __fdiv_rn, divisors 20, 80 and 18, on every float with
+ * magnitude at least 2^-100 (infinities included) and on both zeros */
+__global__ void
+k_hh_div_check(unsigned long long* bad)
+{
+	const float ds[3] = {20.0f, 80.0f, 18.0f};
+	unsigned long long nb[3] = {0, 0, 0};
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for(uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < (uint64_t(1) << 32); u += stride) {
+		const float a = libm::u2f(uint32_t(u));
+		if(!(fabsf(a) >= 0x1p-100f) && a != 0.0f) continue;   /* NaN and tiny magnitudes */
+#pragma unroll
+		for(int q = 0; q < 3; ++q) {
+			const float y = __fdiv_rn(1.0f, ds[q]);
+			if(libm::f2u(hhDivConst(a, ds[q], y)) != libm::f2u(__fdiv_rn(a, ds[q]))) nb[q]++;
+		}
+	}
+	for(int q = 0; q < 3; ++q) {
+		if(nb[q]) atomicAdd(&bad[q], nb[q]);
+	}
+}
+
 int g_smCount = 0;
 
 } // namespace
@@ -1313,6 +1362,12 @@ launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* s
 {
 	if(n == 0) return;
 	k_exp_eval<<<smCount() * 8, 256, 0, S(stream)>>>(first, n, out, net);
+}
+
+void
+launchHhDivCheck(unsigned long long* bad, void* stream)
+{
+	k_hh_div_check<<<smCount() * 8, 256, 0, S(stream)>>>(bad);
 }
 
 void

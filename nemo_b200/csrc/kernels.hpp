@@ -139,6 +139,9 @@ struct GroupDev {
 	float* param;           /* [nParam][count] */
 	float* state;           /* [nState][count] */
 	uint4* rng;             /* [count] xorshift128 state */
+	uint32_t shift;         /* neuron i at device index devBase + (i << shift):
+	                         * HH neurons take 8 lanes each (shift 3), the
+	                         * other models one */
 };
 
 /* The STDP rule in fixed point (src/nemo/StdpProcess.cpp:20-46) */
@@ -228,6 +231,8 @@ void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 /* device expf (glibc-matching) of the floats with bits [first, first + n) */
 void launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* stream);
+/* counts of mismatches [3] (zeroed by the caller) of the HH constant divisions */
+void launchHhDivCheck(unsigned long long* bad, void* stream);
 int smCount();
 
 } // namespace nemo_b200

@@ -423,6 +423,12 @@ nemo_b200_expf_check(nemo_simulation_t s, uint64_t* mismatches)
 }
 
 nemo_status_t
+nemo_b200_hh_division_check(uint64_t mismatches[3])
+{
+	RETURN_CALL(nemo_b200::hhDivisionCheck(mismatches));
+}
+
+nemo_status_t
 nemo_b200_expf_exceptions(size_t* count, double* tau)
 {
 	RETURN_CALL({

@@ -118,6 +118,9 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		g.localBase = local;
 		g.devBase = devPos;
 		g.count = n;
+		/* an HH neuron's six exponentials per substep run on six lanes of
+		 * its own eight (kernels.cu modelHH) */
+		g.shift = ng.type.kind == MODEL_HH ? 3u : 0u;
 		g.param.resize(size_t(ng.type.nParam) * n);
 		g.state.resize(size_t(ng.type.nState) * n);
 		for(unsigned p = 0; p < ng.type.nParam; ++p)
@@ -125,7 +128,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		for(unsigned s = 0; s < ng.type.nState; ++s)
 			std::copy(ng.state[s].begin(), ng.state[s].end(), g.state.begin() + size_t(s) * n);
 		for(uint32_t i = 0; i < n; ++i) {
-			if(!m_g2d.emplace(ng.gidx[i], devPos + i).second) {
+			if(!m_g2d.emplace(ng.gidx[i], devPos + (i << g.shift)).second) {
 				fail(NEMO_INVALID_INPUT, "Duplicate neuron index " + std::to_string(ng.gidx[i]));
 			}
 		}
@@ -133,7 +136,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		groupGidx.push_back(&ng.gidx);
 		groupSeedKey.push_back(ngi < net.seedKey.size() ? &net.seedKey[ngi] : nullptr);
 		local += n;
-		devPos = uint32_t(roundUp(uint64_t(devPos) + n, 32));
+		devPos = uint32_t(roundUp(uint64_t(devPos) + (uint64_t(n) << m_groups.back().shift), 32));
 	}
 	m_nDev = std::max<uint32_t>(devPos, 32);
 	if(uint64_t(m_nDev) >= (uint64_t(1) << 26)) {
@@ -144,8 +147,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
 		const Group& g = m_groups[gi];
 		for(uint32_t i = 0; i < g.count; ++i) {
-			m_d2g[g.devBase + i] = (*groupGidx[gi])[i];
-			m_d2group[g.devBase + i] = int32_t(gi);
+			m_d2g[g.devBase + (i << g.shift)] = (*groupGidx[gi])[i];
+			m_d2group[g.devBase + (i << g.shift)] = int32_t(gi);
 		}
 	}
 	/* dense user -> device table when the user indices are compact */
@@ -488,8 +491,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_args.groupWarp[0] = 0;
 	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
 		const Group& g = m_groups[gi];
-		m_args.groups[gi] = GroupDev{g.devBase, g.count, 0u, int(g.type.kind), g.dParam, g.dState, g.dRng};
-		m_args.groupWarp[gi + 1] = m_args.groupWarp[gi] + (g.count + 31) / 32;
+		m_args.groups[gi] = GroupDev{g.devBase, g.count, 0u, int(g.type.kind), g.dParam, g.dState, g.dRng, g.shift};
+		m_args.groupWarp[gi + 1] = m_args.groupWarp[gi] + uint32_t(((uint64_t(g.count) << g.shift) + 31) / 32);
 	}
 	/* a grid barrier that waits this long has lost a block: give up */
 	m_args.timeoutNs = 10ull * 1000 * 1000 * 1000;
@@ -526,7 +529,7 @@ Simulation::Group&
 Simulation::groupOfDev(uint32_t dev, uint32_t* i)
 {
 	Group& g = m_groups.at(size_t(m_d2group.at(dev)));
-	*i = dev - g.devBase;
+	*i = (dev - g.devBase) >> g.shift;
 	return g;
 }
 
@@ -534,7 +537,7 @@ const Simulation::Group&
 Simulation::groupOfDev(uint32_t dev, uint32_t* i) const
 {
 	const Group& g = m_groups.at(size_t(m_d2group.at(dev)));
-	*i = dev - g.devBase;
+	*i = (dev - g.devBase) >> g.shift;
 	return g;
 }
 
@@ -1401,6 +1404,20 @@ Simulation::libmCheck()
 	uint64_t total = 0;
 	for(uint64_t b : bad) total += b;
 	return total;
+}
+
+void
+hhDivisionCheck(uint64_t mismatches[3])
+{
+	unsigned long long* bad = nullptr;
+	NEMO_CUDA(cudaMalloc(&bad, 3 * sizeof(unsigned long long)));
+	NEMO_CUDA(cudaMemset(bad, 0, 3 * sizeof(unsigned long long)));
+	launchHhDivCheck(bad, nullptr);
+	unsigned long long h[3] = {0, 0, 0};
+	const cudaError_t err = cudaMemcpy(h, bad, sizeof(h), cudaMemcpyDeviceToHost);
+	cudaFree(bad);
+	NEMO_CUDA(err);
+	for(int q = 0; q < 3; ++q) mismatches[q] = h[q];
 }
 
 } // namespace nemo_b200

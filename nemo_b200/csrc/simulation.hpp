@@ -131,6 +131,7 @@ private:
 		uint32_t localBase;   /* contiguous simulation index of the first neuron */
 		uint32_t devBase;     /* device index (multiple of 32) */
 		uint32_t count;
+		uint32_t shift = 0;   /* neuron i at devBase + (i << shift) (GroupDev) */
 		std::vector<float> param;   /* host copy, [nParam][count] */
 		std::vector<float> state;   /* host copy, [nState][count] */
 		float* dParam = nullptr;
@@ -216,6 +217,10 @@ private:
 	uint64_t m_graphKey[4] = {0, 0, 0, 0};
 	bool m_graphUsable = true;
 };
+
+/* The HH model's constant divisions against correctly rounded division on
+ * the current device (kernels.cu k_hh_div_check): mismatches per divisor. */
+void hhDivisionCheck(uint64_t mismatches[3]);
 
 } // namespace nemo_b200
 

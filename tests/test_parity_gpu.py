@@ -122,6 +122,18 @@ def test_expf_exhaustive():
     assert mism.value == 0
 
 
+def test_hh_constant_divisions_exhaustive():
+    """The Hodgkin-Huxley model divides -(v + 65) by 20, 80 and 18 with an
+    FMA-corrected product: equal to correctly rounded division on every float
+    of magnitude at least 2^-100 and on the zeros (v + 65 is zero or at least
+    2^-17 in magnitude)."""
+    lib = Library()
+    mism = (ctypes.c_uint64 * 3)(9, 9, 9)
+    lib.dll.nemo_b200_hh_division_check.argtypes = [ctypes.c_uint64 * 3]
+    lib.call("nemo_b200_hh_division_check", mism)
+    assert list(mism) == [0, 0, 0]
+
+
 def _hh_network(n, m, seed):
     rng = np.random.default_rng(seed)
     f32 = np.float32
@@ -139,8 +151,9 @@ def _hh_network(n, m, seed):
 def test_hodgkin_huxley_network(oracle_lib):
     """A network of Hodgkin-Huxley neurons alone (simulation index base 0,
     where the reference plugin is well defined) driven by current stimulus:
-    identical firing every cycle and identical v, n, m, h, dir bits."""
-    n = 160
+    identical firing every cycle and identical v, n, m, h, dir bits. 157
+    neurons take eight lanes each: the last warp is partly empty."""
+    n = 157
     spec = _hh_network(n, 20, seed=8)
     (_, g), (_, o) = _pair(spec, oracle_lib)
     rng = np.random.default_rng(1)
