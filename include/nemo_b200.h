@@ -92,6 +92,48 @@ nemo_status_t nemo_b200_counters(nemo_simulation_t sim, uint64_t out[4]);
  * (nemo_strerror). */
 nemo_simulation_t nemo_b200_new_batch(nemo_network_t nets[], size_t count, nemo_configuration_t conf);
 
+/* ---- sharded simulation: one network over several GPUs ----
+ *
+ * A network too large for one GPU runs as `world` shards, one per process
+ * and GPU (the reference's MPI workers, src/mpi/Worker.cpp:265-292, over
+ * NVLink). Shard `rank` owns a contiguous range of the simulation's device
+ * warps (32 neuron slots each, types in registration order; equal warp
+ * counts) and holds only the synapses to its own neurons. Every cycle:
+ *
+ *   nemo_b200_shard_step     stimulus for this shard's neurons (entries for
+ *                            other shards' neurons are skipped), the update
+ *                            of its neurons; writes the fired words of its
+ *                            own warps (shard_range: `words` uint32 from
+ *                            `first_word`) to local_words (host memory);
+ *   (the caller all-gathers the words of all shards, e.g. with
+ *    torch.distributed, into the total_words words of the cycle)
+ *   nemo_b200_shard_deliver  brings the other shards' firing of the cycle
+ *                            in; returns every neuron fired in the cycle
+ *                            (user indices), valid until the next call.
+ *
+ * Firing, currents and STDP equal those of the unsharded simulation bit for
+ * bit. nemo_apply_stdp applies to the shard's synapses. A neuron's state is
+ * read on the shard that owns it; synapse queries answer for the synapses
+ * whose target the shard owns. nemo_step and the device-resident runs are
+ * not available on a shard. Returns NULL on error (nemo_strerror). */
+nemo_simulation_t nemo_b200_new_shard(nemo_network_t net, nemo_configuration_t conf, unsigned rank, unsigned world);
+
+/* The warps shard `rank` of `world` owns out of total_words: [first_word,
+ * first_word + words). Host arithmetic, no device needed. */
+nemo_status_t nemo_b200_shard_warps(unsigned total_words, unsigned rank, unsigned world, unsigned* first_word,
+		unsigned* words);
+
+/* The shard's own warps and the simulation's total warps (the length of the
+ * fired-word vector of a cycle). */
+nemo_status_t nemo_b200_shard_range(nemo_simulation_t sim, unsigned* first_word, unsigned* words,
+		unsigned* total_words);
+
+nemo_status_t nemo_b200_shard_step(nemo_simulation_t sim, unsigned fstim_nidx[], size_t fstim_count,
+		unsigned istim_nidx[], float istim_current[], size_t istim_count, uint32_t local_words[]);
+
+nemo_status_t nemo_b200_shard_deliver(nemo_simulation_t sim, const uint32_t all_words[], unsigned* fired[],
+		size_t* fired_count);
+
 /* Number of networks of a batch (1 for an ordinary simulation). */
 nemo_status_t nemo_b200_batch_instances(nemo_simulation_t sim, size_t* count);
 

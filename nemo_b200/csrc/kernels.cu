@@ -10,6 +10,7 @@
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
@@ -630,7 +631,7 @@ __global__ void __launch_bounds__(T, 1)
 k_cycles(const __grid_constant__ CycleArgs A)
 {
 	extern __shared__ int2 sAcc[];
-	__shared__ uint32_t sPreF[MAX_BLOCKS + 1];
+	__shared__ uint32_t sPreF[MAX_BLOCKS + 2];    /* + the remote list of a shard */
 	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
 	__shared__ uint32_t sNFired, sNPost, sWork;
 	__shared__ unsigned long long sEvents, sPushed, sVisits;
@@ -645,7 +646,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t b = blockIdx.x;
 	const size_t nDev = net.nDev;
 	const uint32_t ownN = net.ownWarps * 32u;       /* list and slot stride per block */
-	const uint32_t firstWarp = ownFirst(b, net.ownQ, net.ownR);
+	const uint32_t firstWarp = net.warpBase + ownFirst(b, net.ownQ, net.ownR);
 	const uint32_t myWarps = net.ownQ + (b < net.ownR ? 1u : 0u);
 	const uint32_t myN = myWarps * 32u;
 	const uint32_t ownBase = firstWarp * 32u;
@@ -667,11 +668,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		}
 	}
 
-	for(uint32_t k = 0; k <= A.cycles; ++k) {
+	const uint32_t phases = A.cycles + ((A.carry & 2u) ? 0u : 1u);
+	for(uint32_t k = 0; k < phases; ++k) {
 		const uint64_t t64 = first + k;
 		const uint32_t t = uint32_t(t64);
 		const bool doUpdate = k < A.cycles;
-		const bool doPrev = k > 0;     /* gather and learn for cycle t-1 */
+		const bool doPrev = k > 0 || (A.carry & 1u);     /* gather and learn for cycle t-1 */
 		const uint32_t slotT = uint32_t(t64 % net.slots);
 
 		if(tid == 0) {
@@ -688,7 +690,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		}
 		if(doPrev) {
 			const uint32_t par = (t - 1u) & 1u;
-			if(warp == 0) warpPrefix(net.firedCnt + par * B, B, sPreF, lane);
+			if(warp == 0) {
+				warpPrefix(net.firedCnt + par * B, B, sPreF, lane);
+				/* a shard's remote fired sources: list B */
+				if(lane == 31 && net.remoteList) sPreF[B + 1] = sPreF[B] + net.remoteCnt[par];
+			}
 			if(warp == 1 && net.stdp) warpPrefix(net.postCnt + par * B, B, sPreP, lane);
 		}
 		__syncthreads();
@@ -821,7 +827,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		 * 128-synapse STDP items (item u * B + b) ---- */
 		if(doPrev) {
 			const uint32_t par = (t - 1u) & 1u;
-			const uint32_t F = net.deliver ? sPreF[B] : 0u;
+			const uint32_t nLists = B + (net.remoteList ? 1u : 0u);
+			const uint32_t F = net.deliver ? sPreF[nLists] : 0u;
 			const uint32_t G = (F + 31u) / 32u;
 			const uint32_t P = net.stdp ? sPreP[B] : 0u;
 			const uint32_t chunks = net.stdpChunks;
@@ -849,8 +856,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t j = u * 32u + lane;
 					uint32_t beg = 0, cnt = 0;
 					if(j < F) {
-						const uint32_t bb = findList(sPreF, B, j);
-						const uint32_t s = flist[size_t(bb) * ownN + (j - sPreF[bb])];
+						const uint32_t bb = findList(sPreF, nLists, j);
+						const uint32_t s = bb < B ? flist[size_t(bb) * ownN + (j - sPreF[bb])]
+							: net.remoteList[size_t(par) * nDev + (j - sPreF[B])];
 						const uint32_t* row = net.segOff + size_t(b) * (nDev + 1u) + s;
 						beg = row[0];
 						cnt = row[1] - beg;
@@ -1176,6 +1184,52 @@ k_exp_eval(uint32_t first, uint32_t n, float* out, NetDev net)
 	}
 }
 
+/* A sharded simulation: the firing of cycle t of the neurons other shards
+ * own (allWords holds every device warp's word; this shard's own warps
+ * [ownLo, ownHi) are skipped) enters this shard as its own update would have
+ * entered it: the history shift, the fired-ring word, the delay-1 pushes
+ * into the inbox of cycle t + 1, the list of remote fired sources that the
+ * next launch gathers from (its count zeroed before the launch), and the
+ * synaptic events they generate here. One warp per device warp. */
+__global__ void
+k_shard_inject(NetDev net, uint64_t t64, const uint32_t* allWords, uint32_t ownLo, uint32_t ownHi)
+{
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint32_t firstW = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint32_t strideW = (gridDim.x * blockDim.x) >> 5;
+	const uint32_t t = uint32_t(t64);
+	const uint32_t par = t & 1u;
+	const size_t nDev = net.nDev;
+	const uint64_t* rfIn = net.rf + par * nDev;
+	uint64_t* rfOut = net.rf + (par ^ 1u) * nDev;
+	unsigned long long events = 0;
+	unsigned long long pushed = 0;
+	for(uint32_t w = firstW; w < net.nWords; w += strideW) {
+		if(w >= ownLo && w < ownHi) continue;
+		const uint32_t word = allWords[w];
+		const uint32_t n = w * 32u + lane;
+		const bool fired = (word >> lane) & 1u;
+		rfOut[n] = (rfIn[n] << 1) | uint64_t(fired);
+		if(lane == 0) net.firedRing[size_t(t & net.ringMask) * net.nWords + w] = word;
+		if(word) {
+			uint32_t base = 0;
+			if(lane == 0) base = atomicAdd(&net.remoteCnt[par], uint32_t(__popc(word)));
+			base = __shfl_sync(FULL, base, 0);
+			if(fired) net.remoteList[size_t(par) * nDev + base + __popc(word & ((1u << lane) - 1u))] = n;
+			events += __reduce_add_sync(FULL, fired ? __ldg(&net.outDegree[n]) : 0u);
+			if(net.deliver) {
+				const uint2 d1 = fired ? make_uint2(__ldg(&net.d1Start[n]), __ldg(&net.d1Start[n + 1]))
+					: make_uint2(0u, 0u);
+				pushed += pushDelayOne(net, word, d1, (t + 1u) & 1u, lane);
+			}
+		}
+	}
+	if(lane == 0) {
+		if(events) atomicAdd(&net.stats[3], events);
+		if(pushed) atomicAdd(&net.stats[0], pushed);
+	}
+}
+
 /* hhDivConst against __fdiv_rn, divisors 20, 80 and 18, on every float with
  * magnitude at least 2^-100 (infinities included) and on both zeros */
 __global__ void
@@ -1362,6 +1416,15 @@ launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* s
 {
 	if(n == 0) return;
 	k_exp_eval<<<smCount() * 8, 256, 0, S(stream)>>>(first, n, out, net);
+}
+
+void
+launchShardInject(const NetDev& net, uint64_t t, const uint32_t* allWords, uint32_t ownLo, uint32_t ownHi,
+		void* stream)
+{
+	const uint32_t warps = net.nWords;
+	const uint32_t blocks = std::max<uint32_t>(1u, std::min<uint32_t>((warps + 7u) / 8u, uint32_t(smCount()) * 8u));
+	k_shard_inject<<<blocks, 256, 0, S(stream)>>>(net, t, allWords, ownLo, ownHi);
 }
 
 void

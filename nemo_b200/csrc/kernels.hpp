@@ -70,6 +70,9 @@ struct NetDev {
 	uint32_t ownWarps;
 	uint32_t ownQ;
 	uint32_t ownR;
+	/* first warp of the owned range: 0, or in a sharded simulation the
+	 * shard's first warp (block b owns warps warpBase + ownFirst(b)...) */
+	uint32_t warpBase;
 	int smemAcc;            /* current slots of the owned neurons in shared memory */
 
 	/* forward connectivity. Delays >= 2, partitioned by target owner:
@@ -123,6 +126,12 @@ struct NetDev {
 	uint32_t expProbe;
 	uint32_t expNear;
 
+	/* sharded simulation: the fired sources other shards own, by cycle
+	 * parity ([2][nDev], counts [2]), gathered like a block's fired list;
+	 * null when the simulation owns every neuron */
+	uint32_t* remoteList;
+	uint32_t* remoteCnt;
+
 	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
 	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */
 	unsigned long long* stats;
@@ -164,6 +173,12 @@ struct CycleArgs {
 	int ngroups;
 	uint64_t firstCycle;
 	uint32_t cycles;
+	/* bit 0: the first phase also gathers and learns for cycle
+	 * firstCycle - 1 (left pending by the previous launch); bit 1: no
+	 * trailing gather phase (the launch leaves its last cycle pending).
+	 * 0 for the unsharded simulation; a sharded step is one update phase,
+	 * its flush one gather phase (cycles 0, carry 1). */
+	uint32_t carry;
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
 	/* when set, the first cycle is read from here instead of firstCycle and
 	 * advanced by the launch (launches replayed from a CUDA graph) */
@@ -231,6 +246,9 @@ void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 /* device expf (glibc-matching) of the floats with bits [first, first + n) */
 void launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* stream);
+/* sharded simulation: the remote firing of cycle t (k_shard_inject) */
+void launchShardInject(const NetDev& net, uint64_t t, const uint32_t* allWords, uint32_t ownLo, uint32_t ownHi,
+		void* stream);
 /* counts of mismatches [3] (zeroed by the caller) of the HH constant divisions */
 void launchHhDivCheck(unsigned long long* bad, void* stream);
 int smCount();

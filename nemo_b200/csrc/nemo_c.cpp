@@ -21,7 +21,8 @@ using namespace nemo_b200;
 struct nemo_network_class { Network net; };
 struct nemo_configuration_class { Configuration conf; };
 struct nemo_simulation_class {
-	nemo_simulation_class(const Network& n, const Configuration& c) : sim(n, c) {}
+	nemo_simulation_class(const Network& n, const Configuration& c, const ShardSpec* shard = nullptr) :
+		sim(n, c, shard) {}
 	Simulation sim;
 	std::vector<unsigned> fired;
 };
@@ -247,6 +248,63 @@ nemo_b200_new_batch(nemo_network_t nets[], size_t count, nemo_configuration_t c)
 		setResult("Unknown error", NEMO_UNKNOWN_ERROR);
 	}
 	return NULL;
+}
+
+nemo_simulation_t
+nemo_b200_new_shard(nemo_network_t n, nemo_configuration_t c, unsigned rank, unsigned world)
+{
+	try {
+		ShardSpec spec;
+		Network local = shardNetwork(n->net, rank, world, &spec);
+		return new nemo_simulation_class(local, c->conf, &spec);
+	} catch(Exception& e) {
+		setResult(e.what(), e.code());
+	} catch(std::exception& e) {
+		setResult(e.what(), NEMO_UNKNOWN_ERROR);
+	} catch(...) {
+		setResult("Unknown error", NEMO_UNKNOWN_ERROR);
+	}
+	return NULL;
+}
+
+nemo_status_t
+nemo_b200_shard_warps(unsigned total_words, unsigned rank, unsigned world, unsigned* first_word, unsigned* words)
+{
+	RETURN_CALL({
+		uint32_t lo = 0, hi = 0;
+		shardWarps(total_words, rank, world, &lo, &hi);
+		*first_word = lo;
+		*words = hi - lo;
+	});
+}
+
+nemo_status_t
+nemo_b200_shard_range(nemo_simulation_t s, unsigned* first_word, unsigned* words, unsigned* total_words)
+{
+	RETURN_CALL({
+		const ShardSpec& sp = s->sim.shard();
+		*first_word = sp.warpLo;
+		*words = sp.warpHi - sp.warpLo;
+		*total_words = sp.totalWarps;
+	});
+}
+
+nemo_status_t
+nemo_b200_shard_step(nemo_simulation_t s, unsigned fstim_nidx[], size_t fstim_count,
+		unsigned istim_nidx[], float istim_current[], size_t istim_count, uint32_t local_words[])
+{
+	RETURN_CALL(s->sim.shardStep(fstim_nidx, fstim_count, istim_nidx, istim_current, istim_count, local_words));
+}
+
+nemo_status_t
+nemo_b200_shard_deliver(nemo_simulation_t s, const uint32_t all_words[], unsigned* fired[], size_t* fired_count)
+{
+	RETURN_CALL({
+		const std::vector<unsigned>& f = s->sim.shardDeliver(all_words);
+		s->fired = f;
+		*fired = s->fired.empty() ? NULL : s->fired.data();
+		*fired_count = s->fired.size();
+	});
 }
 
 nemo_status_t

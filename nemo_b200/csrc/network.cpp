@@ -473,6 +473,29 @@ Network::merge(const std::vector<const Network*>& nets, std::vector<uint32_t>* b
 	return m;
 }
 
+Network
+Network::subsetByTarget(const std::function<bool(uint32_t)>& keepTarget) const
+{
+	Network m;
+	m.groups = groups;
+	m.typeIds = typeIds;
+	m.mapper = mapper;
+	m.izType = izType;
+	m.seedKey = seedKey;
+	for(size_t k = 0; k < src.size(); ++k) {
+		if(!keepTarget(tgt[k])) continue;
+		m.src.push_back(src[k]);
+		m.tgt.push_back(tgt[k]);
+		m.dly.push_back(dly[k]);
+		m.wgt.push_back(wgt[k]);
+		m.plastic.push_back(plastic[k]);
+		m.sid.push_back(sid[k]);
+		m.m_srcCount[src[k]]++;
+	}
+	m.m_maxDelay = m_maxDelay;
+	return m;
+}
+
 unsigned
 Network::neuronCount() const
 {

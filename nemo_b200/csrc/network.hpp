@@ -12,6 +12,7 @@
  * preserved. */
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -102,6 +103,12 @@ public:
 	 * simulation index within the instance for neuron i of group g, so that
 	 * each instance's neurons get the random seeds they would get alone. */
 	static Network merge(const std::vector<const Network*>& nets, std::vector<uint32_t>* base);
+
+	/* Every neuron and the synapses whose target `keepTarget` accepts, in
+	 * their order, with their ids; the maximum delay stays this network's
+	 * (it decides delivery for every synapse). The network one shard of a
+	 * sharded simulation builds. */
+	Network subsetByTarget(const std::function<bool(uint32_t)>& keepTarget) const;
 	std::vector<std::vector<uint64_t>> seedKey;
 
 	std::vector<NeuronGroup> groups;

@@ -64,10 +64,10 @@ Simulation::alloc(size_t bytes)
 	return p;
 }
 
-Simulation::Simulation(const Network& net, const Configuration& conf) :
+Simulation::Simulation(const Network& net, const Configuration& conf, const ShardSpec* shard) :
 	m_nNeurons(net.neuronCount()),
 	m_nDev(0),
-	m_maxDelay(net.maxDelay()),
+	m_maxDelay(shard ? shard->maxDelay : net.maxDelay()),
 	m_fbits(conf.fractionalBits),
 	m_nsyn(net.synapseCount()),
 	m_nrcm(0),
@@ -95,7 +95,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		fail(NEMO_INVALID_INPUT, "Cannot create simulation from empty network");
 	}
 	if(m_stdpOn) {
-		m_stdpFn.verifyDynamicWindowLength(net.maxDelay());
+		m_stdpFn.verifyDynamicWindowLength(m_maxDelay);
 	}
 	if(m_maxDelay > 64) {
 		fail(NEMO_INVALID_INPUT, "The network has synapses with delay " + std::to_string(m_maxDelay)
@@ -139,6 +139,21 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		devPos = uint32_t(roundUp(uint64_t(devPos) + (uint64_t(n) << m_groups.back().shift), 32));
 	}
 	m_nDev = std::max<uint32_t>(devPos, 32);
+	if(shard) {
+		/* the shard's synapses were chosen with this same layout */
+		if(shard->totalWarps != m_nDev / 32 || shard->warpLo > shard->warpHi || shard->warpHi > m_nDev / 32
+				|| shard->world == 0 || shard->rank >= shard->world) {
+			fail(NEMO_LOGIC_ERROR, "Shard: the warp range does not match the network's device layout");
+		}
+		m_shardMode = true;
+		m_shard = *shard;
+	} else {
+		m_shard.warpLo = 0;
+		m_shard.warpHi = m_nDev / 32;
+		m_shard.totalWarps = m_nDev / 32;
+		m_shard.maxDelay = m_maxDelay;
+	}
+	const uint32_t warpLo = m_shard.warpLo;
 	if(uint64_t(m_nDev) >= (uint64_t(1) << 26)) {
 		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^26 neurons per simulation");
 	}
@@ -257,7 +272,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 
 	uint32_t ownQ = 0, ownR = 0;
 	bool smemAcc = false;
-	cyclesPlan(m_nDev / 32, slots, acc32, &m_blocks, &ownQ, &ownR, &smemAcc);
+	cyclesPlan(m_shard.warpHi - warpLo, slots, acc32, &m_blocks, &ownQ, &ownR, &smemAcc);
 	const uint32_t ownWarps = ownQ + (ownR ? 1u : 0u);
 	NEMO_CUDA(cudaGetLastError());
 	if(m_blocks == 0) {
@@ -281,7 +296,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
 			if(net.dly[s] == 1) d1Start[dsrc[s] + 1]++;
-			else cursor[size_t(ownerOf(dtgt[s] / 32, ownQ, ownR)) * m_nDev + dsrc[s]]++;
+			else cursor[size_t(ownerOf(dtgt[s] / 32 - warpLo, ownQ, ownR)) * m_nDev + dsrc[s]]++;
 		}
 		for(uint32_t b = 0; b < B; ++b) {
 			uint32_t* c = &cursor[size_t(b) * m_nDev];
@@ -303,7 +318,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 			if(net.dly[s] == 1) {
 				pos = d1Base + d1Fill[dsrc[s]]++;
 			} else {
-				const uint32_t b = ownerOf(dtgt[s] / 32, ownQ, ownR);
+				const uint32_t b = ownerOf(dtgt[s] / 32 - warpLo, ownQ, ownR);
 				pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
 			}
 			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(wfx[s]));
@@ -314,11 +329,11 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 
 	/* applyStdp launches: consecutive owner blocks grouped until their
 	 * regions hold APPLY_GROUP_SYNAPSES synapses, as target ranges */
-	m_applyGroups.assign(1, 0u);
+	m_applyGroups.assign(1, warpLo * 32u);
 	for(uint32_t b = 0; b < B;) {
 		uint32_t e = b + 1;
 		while(e < B && regionBase[e + 1] - regionBase[b] <= APPLY_GROUP_SYNAPSES) ++e;
-		m_applyGroups.push_back(std::min(ownFirst(e, ownQ, ownR) * 32u, m_nDev));
+		m_applyGroups.push_back(std::min((warpLo + ownFirst(e, ownQ, ownR)) * 32u, m_nDev));
 		b = e;
 	}
 
@@ -362,6 +377,12 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 			size_t s = net.m_bySource[k];
 			m_aux[k] = Aux{fcmPos[s], net.tgt[s], uint8_t(net.dly[s]), net.plastic[s]};
 		}
+		/* a shard holds some of a source's synapses: their ids keep the
+		 * per-source index of the whole network */
+		if(m_shardMode) {
+			m_auxSid.resize(S);
+			for(size_t k = 0; k < S; ++k) m_auxSid[k] = net.sid[net.m_bySource[k]];
+		}
 	}
 
 	/* ---- device ---- */
@@ -387,6 +408,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.ownWarps = ownWarps;
 	m_net.ownQ = ownQ;
 	m_net.ownR = ownR;
+	m_net.warpBase = warpLo;
 	m_net.smemAcc = smemAcc ? 1 : 0;
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
 	m_net.regionBase = (const uint64_t*) put(regionBase.data(), regionBase.size() * 8);
@@ -409,6 +431,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf) :
 	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	m_net.postList = (uint2*) alloc(size_t(2) * B * ownN * 8);
 	m_net.postCnt = (uint32_t*) alloc(size_t(2) * B * 4);
+	if(m_shard.world > 1) {
+		m_net.remoteList = (uint32_t*) alloc(size_t(2) * m_nDev * 4);
+		m_net.remoteCnt = (uint32_t*) alloc(2 * 4);
+	}
 	m_net.stdp = m_stdpOn ? 1 : 0;
 	m_net.stdpChunks = uint32_t(stdpChunks);
 	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
@@ -543,11 +569,12 @@ Simulation::groupOfDev(uint32_t dev, uint32_t* i) const
 
 /* One persistent launch for cycles [first, first + cycles) */
 void
-Simulation::launchBlock(uint64_t first, unsigned cycles)
+Simulation::launchBlock(uint64_t first, unsigned cycles, uint32_t carry)
 {
 	CycleArgs a = m_args;
 	a.firstCycle = first;
 	a.cycles = cycles;
+	a.carry = carry;
 	for(int gi = 0; gi < a.ngroups; ++gi) {
 		a.groups[gi].timerBase = uint32_t(m_timerBase);
 	}
@@ -582,8 +609,9 @@ Simulation::decodeFired(const uint32_t* words, std::vector<unsigned>& out) const
 /* src/nemo/nemo_c.cpp:439-461 and cpu/Simulation.cpp:140-163: firing
  * stimulus, then current stimulus; an invalid index raises after the entries
  * before it have been applied. */
-const std::vector<unsigned>&
-Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
+void
+Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+		bool ownedOnly)
 {
 	cudaStream_t stream = STREAM(m_stream);
 	size_t need = nf + ni;
@@ -604,6 +632,7 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	for(size_t k = 0; k < nf; ++k) {
 		auto it = m_g2d.find(fstim[k]);
 		if(it == m_g2d.end()) { err = 1; badIdx = fstim[k]; break; }
+		if(ownedOnly && !owns(it->second)) continue;
 		m_hStim[nfOk++] = it->second;
 	}
 	if(!err && ni) {
@@ -613,6 +642,7 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 		for(size_t k = 0; k < ni; ++k) {
 			auto it = m_g2d.find(inidx[k]);
 			if(it == m_g2d.end()) { err = 1; badIdx = inidx[k]; break; }
+			if(ownedOnly && !owns(it->second)) continue;
 			auto s = seen.find(it->second);
 			if(s != seen.end()) {
 				m_hCur[s->second] = icur[k];
@@ -634,7 +664,14 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 		NEMO_CUDA(cudaStreamSynchronize(stream));
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
 	}
+}
 
+const std::vector<unsigned>&
+Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
+{
+	notShard("step");
+	stageStimulus(fstim, nf, inidx, icur, ni, false);
+	cudaStream_t stream = STREAM(m_stream);
 	launchBlock(m_cycle, 1);
 	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
@@ -649,6 +686,83 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	return m_fired;
 }
 
+void
+Simulation::notShard(const char* what) const
+{
+	if(m_shardMode) {
+		fail(NEMO_LOGIC_ERROR, std::string(what) + ": this simulation is one shard of a sharded simulation; "
+				"its cycles run through the shard step and deliver calls");
+	}
+}
+
+/* A shard's update launch: one phase that updates the owned neurons for this
+ * cycle and gathers and learns for the previous one when that is pending
+ * (carry bit 0), with no trailing gather (carry bit 1): the cycle's firing of
+ * the other shards is not known yet. */
+void
+Simulation::shardStep(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+		uint32_t* localWords)
+{
+	if(!m_shardMode) {
+		fail(NEMO_LOGIC_ERROR, "shard step: the simulation is not a shard");
+	}
+	if(m_awaitDeliver) {
+		fail(NEMO_LOGIC_ERROR, "shard step: the previous cycle's firing has not been delivered");
+	}
+	stageStimulus(fstim, nf, inidx, icur, ni, true);
+	cudaStream_t stream = STREAM(m_stream);
+	launchBlock(m_cycle, 1, (m_pendingGather ? 1u : 0u) | 2u);
+	const uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
+	const uint32_t words = m_shard.warpHi - m_shard.warpLo;
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords + m_shard.warpLo,
+				size_t(words) * 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	NEMO_CUDA(cudaGetLastError());
+	checkDeviceError();
+	std::memcpy(localWords, m_hWords, size_t(words) * 4);
+	m_cycle++;
+	m_stateDirty = true;
+	m_pendingGather = true;
+	m_awaitDeliver = true;
+}
+
+const std::vector<unsigned>&
+Simulation::shardDeliver(const uint32_t* allWords)
+{
+	if(!m_awaitDeliver) {
+		fail(NEMO_LOGIC_ERROR, "shard deliver: no shard step is waiting for its cycle's firing");
+	}
+	cudaStream_t stream = STREAM(m_stream);
+	const uint64_t t = m_cycle - 1;
+	if(!m_dAllWords) m_dAllWords = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
+	std::memcpy(m_hWords, allWords, size_t(m_net.nWords) * 4);
+	NEMO_CUDA(cudaMemcpyAsync(m_dAllWords, m_hWords, size_t(m_net.nWords) * 4, cudaMemcpyHostToDevice, stream));
+	if(m_net.remoteCnt) {
+		NEMO_CUDA(cudaMemsetAsync(m_net.remoteCnt + (t & 1u), 0, 4, stream));
+		launchShardInject(m_net, t, m_dAllWords, m_shard.warpLo, m_shard.warpHi, m_stream);
+		NEMO_CUDA(cudaGetLastError());
+	}
+	NEMO_CUDA(cudaStreamSynchronize(stream));
+	m_awaitDeliver = false;
+	decodeFired(allWords, m_fired);
+	return m_fired;
+}
+
+/* The pending gathering and learning of a shard's last cycle: one gather
+ * phase (carry bit 0, no cycles). */
+void
+Simulation::flushShard()
+{
+	if(m_awaitDeliver) {
+		fail(NEMO_LOGIC_ERROR, "the last shard step's firing has not been delivered");
+	}
+	if(m_pendingGather) {
+		launchBlock(m_cycle, 0, 1u);
+		m_pendingGather = false;
+	}
+}
+
 /* step() without allocation. Indices are mapped on the host into a small
  * stack buffer and copied chunk by chunk into the module-static scratch
  * (a pageable-source cudaMemcpyAsync returns once the source has been
@@ -659,6 +773,7 @@ size_t
 Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 		unsigned* firedOut, size_t firedCapacity)
 {
+	notShard("stepNoAlloc");
 	if(nf > NOALLOC_STIM_MAX || ni > NOALLOC_STIM_MAX) {
 		fail(NEMO_INVALID_INPUT, "nemo_b200_step_noalloc: at most " + std::to_string(NOALLOC_STIM_MAX)
 				+ " firing-stimulus and " + std::to_string(NOALLOC_STIM_MAX)
@@ -745,6 +860,7 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 void
 Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 {
+	notShard("run");
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
@@ -809,6 +925,7 @@ Simulation::destroyGraph()
 void
 Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
 {
+	notShard("runGraph");
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
@@ -869,6 +986,7 @@ Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
 unsigned
 Simulation::autotune(unsigned trialCycles, double ms[3])
 {
+	notShard("autotune");
 	if(trialCycles == 0 || trialCycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "autotune: trial cycles must be in 1.." + std::to_string(m_ring));
 	}
@@ -946,6 +1064,9 @@ Simulation::applyStdp(float reward)
 		std::ostringstream msg;
 		msg << "STDP reward rounded down to zero. The smallest valid reward is " << fixToFloat(1, m_fbits);
 		fail(NEMO_INVALID_INPUT, msg.str());
+	}
+	if(m_shardMode) {
+		flushShard();
 	}
 	if(m_nrcm) {
 		launchApplyStdp(m_net, m_rule, fx, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
@@ -1071,7 +1192,8 @@ Simulation::getSynapsesFrom(unsigned source)
 	}
 	m_queried.resize(n);
 	for(uint32_t i = 0; i < n; ++i) {
-		m_queried[i] = (uint64_t(source) << 32) | i;
+		const uint32_t sid = m_auxSid.empty() ? i : m_auxSid[it->second.first + i];
+		m_queried[i] = (uint64_t(source) << 32) | sid;
 	}
 	return m_queried;
 }
@@ -1089,6 +1211,16 @@ Simulation::aux(synapse_id id) const
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron id (" + std::to_string(neuron) + ") in synapse query");
 	}
 	uint32_t idx = uint32_t(id & 0xffffffffu);
+	if(!m_auxSid.empty()) {
+		/* a shard: the entry with this per-source index, if the shard holds it */
+		const auto b = m_auxSid.begin() + ptrdiff_t(it->second.first);
+		const auto e = b + ptrdiff_t(it->second.second);
+		const auto p = std::lower_bound(b, e, idx);
+		if(p == e || *p != idx) {
+			throw std::out_of_range("synapse index out of range (the synapse's target is another shard's)");
+		}
+		return m_aux[size_t(p - m_auxSid.begin())];
+	}
 	if(idx >= it->second.second) {
 		throw std::out_of_range("synapse index out of range");
 	}
@@ -1164,6 +1296,7 @@ Simulation::readStats(uint64_t out[4])
 void
 Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4])
 {
+	notShard("timedSteps");
 	if(cyclesPerStep == 0 || cyclesPerStep > m_ring) {
 		fail(NEMO_INVALID_INPUT, "timed steps: cycles per step must be in 1.." + std::to_string(m_ring));
 	}
@@ -1206,6 +1339,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 void
 Simulation::profile(unsigned cycles, float reward, double out[10])
 {
+	notShard("profile");
 	cudaStream_t stream = STREAM(m_stream);
 	cudaEvent_t e0, e1, e2;
 	NEMO_CUDA(cudaEventCreate(&e0));
@@ -1248,6 +1382,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 void
 Simulation::trace(unsigned cycles, double out[14])
 {
+	notShard("trace");
 	if(cycles == 0) {
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");
 	}
@@ -1418,6 +1553,44 @@ hhDivisionCheck(uint64_t mismatches[3])
 	cudaFree(bad);
 	NEMO_CUDA(err);
 	for(int q = 0; q < 3; ++q) mismatches[q] = h[q];
+}
+
+void
+shardWarps(uint32_t totalWarps, unsigned rank, unsigned world, uint32_t* lo, uint32_t* hi)
+{
+	if(world == 0 || rank >= world) {
+		fail(NEMO_INVALID_INPUT, "Shard: rank " + std::to_string(rank) + " of " + std::to_string(world));
+	}
+	const uint32_t q = totalWarps / world, r = totalWarps % world;
+	*lo = rank * q + std::min<uint32_t>(rank, r);
+	*hi = *lo + q + (rank < r ? 1u : 0u);
+}
+
+Network
+shardNetwork(const Network& net, unsigned rank, unsigned world, ShardSpec* spec)
+{
+	/* the device layout of Simulation's constructor */
+	std::unordered_map<uint32_t, uint32_t> g2d;
+	uint64_t devPos = 0;
+	for(const NeuronGroup& ng : net.groups) {
+		const uint32_t n = uint32_t(ng.gidx.size());
+		if(n == 0) continue;
+		const uint32_t shift = ng.type.kind == MODEL_HH ? 3u : 0u;
+		for(uint32_t i = 0; i < n; ++i) g2d.emplace(ng.gidx[i], uint32_t(devPos + (uint64_t(i) << shift)));
+		devPos = roundUp(devPos + (uint64_t(n) << shift), 32);
+	}
+	const uint32_t total = uint32_t(std::max<uint64_t>(devPos, 32) / 32);
+	ShardSpec sp;
+	sp.rank = rank;
+	sp.world = world;
+	sp.totalWarps = total;
+	sp.maxDelay = net.maxDelay();
+	shardWarps(total, rank, world, &sp.warpLo, &sp.warpHi);
+	*spec = sp;
+	return net.subsetByTarget([&](uint32_t tgt) {
+		auto it = g2d.find(tgt);
+		return it != g2d.end() && it->second / 32 >= sp.warpLo && it->second / 32 < sp.warpHi;
+	});
 }
 
 } // namespace nemo_b200

@@ -16,9 +16,31 @@
 
 namespace nemo_b200 {
 
+/* One shard of a sharded simulation: shard `rank` of `world` owns the
+ * device warps [warpLo, warpHi) (contiguous, equal counts of warps) and
+ * holds the synapses whose target it owns; maxDelay is the whole network's. */
+struct ShardSpec {
+	unsigned rank = 0;
+	unsigned world = 1;
+	uint32_t warpLo = 0;
+	uint32_t warpHi = 0;
+	uint32_t totalWarps = 0;
+	unsigned maxDelay = 0;
+};
+
+/* Shard `rank` of `world` of a whole network: its owned warp range and the
+ * network it builds (every neuron, the synapses to its own neurons). The
+ * device layout is the simulation's: types in registration order, each
+ * padded to whole warps, Hodgkin-Huxley neurons eight lanes apart. */
+Network shardNetwork(const Network& net, unsigned rank, unsigned world, ShardSpec* spec);
+
+/* The warps shard `rank` of `world` owns out of `totalWarps`: sizes differ by
+ * at most one, lower ranks take the extra ones. */
+void shardWarps(uint32_t totalWarps, unsigned rank, unsigned world, uint32_t* lo, uint32_t* hi);
+
 class Simulation {
 public:
-	Simulation(const Network& net, const Configuration& conf);
+	Simulation(const Network& net, const Configuration& conf, const ShardSpec* shard = nullptr);
 	~Simulation();
 
 	/* One cycle with stimulus; returns the fired neurons (user indices) in
@@ -44,6 +66,19 @@ public:
 	const std::vector<unsigned>& firedAt(uint64_t cycle);
 
 	void applyStdp(float reward);
+
+	/* A shard's cycle, in two calls. shardStep: stimulus for the neurons this
+	 * shard owns (entries for other shards' neurons are skipped), the update
+	 * of its neurons, and the gathering and learning of the previous cycle;
+	 * the fired words of its own warps are written to localWords (host).
+	 * shardDeliver: every warp's fired words of that cycle (host, from all
+	 * shards) bring the other shards' firing in; returns all fired neurons
+	 * (user indices). The cycle's own gathering waits for the next step,
+	 * or for applyStdp. */
+	void shardStep(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+			uint32_t* localWords);
+	const std::vector<unsigned>& shardDeliver(const uint32_t* allWords);
+	const ShardSpec& shard() const { return m_shard; }
 
 	float getNeuronState(unsigned gidx, unsigned var);
 	float getNeuronParameter(unsigned gidx, unsigned param) const;
@@ -150,7 +185,12 @@ private:
 	Group& groupOfDev(uint32_t dev, uint32_t* i);
 	const Group& groupOfDev(uint32_t dev, uint32_t* i) const;
 	const Aux& aux(synapse_id id) const;
-	void launchBlock(uint64_t first, unsigned cycles);
+	void launchBlock(uint64_t first, unsigned cycles, uint32_t carry = 0);
+	void stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+			bool ownedOnly);
+	void notShard(const char* what) const;
+	bool owns(uint32_t dev) const { return dev / 32 >= m_shard.warpLo && dev / 32 < m_shard.warpHi; }
+	void flushShard();
 	void checkDeviceError();
 	void syncStateToHost();
 	void* alloc(size_t bytes);
@@ -180,6 +220,7 @@ private:
 	bool m_writeOnly;
 	std::unordered_map<uint32_t, std::pair<size_t, uint32_t>> m_auxRange;
 	std::vector<Aux> m_aux;
+	std::vector<uint32_t> m_auxSid;   /* a shard's: each entry's per-source index (ascending per source) */
 	std::vector<synapse_id> m_queried;
 	std::vector<uint2> m_fcmHost;
 	bool m_fcmHostValid;
@@ -209,6 +250,13 @@ private:
 	std::vector<uint32_t> m_batchBase;
 	std::vector<unsigned> m_batchFired;
 	std::vector<size_t> m_batchOffsets;
+
+	/* sharded simulation */
+	bool m_shardMode = false;
+	ShardSpec m_shard;
+	bool m_pendingGather = false;   /* the last cycle's gathering and learning wait */
+	bool m_awaitDeliver = false;    /* the last cycle's remote firing has not come in */
+	uint32_t* m_dAllWords = nullptr;
 
 	/* graph run */
 	void destroyGraph();

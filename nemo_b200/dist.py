@@ -1,8 +1,11 @@
 """Several GPUs, one process each (torch.distributed; NCCL on GPUs, gloo for
 the CPU tests).
 
-* The plain step path runs one simulation per GPU (replicas; bench.py
-  --gpus N): no data-path collective.
+* The plain step path either runs one simulation per GPU (replicas; bench.py
+  --gpus N, no data-path collective) or one network over all GPUs as shards
+  (``ShardedSimulation``; bench.py --sharded): each shard owns a contiguous
+  range of neuron warps and the synapses to them, and the shards' fired
+  words are all-gathered once per cycle (``exchange_fired_words``).
 * The batched form splits its independent networks over the ranks
   (``shard_instances``): each rank advances its own batch, no collective.
 * The differentiable form is data-parallel over trials: each rank runs its
@@ -45,3 +48,43 @@ def dp_grad(local_grad, local_trials, total_trials, group=None):
     if dist.is_available() and dist.is_initialized():
         dist.all_reduce(local_grad, op=dist.ReduceOp.SUM, group=group)
     return local_grad
+
+
+def shard_warps(total, rank, world):
+    """The warps [first, first + count) shard `rank` of `world` owns out of
+    `total` (the library's nemo_b200_shard_warps): sizes differ by at most
+    one, lower ranks take the extra ones."""
+    q, r = divmod(int(total), int(world))
+    first = rank * q + min(rank, r)
+    return first, q + (1 if rank < r else 0)
+
+
+def exchange_fired_words(local_words, first_word, total_words, group=None):
+    """One cycle's fired words of all shards: every rank contributes the
+    words of its own warps (shard_warps of the group's size); one all-gather
+    of equal-length tensors (padded to the largest share). On NCCL the
+    tensors travel through the current CUDA device. Returns total_words
+    uint32 words."""
+    import torch
+    import torch.distributed as dist
+    local = np.ascontiguousarray(local_words, dtype=np.uint32)
+    if not (dist.is_available() and dist.is_initialized()):
+        if first_word != 0 or local.size != total_words:
+            raise ValueError("without a process group the shard must own every warp")
+        return local
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    if (first_word, local.size) != shard_warps(total_words, rank, world):
+        raise ValueError("rank %d does not own warps [%d, %d)" % (rank, first_word, first_word + local.size))
+    width = -(-int(total_words) // world)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+    send = torch.zeros(width, dtype=torch.int32, device=dev)
+    send[:local.size] = torch.from_numpy(local.view(np.int32)).to(dev)
+    parts = [torch.empty(width, dtype=torch.int32, device=dev) for _ in range(world)]
+    dist.all_gather(parts, send, group=group)
+    full = np.empty(int(total_words), dtype=np.uint32)
+    for r, part in enumerate(parts):
+        f, c = shard_warps(total_words, r, world)
+        full[f:f + c] = part[:c].cpu().numpy().view(np.uint32)
+    return full

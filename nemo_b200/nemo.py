@@ -388,3 +388,83 @@ class Simulation:
 
     def reset_timer(self):
         self.lib.call("nemo_reset_timer", self.handle)
+def _bind_shard(lib):
+    d = lib.dll
+    if getattr(d, "_shard_bound", False):
+        return d
+    d.nemo_b200_new_shard.restype = ctypes.c_void_p
+    d.nemo_b200_new_shard.argtypes = [ctypes.c_void_p, ctypes.c_void_p, c_uint, c_uint]
+    d.nemo_b200_shard_warps.argtypes = [c_uint, c_uint, c_uint, POINTER(c_uint), POINTER(c_uint)]
+    d.nemo_b200_shard_range.argtypes = [ctypes.c_void_p, POINTER(c_uint), POINTER(c_uint), POINTER(c_uint)]
+    d.nemo_b200_shard_step.argtypes = [ctypes.c_void_p, POINTER(c_uint), c_size_t, POINTER(c_uint), POINTER(c_float),
+                                       c_size_t, POINTER(ctypes.c_uint32)]
+    d.nemo_b200_shard_deliver.argtypes = [ctypes.c_void_p, POINTER(ctypes.c_uint32), POINTER(POINTER(c_uint)),
+                                          POINTER(c_size_t)]
+    d._shard_bound = True
+    return d
+
+
+class ShardedSimulation(Simulation):
+    """Shard `rank` of `world` of one network simulated over several GPUs,
+    one process each (nemo_b200_new_shard): the shard updates the neurons of
+    its own warp range and holds the synapses to them. Every cycle the
+    shards' fired words are all-gathered -- ``exchange(local_words)`` returns
+    the cycle's words of all warps; by default
+    ``nemo_b200.dist.exchange_fired_words`` over torch.distributed -- and
+    delivered. Firing and weights equal the unsharded simulation's."""
+
+    def __init__(self, net, conf, rank, world, exchange=None):
+        self.lib = net.lib
+        d = _bind_shard(self.lib)
+        self.handle = d.nemo_b200_new_shard(net.handle, conf.handle, int(rank), int(world))
+        if not self.handle:
+            raise NemoError(-1, d.nemo_strerror().decode(errors="replace"))
+        first, words, total = c_uint(), c_uint(), c_uint()
+        self.lib.call("nemo_b200_shard_range", self.handle, byref(first), byref(words), byref(total))
+        self.rank, self.world = int(rank), int(world)
+        self.first_word, self.words, self.total_words = first.value, words.value, total.value
+        self._exchange = exchange
+        self._fired = POINTER(c_uint)()
+        self._nfired = c_size_t()
+
+    def step_local(self, fstim=(), istim=()):
+        """Stimulus (entries for other shards' neurons are skipped) and the
+        update of this shard's neurons; returns its fired words."""
+        f = _u32(fstim) if len(fstim) else None
+        if len(istim):
+            inidx = _u32([p[0] for p in istim])
+            icur = _f32([p[1] for p in istim])
+        else:
+            inidx = icur = None
+        out = np.zeros(self.words, dtype=np.uint32)
+        self.lib.call("nemo_b200_shard_step", self.handle,
+                      _ptr(f, c_uint) if f is not None else None, 0 if f is None else f.size,
+                      _ptr(inidx, c_uint) if inidx is not None else None,
+                      _ptr(icur, c_float) if icur is not None else None,
+                      0 if inidx is None else inidx.size,
+                      out.ctypes.data_as(POINTER(ctypes.c_uint32)))
+        return out
+
+    def deliver(self, all_words):
+        """The cycle's fired words of every warp; returns all fired neurons."""
+        a = np.ascontiguousarray(all_words, dtype=np.uint32)
+        if a.size != self.total_words:
+            raise ValueError("expected %d fired words, got %d" % (self.total_words, a.size))
+        self.lib.call("nemo_b200_shard_deliver", self.handle, a.ctypes.data_as(POINTER(ctypes.c_uint32)),
+                      byref(self._fired), byref(self._nfired))
+        n = self._nfired.value
+        if n == 0:
+            return np.zeros(0, dtype=np.uint32)
+        return np.ctypeslib.as_array(self._fired, shape=(n,)).copy()
+
+    def step(self, fstim=(), istim=()):
+        local = self.step_local(fstim, istim)
+        if self._exchange is not None:
+            all_words = self._exchange(local)
+        else:
+            from .dist import exchange_fired_words
+            all_words = exchange_fired_words(local, self.first_word, self.total_words)
+        return self.deliver(all_words)
+
+
+

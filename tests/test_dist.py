@@ -12,7 +12,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from nemo_b200.dist import dp_grad, shard_instances, shard_trials
+from nemo_b200.dist import dp_grad, exchange_fired_words, shard_instances, shard_trials, shard_warps
 
 
 def test_shard_trials_covers_all_trials():
@@ -92,3 +92,56 @@ def test_data_parallel_gradient_equals_full_batch():
     net, ins, w, target, B = _problem()
     full = _grad(net, ins, w, target, 0, B).numpy()
     assert np.allclose(g, full, rtol=1e-12, atol=1e-12 * np.abs(full).max())
+
+
+def test_shard_warps_matches_library():
+    """The Python partition of warps over shards is the library's."""
+    import ctypes
+    from nemo_b200.nemo import PRODUCT_LIBRARY
+    lib = ctypes.CDLL(PRODUCT_LIBRARY)
+    first, count = ctypes.c_uint(), ctypes.c_uint()
+    for total in (1, 7, 100, 3125, 3126):
+        for world in (1, 2, 3, 8):
+            covered = 0
+            for rank in range(world):
+                assert lib.nemo_b200_shard_warps(total, rank, world, ctypes.byref(first), ctypes.byref(count)) == 0
+                assert (first.value, count.value) == shard_warps(total, rank, world)
+                assert first.value == covered
+                covered += count.value
+            assert covered == total
+    assert lib.nemo_b200_shard_warps(10, 2, 2, ctypes.byref(first), ctypes.byref(count)) != 0
+
+
+def _words_of(total):
+    return (np.arange(total, dtype=np.uint64) * 2654435761 % (1 << 32)).astype(np.uint32)
+
+
+def _exchange_worker(rank, world, port, total, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        f, c = shard_warps(total, rank, world)
+        full = exchange_fired_words(_words_of(total)[f:f + c], f, total)
+        out.put((rank, full))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+@pytest.mark.parametrize("total", [5, 3125])
+def test_exchange_fired_words_two_ranks(total):
+    """Each of two gloo ranks contributes the words of its own warps (shares
+    of unequal size when total is odd); both get every warp's word."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_exchange_worker, args=(r, 2, port, total, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(out.get(timeout=240) for _ in range(2))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in range(2):
+        assert np.array_equal(got[r], _words_of(total))
