@@ -26,6 +26,8 @@ One bench step = 100 simulated 1 ms cycles followed by applyStdp(1.0).
 
 Multi-GPU (--gpus N under torchrun): N independent replicas of the workload,
 one per GPU (weak scaling); value = all replicas' events / max device time.
+--sharded: one network over the N GPUs as shards, the fired words
+all-gathered every cycle (strong scaling).
 """
 
 import argparse
@@ -684,6 +686,82 @@ def run_mixed(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args):
+    """One network over all ranks (--sharded under torchrun): the
+    1e8-synapse STDP network as N shards (ShardedSimulation), one per GPU,
+    each owning a contiguous range of the neuron warps and the synapses to
+    them; every cycle the shards' fired words are all-gathered (NCCL) and
+    delivered, and applyStdp runs every 100 cycles (strong scaling). Every
+    cycle is host-synchronous (the step's fired words come back before the
+    exchange), so the time is the host clock between device
+    synchronisations, max over ranks; events are the shards' device
+    counters summed over ranks."""
+    import torch
+    import torch.distributed as dist
+    from nemo_b200.nemo import ShardedSimulation
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    wl = workload(args.small)
+    lib = Library()
+    spec = netgen.izhikevich_random(wl["n"], wl["m"], dmax=wl["dmax"], seed=wl["seed"], stdp=True)
+    net = spec.build(Network(lib))
+    conf = Configuration(lib)
+    pre, post = netgen.standard_stdp()
+    conf.set_stdp_function(pre, post, 0.0, 1.0, 0.0, -1.0)
+    conf.set_write_only_synapses()
+    conf.set_cuda_backend(local)
+    sim = ShardedSimulation(net, conf, rank, world)
+    del net
+    lib.dll.nemo_b200_counters.argtypes = [ctypes.c_void_p, ctypes.c_uint64 * 4]
+    counters = (ctypes.c_uint64 * 4)()
+
+    def steps(k):
+        for _ in range(k):
+            for _ in range(CYCLES_PER_STEP):
+                sim.step()
+            sim.apply_stdp(REWARD)
+
+    steps(max(args.warmup, 1))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    lib.call("nemo_b200_counters", sim.handle, counters)
+    ev0 = counters[3]
+    t0 = time.perf_counter()
+    steps(args.steps)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    lib.call("nemo_b200_counters", sim.handle, counters)
+    events = float(counters[3] - ev0)
+    if world > 1:
+        t = torch.tensor([secs, events], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        secs, events = float(mx[0]), float(t[1])
+    launches = args.steps * (CYCLES_PER_STEP * (1 + (1 if world > 1 else 0)) + 1 + apply_launches(sim, lib))
+    line = {"metric": METRIC, "value": round(events / secs, 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs * 1e3 / args.steps, 4),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "int32/int64 fixed point + f32/f64 state",
+            "data": "synthetic (seeded generator, numpy PCG64 seed %d)" % wl["seed"],
+            "config": {"workload": wl["name"], "neurons": wl["n"], "synapses": wl["n"] * wl["m"],
+                       "parallelism": "shards%d" % world, "cycles_per_step": CYCLES_PER_STEP,
+                       "exchange": "all-gather of the fired words every cycle"},
+            "timing": "host clock around host-synchronous cycles, max over ranks",
+            "sim_ms_per_wall_s": round(CYCLES_PER_STEP * args.steps / secs, 1),
+            "gpu_launches": launches}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -699,11 +777,15 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--bptt", action="store_true",
                     help="measure the differentiable form (BPTT grad steps/s) instead of the headline workload")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one network over all ranks as shards (fired words all-gathered every cycle)")
     ap.add_argument("--mixed", action="store_true",
                     help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
     ap.add_argument("--mixed-cycles", type=int, default=1000)
     args = ap.parse_args()
-    if args.mixed:
+    if args.sharded:
+        run_sharded(args)
+    elif args.mixed:
         run_mixed(args)
     elif args.bptt:
         run_bptt(args)
