@@ -824,7 +824,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		 * handed out by a block counter so that warps without neurons to
 		 * update start at once. Units [0, G): 32 fired
 		 * sources each; units [G, G + S): this block's share of the grid's
-		 * 128-synapse STDP items (item u * B + b) ---- */
+		 * STDP items (item u * B + b) ---- */
 		if(doPrev) {
 			const uint32_t par = (t - 1u) & 1u;
 			const uint32_t nLists = B + (net.remoteList ? 1u : 0u);
@@ -872,10 +872,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t total = __shfl_sync(FULL, incl, 31);
 					const uint32_t excl = incl - cnt;
 					pushed += lane == 0 ? total : 0u;
-					for(uint32_t base = 0; base < total; base += 128u) {
-						uint2 r[4];
+					for(uint32_t base = 0; base < total; base += 32u * GATHER_PER_LANE) {
+						uint2 r[GATHER_PER_LANE];
 #pragma unroll
-						for(int x = 0; x < 4; ++x) {
+						for(int x = 0; x < GATHER_PER_LANE; ++x) {
 							const uint32_t idx = base + uint32_t(x) * 32u + lane;
 							/* the lane whose range holds idx: the last with excl <= idx */
 							uint32_t lo = 0;
@@ -889,7 +889,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							r[x] = idx < total ? __ldcs(&region[bL + (idx - eL)]) : make_uint2(0u, 0u);
 						}
 #pragma unroll
-						for(int x = 0; x < 4; ++x) {
+						for(int x = 0; x < GATHER_PER_LANE; ++x) {
 							if(base + uint32_t(x) * 32u + lane < total) {
 								uint32_t slot = slotPrev + (r[x].x & 63u) + 1u;
 								slot = slot >= net.slots ? slot - net.slots : slot;
@@ -914,29 +914,32 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					 * one writer */
 					const uint32_t it = (u - G - NW) * B + b;
 					const uint32_t tg = it / chunks;
-					const uint32_t off = (it - tg * chunks) * 128u;
+					const uint32_t item = 32u * STDP_PER_LANE;
+					const uint32_t off = (it - tg * chunks) * item;
 					const uint32_t bb = findList(sPreP, B, tg);
 					const uint2 range = plist[size_t(bb) * ownN + (tg - sPreP[bb])];
 					if(off < range.y) {
 						const uint32_t b0 = range.x + off;
-						const uint32_t cnt = range.y - off < 128u ? range.y - off : 128u;
+						const uint32_t cnt = range.y - off < item ? range.y - off : item;
 						visited += cnt;
-						uint32_t sd[4];
+						/* the accumulators do not depend on the sources: load
+						 * them with the source words, before the histories */
+						uint32_t sd[STDP_PER_LANE];
+						int32_t old[STDP_PER_LANE];
 #pragma unroll
-						for(int x = 0; x < 4; ++x) {
+						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
 							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
-						}
-						uint64_t pre[4];
-						int32_t old[4];
-#pragma unroll
-						for(int x = 0; x < 4; ++x) {
-							const uint32_t jj = lane + 32u * x;
-							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
 							old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
 						}
+						uint64_t pre[STDP_PER_LANE];
 #pragma unroll
-						for(int x = 0; x < 4; ++x) {
+						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+							const uint32_t jj = lane + 32u * x;
+							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
+						}
+#pragma unroll
+						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
 							if(jj < cnt) {
 								const int32_t dw = weightChange(pre[x], A.rule);

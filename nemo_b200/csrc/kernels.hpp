@@ -27,7 +27,8 @@
  *     t-1 (all blocks' lists) and, for each, its segment of region b, adding
  *     each weight of delay d >= 2 into slot (t-1+d) mod Q of the target (E or
  *     I by sign), and the STDP accumulation of cycle t-1 over all blocks'
- *     post-spiking targets, dealt out over the grid in 128-synapse items.
+ *     post-spiking targets, dealt out over the grid in items of 32 x
+ *     STDP_PER_LANE synapses.
  *     Together the inbox and the gather are the reference's deliverSpikes at
  *     cycle t0+d (src/nemo/cpu/Simulation.cpp:259-308);
  *   - grid barrier.
@@ -50,6 +51,12 @@ const uint32_t MAX_BLOCKS = 256;
 const uint64_t APPLY_GROUP_SYNAPSES = uint64_t(1) << 24;
 /* plastic synapses per lane in one applyStdp work item */
 const uint32_t APPLY_PER_LANE = 4;
+/* forward records a gather lane loads per round (one round covers a unit of
+ * 32 sources of about 7 records each in a block's region) */
+const int GATHER_PER_LANE = 8;
+/* plastic synapses a lane visits in one STDP accumulation item (an item is
+ * 32 x STDP_PER_LANE synapses of one post-spiking target) */
+const uint32_t STDP_PER_LANE = 4;
 /* shared memory the step kernel may use for current slots */
 const uint32_t SMEM_ACC_LIMIT = 200 * 1024;
 
@@ -108,7 +115,7 @@ struct NetDev {
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
-	uint32_t stdpChunks;           /* 128-synapse chunks per target (max in-degree) */
+	uint32_t stdpChunks;           /* STDP items per target (max in-degree / (32 x STDP_PER_LANE)) */
 	uint32_t applyChunks;          /* (32 x APPLY_PER_LANE)-synapse chunks per target */
 	const uint32_t* rcmStart;      /* [nDev + 1] (fewer than 2^32 synapses) */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */

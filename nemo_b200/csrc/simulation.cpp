@@ -362,10 +362,11 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 			rcmForward[j] = uint32_t(pos);
 		}
 	}
-	/* 128-synapse STDP work items per post-spiking target */
-	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + 127) / 128);
+	/* STDP work items (32 x STDP_PER_LANE synapses) per post-spiking target */
+	const uint64_t stdpItem = 32u * STDP_PER_LANE;
+	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + stdpItem - 1) / stdpItem);
 	if(uint64_t(m_nDev) * stdpChunks >= (uint64_t(1) << 32)) {
-		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 / 128 plastic synapses per neuron");
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 STDP items (targets x items per target)");
 	}
 
 	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
