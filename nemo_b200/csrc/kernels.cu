@@ -1111,15 +1111,21 @@ __device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule
 	}
 }
 
-/* Items (target, 128-synapse chunk of its plastic synapses) of the targets
- * [t0, t1) over a grid-stride loop. The host launches one such kernel per
- * group of consecutive owner blocks whose forward regions together fit
- * comfortably in L2 (APPLY_GROUP_SYNAPSES): a target's plastic synapses all
- * lie in its owner's region (or the delay-1 part), so every forward record a
- * launch rewrites is loaded from DRAM once and reused from L2 by the other
- * targets that share its sector. */
+/* Items (target, chunk of 32 x APPLY_PER_LANE of its plastic synapses) of
+ * the targets [t0, t1) over a grid-stride loop. The host launches one such
+ * kernel per group of consecutive owner blocks whose forward regions together
+ * fit comfortably in L2 (APPLY_GROUP_SYNAPSES): a target's plastic synapses
+ * all lie in its owner's region (or the delay-1 part), so every forward
+ * record a launch rewrites is loaded from DRAM once and reused from L2 by the
+ * other targets that share its sector.
+ *
+ * skipZero: every plastic weight lies within its bounds, so a synapse whose
+ * accumulator is 0 keeps its weight (updatedWeight only clamps) and its
+ * accumulator: its forward index and record are not loaded. Without it (the
+ * first apply of weights set out of bounds) every synapse is clamped, as in
+ * ConnectivityMatrix.cpp:295-318. */
 __global__ void __launch_bounds__(256)
-k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint32_t t0, uint32_t t1)
+k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint32_t t0, uint32_t t1, int skipZero)
 {
 	const uint64_t* rfNow = net.rf + size_t(cycleNow & 1u) * net.nDev;
 	const uint32_t lane = threadIdx.x & 31u;
@@ -1133,23 +1139,29 @@ k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint3
 		const uint32_t e = net.rcmStart[t + 1];
 		if(b0 >= e) continue;
 		const uint32_t j = b0 + lane;
-		uint32_t f[APPLY_PER_LANE];
+		/* the forward indices are loaded with the accumulators (one round
+		 * trip); only the forward records wait for the accumulator test */
 		int32_t a[APPLY_PER_LANE];
+		uint32_t f[APPLY_PER_LANE];
+		bool live[APPLY_PER_LANE];
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			const uint32_t jj = j + 32u * u;
-			f[u] = jj < e ? __ldcs(&net.rcmForward[jj]) : 0u;
 			a[u] = jj < e ? __ldcs(&net.rcmAcc[jj]) : 0;
+			f[u] = jj < e ? __ldcs(&net.rcmForward[jj]) : 0u;
+		}
+#pragma unroll
+		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
+			live[u] = j + 32u * u < e && (a[u] != 0 || !skipZero);
 		}
 		uint2 syn[APPLY_PER_LANE];
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			syn[u] = j + 32u * u < e ? net.fcm[f[u]] : make_uint2(0u, 0u);
+			syn[u] = live[u] ? net.fcm[f[u]] : make_uint2(0u, 0u);
 		}
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			const uint32_t jj = j + 32u * u;
-			if(jj < e) applyOne(net, rule, reward, cycleNow, rfNow, jj, f[u], a[u], syn[u]);
+			if(live[u]) applyOne(net, rule, reward, cycleNow, rfNow, j + 32u * u, f[u], a[u], syn[u]);
 		}
 	}
 }
@@ -1392,7 +1404,7 @@ applyBlocksPerSm()
 
 void
 launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
-		const uint32_t* groupTargets, uint32_t groups, void* stream)
+		const uint32_t* groupTargets, uint32_t groups, bool skipZero, void* stream)
 {
 	for(uint32_t g = 0; g < groups; ++g) {
 		const uint32_t t0 = groupTargets[g], t1 = groupTargets[g + 1];
@@ -1402,7 +1414,7 @@ launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_
 		uint64_t blocks = (items * 32 + 255) / 256;
 		const uint64_t cap = uint64_t(smCount()) * applyBlocksPerSm();
 		if(blocks > cap) blocks = cap;
-		k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow, t0, t1);
+		k_apply_stdp<<<uint32_t(blocks), 256, 0, S(stream)>>>(net, rule, reward, cycleNow, t0, t1, skipZero ? 1 : 0);
 	}
 }
 

@@ -245,9 +245,10 @@ void launchCycles(const CycleArgs& args, void* stream);
 void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
 		bool* smemAcc);
 /* applyStdp over target groups [groupTargets[g], groupTargets[g+1]), one
- * launch per group (groups of owner blocks, see APPLY_GROUP_SYNAPSES) */
+ * launch per group (groups of owner blocks, see APPLY_GROUP_SYNAPSES);
+ * skipZero when every plastic weight is within its bounds (k_apply_stdp) */
 void launchApplyStdp(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
-		const uint32_t* groupTargets, uint32_t groups, void* stream);
+		const uint32_t* groupTargets, uint32_t groups, bool skipZero, void* stream);
 void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n,
 		const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);

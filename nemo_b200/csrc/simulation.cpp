@@ -253,6 +253,17 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	 * a slot of target t only ever holds at most one arrival per incoming
 	 * synapse, so it is bounded by the sum of its in-weights, taking each
 	 * plastic weight at its STDP limit if that is larger */
+	/* src/nemo/StdpProcess.cpp:129-137: a weight updatedWeight leaves alone
+	 * when the change is 0 */
+	if(m_stdpOn) {
+		m_weightsInRange = true;
+		for(size_t s = 0; s < S && m_weightsInRange; ++s) {
+			if(!net.plastic[s]) continue;
+			const int64_t w = wfx[s];
+			if(w > 0) m_weightsInRange = w >= m_rule.minE && w <= m_rule.maxE;
+			else if(w < 0) m_weightsInRange = w >= m_rule.maxI && w <= m_rule.minI;
+		}
+	}
 	bool acc32 = true;
 	{
 		std::vector<int64_t> pos(m_nDev, 0), neg(m_nDev, 0);
@@ -687,6 +698,16 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	return m_fired;
 }
 
+/* One applyStdp on the simulation's stream. Every plastic weight is within
+ * its bounds afterwards (updatedWeight clamps each one). */
+void
+Simulation::launchApply(int32_t reward)
+{
+	launchApplyStdp(m_net, m_rule, reward, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1),
+			m_weightsInRange, m_stream);
+	m_weightsInRange = true;
+}
+
 void
 Simulation::notShard(const char* what) const
 {
@@ -1070,7 +1091,7 @@ Simulation::applyStdp(float reward)
 		flushShard();
 	}
 	if(m_nrcm) {
-		launchApplyStdp(m_net, m_rule, fx, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
+		launchApply(fx);
 	}
 	m_fcmHostValid = false;
 }
@@ -1316,7 +1337,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 		launchBlock(m_cycle, cyclesPerStep);
 		m_cycle += cyclesPerStep;
 		if(apply && m_nrcm) {
-			launchApplyStdp(m_net, m_rule, fx, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
+			launchApply(fx);
 		}
 	}
 	NEMO_CUDA(cudaEventRecord(e1, stream));
@@ -1353,7 +1374,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	m_cycle += cycles;
 	NEMO_CUDA(cudaEventRecord(e1, stream));
 	if(m_stdpOn && m_nrcm) {
-		launchApplyStdp(m_net, m_rule, toFix(reward, m_fbits), m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1), m_stream);
+		launchApply(toFix(reward, m_fbits));
 		m_fcmHostValid = false;
 	}
 	NEMO_CUDA(cudaEventRecord(e2, stream));

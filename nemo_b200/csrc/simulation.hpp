@@ -189,6 +189,7 @@ private:
 	void stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 			bool ownedOnly);
 	void notShard(const char* what) const;
+	void launchApply(int32_t reward);
 	bool owns(uint32_t dev) const { return dev / 32 >= m_shard.warpLo && dev / 32 < m_shard.warpHi; }
 	void flushShard();
 	void checkDeviceError();
@@ -213,6 +214,9 @@ private:
 	std::vector<uint32_t> m_applyGroups;  /* applyStdp launch target ranges (prefix) */
 	bool m_stdpOn;
 	StdpRule m_rule;
+	/* every plastic weight within its STDP bounds (then applyStdp leaves
+	 * synapses with a zero accumulator alone); true after any applyStdp */
+	bool m_weightsInRange = false;
 	StdpFunction m_stdpFn;
 	uint32_t m_ring;
 

@@ -110,6 +110,30 @@ def test_stdp_network_weights(oracle_lib):
             assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid)
 
 
+def test_stdp_clamps_out_of_bound_weights(oracle_lib):
+    """Excitatory weights up to 0.5 with an STDP bound of 0.3: the first
+    applyStdp clamps every plastic weight, those with a zero accumulator
+    included (after it, synapses with a zero accumulator are left alone);
+    every weight equals the oracle's after each apply."""
+    spec = netgen.izhikevich_random(2000, 100, dmax=20, seed=6, stdp=True)
+    pre, post = netgen.standard_stdp()
+    (gn, g), (on, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 0.3, 0.0, -1.0)))
+    sources = range(0, 2000, 11)
+    for epoch in range(3):
+        for c in range(50):
+            a, b = g.step(), o.step()
+            assert np.array_equal(a, b), "epoch %d cycle %d" % (epoch, c)
+        g.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+        clamped = 0
+        for src in sources:
+            for sid in g.get_synapses_from(src):
+                wg = g.get_synapse_weight(sid)
+                assert wg == o.get_synapse_weight(sid), (epoch, src, sid)
+                clamped += abs(wg - 0.3) < 2e-6   # the bound in Q11.20
+        assert clamped > 0
+
+
 def test_expf_exhaustive():
     """The Hodgkin-Huxley model's device expf reproduces host glibc expf on
     every float in [-104, 89]."""
