@@ -1081,7 +1081,7 @@ k_stimulus_scratch(NetDev net, const uint32_t* scratch, uint32_t nf, uint32_t ni
  * source's firing history after the last completed cycle (cycleNow - 1):
  * bit k fired at cycleNow-1-k and arrives at cycleNow-1-k+d. */
 __device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
-		const uint64_t* rfNow, uint32_t j, uint32_t f, int32_t acc, uint2 syn)
+		const uint64_t* rfNow, uint32_t j, uint32_t f, int32_t acc, uint2 syn, uint32_t sd)
 {
 	const int32_t wOld = int32_t(syn.y);
 	const int32_t diff = int32_t((int64_t(reward) * int64_t(acc)) >> net.fbits);
@@ -1089,7 +1089,6 @@ __device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule
 	if(wNew != wOld) {
 		net.fcm[f].y = uint32_t(wNew);
 		if(net.deliver) {
-			const uint32_t sd = net.rcmSrcDelay[j];
 			const uint32_t d = (sd & 63u) + 1u;
 			uint64_t pending = rfNow[sd >> 6] & ((uint64_t(1) << d) - 1u);
 			if(pending) {
@@ -1154,14 +1153,18 @@ k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint3
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			live[u] = j + 32u * u < e && (a[u] != 0 || !skipZero);
 		}
+		/* the source words (for the in-flight correction of a changed
+		 * weight) come with the forward records */
 		uint2 syn[APPLY_PER_LANE];
+		uint32_t sd[APPLY_PER_LANE];
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			syn[u] = live[u] ? net.fcm[f[u]] : make_uint2(0u, 0u);
+			sd[u] = live[u] && net.deliver ? __ldcs(&net.rcmSrcDelay[j + 32u * u]) : 0u;
 		}
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			if(live[u]) applyOne(net, rule, reward, cycleNow, rfNow, j + 32u * u, f[u], a[u], syn[u]);
+			if(live[u]) applyOne(net, rule, reward, cycleNow, rfNow, j + 32u * u, f[u], a[u], syn[u], sd[u]);
 		}
 	}
 }
