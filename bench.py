@@ -550,7 +550,7 @@ def run_bptt(args):
     net = LIFNetwork.random(n, fan, chans, infan, seed=7, checkpoint=50, bin_steps=binsteps, kappa=10.0)
     w = net.initial_weights(seed=7, scale_in=0.35).requires_grad_(True)
     # data parallel over trials: every rank runs 32 trials of its own
-    bits, _ = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8 + 1000 * rank)
+    bits, in_spikes = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8 + 1000 * rank)
     target = sinusoid_target(steps // binsteps, binsteps)
     build_s = time.perf_counter() - t0
 
@@ -603,10 +603,89 @@ def run_bptt(args):
         "forward_ms": round(fwd_ms, 3), "backward_ms": round(bwd_ms, 3),
         "synapse_steps_per_s": round(net.synapses * trials * world * steps / (ms * 1e-3), 1),
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the float64 PyTorch reference of the model (the differentiable
+        # form's oracle) on the host cores: a bounded sample of the grad step
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import lif_reference as ref
+        cnet = LIFNetwork.random(n, fan, chans, infan, seed=7, checkpoint=50, bin_steps=binsteps, kappa=10.0,
+                                 device="cpu")
+        t_s, b_s = 10, 4
+        w64 = torch.tensor(w.detach().cpu().numpy().astype(np.float64), requires_grad=True)
+        c0 = time.perf_counter()
+        c = ref.counts(cnet, w64, in_spikes[:t_s], b_s)
+        rate_loss(c, n, binsteps, target.cpu().double()[:t_s // binsteps]).backward()
+        secs = time.perf_counter() - c0
+        scale = (steps / t_s) * (trials / b_s)
+        line["cpu_baseline"] = {"value": round(1.0 / (secs * scale), 8), "unit": "grad steps/s",
+                                "cores": torch.get_num_threads(), "kind": "port",
+                                "sample": "float64 PyTorch reference (autograd, surrogate gradient), %d of %d trials x "
+                                          "%d of %d steps in %.2f s, scaled linearly to the full grad step"
+                                          % (b_s, trials, t_s, steps, secs)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def run_random1k(args):
+    """The 1000-neuron benchmark network (800 excitatory / 200 inhibitory
+    Izhikevich neurons with thalamic noise sigma 5 / 2, 100 synapses per
+    neuron, delays U{1..20}, no STDP), 1000 cycles: device-resident (one
+    persistent launch per 1000 cycles, CUDA events) and through nemo_step
+    per cycle; the oracle on the host cores runs the same 1000 cycles, and
+    the per-cycle firing counts must agree."""
+    lib = Library()
+    spec = netgen.izhikevich_random(1000, 100, dmax=20, seed=1)
+    cycles = 1000
+    P = ctypes.POINTER
+    outdeg = spec.out_degree()
+
+    def step_run(sim_lib, sim):
+        fptr = P(ctypes.c_uint)()
+        nf = ctypes.c_size_t()
+        counts, events = [], 0
+        t0 = time.perf_counter()
+        for _ in range(cycles):
+            if sim_lib.dll.nemo_step(sim.handle, None, 0, None, None, 0, ctypes.byref(fptr), ctypes.byref(nf)) != 0:
+                raise RuntimeError(sim_lib.dll.nemo_strerror().decode())
+            counts.append(nf.value)
+            if nf.value:
+                events += int(outdeg[np.ctypeslib.as_array(fptr, shape=(nf.value,))].sum())
+        return time.perf_counter() - t0, counts, events
+
+    net = spec.build(Network(lib))
+    sim = Simulation(net, Configuration(lib))
+    e2e_s, e2e_counts, e2e_events = step_run(lib, sim)
+    # device-resident: fresh simulations, K timed launches of 1000 cycles after W
+    lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                              ctypes.c_float, ctypes.c_double * 4]
+    out = (ctypes.c_double * 4)()
+    sim2 = Simulation(spec.build(Network(lib)), Configuration(lib))
+    lib.call("nemo_b200_timed_steps", sim2.handle, max(args.warmup, 1), cycles, 0, ctypes.c_float(0), out)
+    lib.call("nemo_b200_timed_steps", sim2.handle, max(args.steps, 1), cycles, 0, ctypes.c_float(0), out)
+    ms, events = out[0], out[2]
+    k = max(args.steps, 1)
+    line = {"metric": "synaptic events/s (1000-neuron network)", "value": round(events / (ms * 1e-3), 1),
+            "unit": UNIT, "n_gpus": 1, "steps": k, "warmup": max(args.warmup, 1),
+            "ms_per_step": round(ms / k, 4), "higher_is_better": True,
+            "dtype": "int32/int64 fixed point + f32/f64 state", "data": "synthetic (seeded generator)",
+            "config": {"workload": "izhikevich-1k-m100", "neurons": 1000, "synapses": 100000,
+                       "cycles_per_step": cycles, "noise": "sigma 5 / 2"},
+            "sim_ms_per_wall_s": round(cycles * k / (ms * 1e-3), 1),
+            "e2e": {"value": round(e2e_events / e2e_s, 1), "unit": UNIT, "sim_ms_per_wall_s": round(cycles / e2e_s, 1),
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * sum(e2e_counts)}}
+    if not args.no_cpu_baseline:
+        ol = Library(oracle_library())
+        oconf = Configuration(ol)
+        oconf.set_cpu_backend()
+        osim = Simulation(spec.build(Network(ol)), oconf)
+        o_s, o_counts, o_events = step_run(ol, osim)
+        line["cpu_baseline"] = {"value": round(o_events / o_s, 1), "unit": UNIT, "cores": os.cpu_count(),
+                                "kind": "port", "sample": "the same 1000 cycles, %.2f s" % o_s,
+                                "sim_ms_per_wall_s": round(cycles / o_s, 1),
+                                "firing_counts_equal": o_counts == e2e_counts}
+    print(json.dumps(line), flush=True)
 
 
 def run_mixed(args):
@@ -777,13 +856,17 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--bptt", action="store_true",
                     help="measure the differentiable form (BPTT grad steps/s) instead of the headline workload")
+    ap.add_argument("--random1k", action="store_true",
+                    help="measure the 1000-neuron benchmark network (no STDP)")
     ap.add_argument("--sharded", action="store_true",
                     help="one network over all ranks as shards (fired words all-gathered every cycle)")
     ap.add_argument("--mixed", action="store_true",
                     help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
     ap.add_argument("--mixed-cycles", type=int, default=1000)
     args = ap.parse_args()
-    if args.sharded:
+    if args.random1k:
+        run_random1k(args)
+    elif args.sharded:
         run_sharded(args)
     elif args.mixed:
         run_mixed(args)

@@ -1,5 +1,7 @@
 """A plain-PyTorch float64 restatement of the discrete LIF network of
-nemo_b200/csrc/lif_bptt.cu (test infrastructure): the same model, with the
+nemo_b200/csrc/lif_bptt.cu -- the oracle of the differentiable form (no
+reference implementation exists; used by the tests and by bench.py's CPU
+baseline of the BPTT line, never by the product): the same model, with the
 spike's derivative replaced by the same fast-sigmoid surrogate through
 torch.autograd, so that its gradient is the reference for the adjoint kernel.
 

@@ -7,6 +7,9 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+# the float64 reference of the differentiable form (oracle/lif_reference.py)
+if os.path.join(ROOT, "oracle") not in sys.path:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 ORACLE_LIB = os.path.join(ROOT, "oracle", "_build", "libnemo_oracle.so")
 ORACLE_REF_DIR = os.path.join(ROOT, "oracle", "_ref")
