@@ -646,8 +646,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t b = blockIdx.x;
 	const size_t nDev = net.nDev;
 	const uint32_t ownN = net.ownWarps * 32u;       /* list and slot stride per block */
-	const uint32_t firstWarp = net.warpBase + ownFirst(b, net.ownQ, net.ownR);
-	const uint32_t myWarps = net.ownQ + (b < net.ownR ? 1u : 0u);
+	const uint32_t firstWarp = net.warpBase + net.ownStart[b];
+	const uint32_t myWarps = net.ownStart[b + 1] - net.ownStart[b];
 	const uint32_t myN = myWarps * 32u;
 	const uint32_t ownBase = firstWarp * 32u;
 	const uint32_t updWarps = min(myWarps, warpsPerBlock);
@@ -1333,17 +1333,32 @@ launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, u
 }
 
 /* The step kernel's plan: one 1024-thread block per SM (its registers allow
- * no more), the neuron warps split as evenly as possible over the blocks; the
- * owned current slots go to shared memory when they are int32 and fit. */
+ * no more) and no block without neurons; the neuron warps split into
+ * contiguous ranges of about equal summed update cost (block b starts at the
+ * first warp whose cost prefix reaches b / B of the total); the owned
+ * current slots go to shared memory when they are int32 and fit. */
 void
-cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
-		bool* smemAcc)
+cyclesPlan(const std::vector<uint32_t>& warpCost, uint32_t slots, bool acc32, uint32_t* blocks,
+		std::vector<uint32_t>* ownStart, uint32_t* ownWarps, bool* smemAcc)
 {
+	const uint32_t totalWarps = uint32_t(warpCost.size());
 	uint32_t B = uint32_t(smCount());
 	if(B > MAX_BLOCKS) B = MAX_BLOCKS;
-	const uint32_t q = totalWarps / B, r = totalWarps % B;
-	const uint32_t own = q + (r ? 1u : 0u);
-	const uint64_t bytes = uint64_t(slots) * own * 32u * 8u;
+	/* no block without neurons (a small network's extra blocks would only
+	 * wait at the grid barrier) */
+	if(B > totalWarps) B = totalWarps > 0 ? totalWarps : 1u;
+	std::vector<uint64_t> prefix(size_t(totalWarps) + 1, 0);
+	for(uint32_t w = 0; w < totalWarps; ++w) prefix[w + 1] = prefix[w] + warpCost[w];
+	ownStart->assign(size_t(B) + 1, totalWarps);
+	uint32_t most = 0;
+	for(uint32_t b = 0; b < B; ++b) {
+		const uint64_t target = prefix[totalWarps] * b / B;
+		(*ownStart)[b] = uint32_t(std::lower_bound(prefix.begin(), prefix.end(), target) - prefix.begin());
+		if((*ownStart)[b] > totalWarps) (*ownStart)[b] = totalWarps;
+	}
+	(*ownStart)[0] = 0;
+	for(uint32_t b = 0; b < B; ++b) most = std::max(most, (*ownStart)[b + 1] - (*ownStart)[b]);
+	const uint64_t bytes = uint64_t(slots) * most * 32u * 8u;
 	const bool smem = acc32 && bytes <= SMEM_ACC_LIMIT;
 	/* the attribute is per device and shared by all simulations: set it to
 	 * the largest size any of them uses */
@@ -1357,8 +1372,7 @@ cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, ui
 		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false, 1024>, 1024, 0);
 	}
 	*blocks = perSm >= 1 ? B : 0u;
-	*ownQ = q;
-	*ownR = r;
+	*ownWarps = most;
 	*smemAcc = smem;
 }
 

@@ -12,7 +12,7 @@
  *
  * The step path is one persistent cooperative kernel (k_cycles) over one
  * block per SM, with one grid barrier per cycle. Block b owns a contiguous
- * range of 32-neuron warps (ownerOf below): it updates them, and it alone adds spikes
+ * range of 32-neuron warps (NetDev::ownStart): it updates them, and it alone adds spikes
  * into their current slots, which it keeps in shared memory for the whole
  * launch (or in global memory when they do not fit). The forward matrix is
  * partitioned to match: region b holds, source by source, the synapses of
@@ -37,6 +37,7 @@
  * in any order, so the result is bit-identical to the CPU reference. */
 
 #include <cstdint>
+#include <vector>
 
 #include <vector_types.h>
 
@@ -69,16 +70,15 @@ struct NetDev {
 	uint32_t fbits;         /* fractional bits of the Q(31-f).f weights */
 	int deliver;            /* 0 when no delay is deliverable (max delay 64) */
 
-	/* ownership: with q = warps / blocks and r = warps % blocks, block b owns
-	 * the q + (b < r) neuron warps from b * q + min(b, r) (ownFirst); ownWarps
-	 * = q + (r > 0) is the most any block owns */
+	/* ownership: block b owns the neuron warps [ownStart[b], ownStart[b+1])
+	 * (relative to warpBase; contiguous, split by the warps' update cost,
+	 * cyclesPlan); ownWarps is the most any block owns */
 	uint32_t blocks;
 	uint32_t threads;       /* threads per block of the step kernel: 1024, 512 or 256 */
 	uint32_t ownWarps;
-	uint32_t ownQ;
-	uint32_t ownR;
+	const uint32_t* ownStart;   /* [blocks + 1] */
 	/* first warp of the owned range: 0, or in a sharded simulation the
-	 * shard's first warp (block b owns warps warpBase + ownFirst(b)...) */
+	 * shard's first warp (block b owns warps warpBase + ownStart[b]...) */
 	uint32_t warpBase;
 	int smemAcc;            /* current slots of the owned neurons in shared memory */
 
@@ -227,23 +227,18 @@ void launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t 
 #endif
 
 /* First neuron warp owned by block b, and the block owning neuron warp w */
-NEMO_HD inline uint32_t ownFirst(uint32_t b, uint32_t q, uint32_t r) { return b * q + (b < r ? b : r); }
-NEMO_HD inline uint32_t ownerOf(uint32_t w, uint32_t q, uint32_t r)
-{
-	const uint32_t big = r * (q + 1u);
-	return w < big ? w / (q + 1u) : r + (w - big) / q;
-}
 
 /* Cooperative launch of k_cycles (grid, block size and shared memory from
  * args.net). */
 void launchCycles(const CycleArgs& args, void* stream);
-/* The step kernel's grid (one block per SM, at most MAX_BLOCKS; 0 when the
- * kernel cannot be resident), the split of the neuron warps over its blocks
- * (q, r: see NetDev), and whether the owned current slots fit in shared
- * memory (`slots` slots of 8-byte int32 E/I pairs; int64 sums use global
- * memory). */
-void cyclesPlan(uint32_t totalWarps, uint32_t slots, bool acc32, uint32_t* blocks, uint32_t* ownQ, uint32_t* ownR,
-		bool* smemAcc);
+/* The step kernel's grid (one block per SM, at most MAX_BLOCKS and at most
+ * one per neuron warp; 0 when the kernel cannot be resident) and the split of
+ * the neuron warps over its blocks: contiguous ranges of about equal summed
+ * cost (warpCost[w]: the update cost of warp w), ownStart[blocks + 1]; the
+ * most warps a block owns, and whether the owned current slots fit in shared
+ * memory. */
+void cyclesPlan(const std::vector<uint32_t>& warpCost, uint32_t slots, bool acc32, uint32_t* blocks,
+		std::vector<uint32_t>* ownStart, uint32_t* ownWarps, bool* smemAcc);
 /* applyStdp over target groups [groupTargets[g], groupTargets[g+1]), one
  * launch per group (groups of owner blocks, see APPLY_GROUP_SYNAPSES);
  * skipZero when every plastic weight is within its bounds (k_apply_stdp) */

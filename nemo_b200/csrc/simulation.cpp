@@ -281,10 +281,25 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		}
 	}
 
-	uint32_t ownQ = 0, ownR = 0;
+	/* update cost per owned warp: an HH warp (999 substeps of six exponentials
+	 * over eight lanes per neuron) counts 2.5 times another model's, so that
+	 * HH warps spread over more blocks while no block owns more warps than it
+	 * has update warps in a mixed network of a few HH neurons per ten others */
+	std::vector<uint32_t> warpCost(m_shard.warpHi - warpLo, 2u);
+	for(const Group& g : m_groups) {
+		if(g.type.kind != MODEL_HH) continue;
+		const uint32_t w0 = g.devBase / 32, w1 = uint32_t((uint64_t(g.devBase) + (uint64_t(g.count) << g.shift) + 31) / 32);
+		for(uint32_t w = std::max(w0, warpLo); w < std::min(w1, m_shard.warpHi); ++w) warpCost[w - warpLo] = 5u;
+	}
+	std::vector<uint32_t> ownStart;
+	uint32_t ownWarps = 0;
 	bool smemAcc = false;
-	cyclesPlan(m_shard.warpHi - warpLo, slots, acc32, &m_blocks, &ownQ, &ownR, &smemAcc);
-	const uint32_t ownWarps = ownQ + (ownR ? 1u : 0u);
+	cyclesPlan(warpCost, slots, acc32, &m_blocks, &ownStart, &ownWarps, &smemAcc);
+	/* owner block of each owned warp */
+	std::vector<uint32_t> ownerOfWarp(warpCost.size(), 0);
+	for(uint32_t b = 0; b + 1 < ownStart.size(); ++b) {
+		for(uint32_t w = ownStart[b]; w < ownStart[b + 1]; ++w) ownerOfWarp[w] = b;
+	}
 	NEMO_CUDA(cudaGetLastError());
 	if(m_blocks == 0) {
 		fail(NEMO_CUDA_INVOCATION_ERROR, "The step kernel cannot be resident on this device");
@@ -307,7 +322,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
 			if(net.dly[s] == 1) d1Start[dsrc[s] + 1]++;
-			else cursor[size_t(ownerOf(dtgt[s] / 32 - warpLo, ownQ, ownR)) * m_nDev + dsrc[s]]++;
+			else cursor[size_t(ownerOfWarp[dtgt[s] / 32 - warpLo]) * m_nDev + dsrc[s]]++;
 		}
 		for(uint32_t b = 0; b < B; ++b) {
 			uint32_t* c = &cursor[size_t(b) * m_nDev];
@@ -329,7 +344,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 			if(net.dly[s] == 1) {
 				pos = d1Base + d1Fill[dsrc[s]]++;
 			} else {
-				const uint32_t b = ownerOf(dtgt[s] / 32 - warpLo, ownQ, ownR);
+				const uint32_t b = ownerOfWarp[dtgt[s] / 32 - warpLo];
 				pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
 			}
 			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(wfx[s]));
@@ -344,7 +359,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	for(uint32_t b = 0; b < B;) {
 		uint32_t e = b + 1;
 		while(e < B && regionBase[e + 1] - regionBase[b] <= APPLY_GROUP_SYNAPSES) ++e;
-		m_applyGroups.push_back(std::min((warpLo + ownFirst(e, ownQ, ownR)) * 32u, m_nDev));
+		m_applyGroups.push_back(std::min((warpLo + ownStart[e]) * 32u, m_nDev));
 		b = e;
 	}
 
@@ -418,8 +433,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	m_net.blocks = B;
 	m_net.threads = 1024;
 	m_net.ownWarps = ownWarps;
-	m_net.ownQ = ownQ;
-	m_net.ownR = ownR;
+	m_net.ownStart = (const uint32_t*) put(ownStart.data(), ownStart.size() * 4);
 	m_net.warpBase = warpLo;
 	m_net.smemAcc = smemAcc ? 1 : 0;
 	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
