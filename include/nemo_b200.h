@@ -186,6 +186,7 @@ typedef struct nemo_b200_lif_net {
 	const int* colptr;
 	const int* post;
 	const int* wpos;
+	int nnz_rec;    /* recurrent synapses (colptr[N]) */
 } nemo_b200_lif_net;
 
 /* Bytes of the work buffer both calls need. */

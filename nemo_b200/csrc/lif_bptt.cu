@@ -58,6 +58,7 @@ struct Net {
 	const int* colptr;   /* [N + 1] recurrent out-synapses of each neuron */
 	const int* post;     /* [nnzRec] target */
 	const int* wpos;     /* [nnzRec] index of the synapse in w / pre */
+	int nnzRec;          /* colptr[N] */
 };
 
 /* spike of presynaptic unit p for the lane's trial at step t */
@@ -163,10 +164,22 @@ k_step(Net n, int t, const float* w, const uint32_t* inBits, uint32_t* sBits, fl
 	}
 }
 
+/* wOut[e] = w[n.wpos[e]]: the recurrent weights in out-synapse order */
+__global__ void
+k_gather_out(Net n, int nnzRec, const float* w, float* wOut)
+{
+	for(int e = int(blockIdx.x * blockDim.x + threadIdx.x); e < nnzRec; e += int(gridDim.x * blockDim.x)) {
+		wOut[e] = w[n.wpos[e]];
+	}
+}
+
 /* One backward step: gu[t] of every neuron j from gu[t+1] (guNext, [N][32])
- * and u[t] (uSeg). Warp per neuron (source view), lane per trial. */
+ * and u[t] (uSeg). Warp per neuron (source view), lane per trial; wOut: the
+ * recurrent weights in out-synapse order. A chunk's 32 rows of guNext are
+ * all loaded before they are summed (in synapse order), so that a warp keeps
+ * 32 loads in flight. */
 __global__ void __launch_bounds__(THREADS)
-k_back(Net n, int t, const float* w, const float* uSeg, int segStart, const float* guNext, float* guOut,
+k_back(Net n, int t, const float* wOut, const float* uSeg, int segStart, const float* guNext, float* guOut,
 		const float* dcounts, bool last)
 {
 	const uint32_t lane = threadIdx.x & 31u;
@@ -182,13 +195,18 @@ k_back(Net n, int t, const float* w, const float* uSeg, int segStart, const floa
 			for(int base = e0; base < e1; base += 32) {
 				const int e = base + int(lane);
 				const int i = e < e1 ? n.post[e] : 0;
-				const float we = e < e1 ? w[n.wpos[e]] : 0.0f;
+				const float we = e < e1 ? wOut[e] : 0.0f;
 				const int cnt = min(32, e1 - base);
-#pragma unroll 8
-				for(int q = 0; q < cnt; ++q) {
+				float g[32];
+#pragma unroll
+				for(int q = 0; q < 32; ++q) {
 					const int iq = __shfl_sync(FULL, i, q);
+					g[q] = q < cnt ? guNext[size_t(iq) * 32 + lane] : 0.0f;
+				}
+#pragma unroll
+				for(int q = 0; q < 32; ++q) {
 					const float wq = __shfl_sync(FULL, we, q);
-					gs = __fadd_rn(gs, __fmul_rn(wq, guNext[size_t(iq) * 32 + lane]));
+					if(q < cnt) gs = __fadd_rn(gs, __fmul_rn(wq, g[q]));
 				}
 			}
 			gv = __fmul_rn(n.beta, guNext[cell]);
@@ -315,6 +333,9 @@ validate(const Net& n)
 	if(n.T % n.binSteps != 0) {
 		fail(NEMO_INVALID_INPUT, "lif: the steps must be a whole number of bins");
 	}
+	if(n.nnzRec < 0) {
+		fail(NEMO_INVALID_INPUT, "lif: negative recurrent synapse count");
+	}
 }
 
 } // namespace
@@ -324,12 +345,13 @@ validate(const Net& n)
 using namespace nemo_b200;
 
 /* work buffer: v state [N][32], gu of the step after the segment [N][32],
- * the segment's u and gu [K][N][32], then the spike and input words
- * transposed to [unit][T] */
+ * the segment's u and gu [K][N][32], the spike and input words transposed to
+ * [unit][T], then the recurrent weights in out-synapse order [nnzRec] */
 static size_t
 workFloats(const lif::Net& n)
 {
-	return size_t(n.N) * 32 * (2 + 2 * size_t(n.K)) + (size_t(n.N) + size_t(n.C)) * size_t(n.T);
+	return size_t(n.N) * 32 * (2 + 2 * size_t(n.K)) + (size_t(n.N) + size_t(n.C)) * size_t(n.T)
+		+ size_t(n.nnzRec);
 }
 
 static std::string g_lifError;
@@ -400,6 +422,9 @@ nemo_b200_lif_backward(const nemo_b200_lif_net* net, const float* w, const uint3
 			lif::transpose(in_bits, inT, n.T, n.C, st);
 		}
 		const int g = lif::grid(n.N);
+		/* the recurrent weights in out-synapse order, for k_back */
+		float* wOut = reinterpret_cast<float*>(inT + size_t(n.C) * n.T);
+		if(n.nnzRec) lif::k_gather_out<<<g, lif::THREADS, 0, st>>>(n, n.nnzRec, w, wOut);
 		const int segments = (n.T + n.K - 1) / n.K;
 		for(int sgi = segments - 1; sgi >= 0; --sgi) {
 			const int c0 = sgi * n.K, c1 = std::min(n.T, c0 + n.K);
@@ -418,7 +443,7 @@ nemo_b200_lif_backward(const nemo_b200_lif_net* net, const float* w, const uint3
 			for(int t = c1 - 1; t >= c0; --t) {
 				const bool last = t == n.T - 1;
 				const float* next = t == c1 - 1 ? guNextSeg : guSeg + size_t(t + 1 - c0) * NS;
-				lif::k_back<<<g, lif::THREADS, 0, st>>>(n, t, w, uSeg, c0, next, guSeg, dcounts, last);
+				lif::k_back<<<g, lif::THREADS, 0, st>>>(n, t, wOut, uSeg, c0, next, guSeg, dcounts, last);
 			}
 			if(relaxed) {
 				lif::k_dw<true><<<g, lif::THREADS, 0, st>>>(n, c0, c1, guSeg, s_bits, s_float, in_bits, dw);

@@ -28,7 +28,7 @@ class LifNetStruct(ctypes.Structure):
                 ("K", ctypes.c_int), ("bin_steps", ctypes.c_int),
                 ("beta", ctypes.c_float), ("theta", ctypes.c_float), ("kappa", ctypes.c_float),
                 ("rowptr", ctypes.c_void_p), ("pre", ctypes.c_void_p), ("colptr", ctypes.c_void_p),
-                ("post", ctypes.c_void_p), ("wpos", ctypes.c_void_p)]
+                ("post", ctypes.c_void_p), ("wpos", ctypes.c_void_p), ("nnz_rec", ctypes.c_int)]
 
 
 def _bind(lib):
@@ -122,7 +122,7 @@ class LIFNetwork:
         return LifNetStruct(self.n, self.n_in, int(trials), int(steps), self.checkpoint, self.bin_steps,
                             self.beta, self.theta, self.kappa,
                             self._rowptr.data_ptr(), self._pre.data_ptr(), self._colptr.data_ptr(),
-                            self._post.data_ptr(), self._wpos.data_ptr())
+                            self._post.data_ptr(), self._wpos.data_ptr(), int(self._post.numel()))
 
 
 def _check(lib, status):
