@@ -71,6 +71,16 @@ nemo_status_t nemo_b200_step_noalloc(nemo_simulation_t sim,
 		const unsigned istim_nidx[], const float istim_current[], size_t istim_count,
 		unsigned fired[], size_t fired_capacity, size_t* fired_count);
 
+/* The status of the last call (NEMO_OK after a success): the code behind a
+ * NULL returned by a constructor, whose message nemo_strerror gives. */
+nemo_status_t nemo_b200_last_status(void);
+
+/* The largest synapse delay and the weight range of a network, as the
+ * reference's Network::maxDelay / minWeight / maxWeight give them (both
+ * weight bounds start at 0; src/nemo/NetworkImpl.cpp:25,108-110). */
+nemo_status_t nemo_b200_network_stats(nemo_network_t net, unsigned* max_delay, float* min_weight,
+		float* max_weight);
+
 /* Kernel launches one applyStdp makes (0 without plastic synapses). */
 nemo_status_t nemo_b200_apply_launches(nemo_simulation_t sim, unsigned* launches);
 

@@ -250,6 +250,23 @@ nemo_b200_new_batch(nemo_network_t nets[], size_t count, nemo_configuration_t c)
 	return NULL;
 }
 
+nemo_status_t nemo_b200_last_status(void) { return g_lastCallStatus; }
+
+nemo_status_t
+nemo_b200_network_stats(nemo_network_t n, unsigned* max_delay, float* min_weight, float* max_weight)
+{
+	RETURN_CALL({
+		float lo = 0.0f, hi = 0.0f;
+		for(float w : n->net.wgt) {
+			lo = std::min(lo, w);
+			hi = std::max(hi, w);
+		}
+		if(max_delay) *max_delay = n->net.maxDelay();
+		if(min_weight) *min_weight = lo;
+		if(max_weight) *max_weight = hi;
+	});
+}
+
 nemo_simulation_t
 nemo_b200_new_shard(nemo_network_t n, nemo_configuration_t c, unsigned rank, unsigned world)
 {

@@ -118,3 +118,39 @@ def test_expf_exception_table_is_small():
     assert lib.nemo_b200_expf_exceptions(ctypes.byref(count), ctypes.byref(tau)) == 0
     assert 0 < count.value < 2_000_000
     assert 0.0 < tau.value < 0.01
+
+
+def _build_cpp_check(tmp_path):
+    import shutil
+    import subprocess
+    from nemo_b200.nemo import PRODUCT_LIBRARY
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "cpp_api_check")
+    cxx = shutil.which("g++") or "g++"
+    libdir = os.path.dirname(PRODUCT_LIBRARY)
+    subprocess.check_call([cxx, "-std=c++11", "-Wall", "-I", os.path.join(root, "include"),
+                           os.path.join(root, "tests", "cpp_api_check.cpp"), "-L", libdir, "-lnemo_b200",
+                           "-Wl,-rpath," + libdir, "-o", exe])
+    return exe
+
+
+def test_cpp_api_without_device(tmp_path):
+    """include/nemo.hpp, the reference's C++ classes over the C ABI, compiled
+    into a C++ caller: construction, queries, configuration checks, and a
+    simulation that fails with a status when there is no device."""
+    import subprocess
+    exe = _build_cpp_check(tmp_path)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.split("\n")[:3] == ["ok construction", "ok configuration", "ok no device"]
+
+
+@pytest.mark.gpu
+def test_cpp_api_simulation(tmp_path):
+    """The C++ caller simulates a 64-neuron ring through nemo::simulation():
+    neuron k fires at cycle k."""
+    import subprocess
+    exe = _build_cpp_check(tmp_path)
+    r = subprocess.run([exe, "simulate"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "ok ring" in r.stdout
