@@ -727,6 +727,19 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				 * issued its loads, so that nothing orders them behind it */
 				uint32_t stimWord = lane == 0 ? net.fstim[dw] : 0u;
 				stimWord = __shfl_sync(FULL, stimWord, 0);
+				if(k == 0 && (A.inlineNf | A.inlineNi)) {
+					/* a step's short stimulus, from the parameters: this warp's
+					 * firing bits, and the currents of its own neurons (read
+					 * by the model below, by every lane of an HH neuron) */
+					for(uint32_t q = 0; q < A.inlineNf; ++q) {
+						const uint32_t x = A.inlineF[q];
+						if((x >> 5) == dw) stimWord |= 1u << (x & 31u);
+					}
+					for(uint32_t q = 0; q < A.inlineNi; ++q) {
+						if(A.inlineI[q] == n) net.ext[n] = A.inlineCur[q];
+					}
+					__syncwarp();
+				}
 				/* operands needed after the update, loaded with its own */
 				const uint64_t rfPrev = valid ? rfIn[n] : 0ull;
 				const uint32_t deg = valid ? __ldg(&net.outDegree[n]) : 0u;
@@ -778,6 +791,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const uint32_t word = __ballot_sync(FULL, fired);
 				if(lane == 0) {
 					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
+					if(A.hostWords) A.hostWords[dw] = word;
 				}
 				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
@@ -983,6 +997,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		if(trace && tid == 0) trace[3] = globalTimer();
 		if(k < A.cycles) {
 			if(!gridSync(net.barrier, A.timeoutNs)) {
+				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
 				return;
 			}
 		}
@@ -1399,7 +1414,7 @@ launchCycles(const CycleArgs& args, void* stream)
 {
 	void* params[] = {const_cast<CycleArgs*>(&args)};
 	const NetDev& net = args.net;
-	if(net.smemAcc) {
+	if(net.smemAcc && !args.globalAcc) {
 		const size_t bytes = size_t(net.slots) * net.ownWarps * 32u * 8u;
 		launchCyclesT<true>(args, params, bytes, S(stream));
 	} else {

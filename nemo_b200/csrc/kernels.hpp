@@ -58,6 +58,9 @@ const int GATHER_PER_LANE = 8;
 /* plastic synapses a lane visits in one STDP accumulation item (an item is
  * 32 x STDP_PER_LANE synapses of one post-spiking target) */
 const uint32_t STDP_PER_LANE = 4;
+/* stimulus entries of each kind a one-cycle step carries in its kernel
+ * parameters (CycleArgs::inlineF / inlineI) */
+const uint32_t INLINE_STIM_MAX = 32;
 /* shared memory the step kernel may use for current slots */
 const uint32_t SMEM_ACC_LIMIT = 200 * 1024;
 
@@ -186,6 +189,24 @@ struct CycleArgs {
 	 * 0 for the unsharded simulation; a sharded step is one update phase,
 	 * its flush one gather phase (cycles 0, carry 1). */
 	uint32_t carry;
+	/* run on the current slots in global memory even when the simulation
+	 * keeps them in shared memory across a launch (the same [slots][nDev]
+	 * array the shared copy is loaded from and spilled to): a launch of one
+	 * phase saves the copy in and out */
+	int globalAcc;
+	/* a one-cycle step's output in mapped host memory ([nWords + 1]): every
+	 * warp's fired word, and 1 in the last word when a grid barrier timed out
+	 * (the host zeroes it first); null otherwise */
+	uint32_t* hostWords;
+	/* a one-cycle step's stimulus when it is short (device indices; the
+	 * owner warp of each neuron applies it before the update), in place of
+	 * k_stimulus: firing stimulus inlineF[inlineNf], current stimulus
+	 * inlineI[inlineNi] with inlineCur (unique indices) */
+	uint32_t inlineNf;
+	uint32_t inlineNi;
+	uint32_t inlineF[INLINE_STIM_MAX];
+	uint32_t inlineI[INLINE_STIM_MAX];
+	float inlineCur[INLINE_STIM_MAX];
 	unsigned long long timeoutNs;        /* grid-barrier wait limit */
 	/* when set, the first cycle is read from here instead of firstCycle and
 	 * advanced by the launch (launches replayed from a CUDA graph) */

@@ -550,6 +550,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	m_args.timeoutNs = 10ull * 1000 * 1000 * 1000;
 
 	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords + 1) * 4));
+	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, size_t(m_net.nWords + 1) * 4, cudaHostAllocMapped));
+	NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dStepWords, m_stepWords, 0));
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	m_wallStart = std::chrono::steady_clock::now();
 }
@@ -560,6 +562,7 @@ Simulation::~Simulation()
 	destroyGraph();
 	for(void* p : m_allocs) cudaFree(p);
 	if(m_hWords) cudaFreeHost(m_hWords);
+	if(m_stepWords) cudaFreeHost(m_stepWords);
 	if(m_hStim) cudaFreeHost(m_hStim);
 	if(m_hCur) cudaFreeHost(m_hCur);
 	if(m_dStim) cudaFree(m_dStim);
@@ -595,12 +598,22 @@ Simulation::groupOfDev(uint32_t dev, uint32_t* i) const
 
 /* One persistent launch for cycles [first, first + cycles) */
 void
-Simulation::launchBlock(uint64_t first, unsigned cycles, uint32_t carry)
+Simulation::launchBlock(uint64_t first, unsigned cycles, uint32_t carry, bool globalAcc, uint32_t* hostWords,
+		const InlineStim* inl)
 {
 	CycleArgs a = m_args;
 	a.firstCycle = first;
 	a.cycles = cycles;
 	a.carry = carry;
+	a.globalAcc = globalAcc ? 1 : 0;
+	a.hostWords = hostWords;
+	if(inl) {
+		a.inlineNf = inl->nf;
+		a.inlineNi = inl->ni;
+		std::copy(inl->f, inl->f + inl->nf, a.inlineF);
+		std::copy(inl->i, inl->i + inl->ni, a.inlineI);
+		std::copy(inl->cur, inl->cur + inl->ni, a.inlineCur);
+	}
 	for(int gi = 0; gi < a.ngroups; ++gi) {
 		a.groups[gi].timerBase = uint32_t(m_timerBase);
 	}
@@ -680,7 +693,15 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 			}
 		}
 	}
-	if(nfOk + niOk) {
+	m_inline.nf = m_inline.ni = 0;
+	if(!err && nfOk <= INLINE_STIM_MAX && niOk <= INLINE_STIM_MAX) {
+		/* short: carried in the step kernel's parameters */
+		m_inline.nf = nfOk;
+		m_inline.ni = niOk;
+		std::copy(m_hStim, m_hStim + nfOk, m_inline.f);
+		std::copy(m_hStim + nfOk, m_hStim + nfOk + niOk, m_inline.i);
+		std::copy(m_hCur, m_hCur + niOk, m_inline.cur);
+	} else if(nfOk + niOk) {
 		NEMO_CUDA(cudaMemcpyAsync(m_dStim, m_hStim, size_t(nfOk + niOk) * 4, cudaMemcpyHostToDevice, stream));
 		if(niOk) NEMO_CUDA(cudaMemcpyAsync(m_dCur, m_hCur, size_t(niOk) * 4, cudaMemcpyHostToDevice, stream));
 		StimDev sd{m_dStim, nfOk, m_dStim + nfOk, m_dCur, niOk};
@@ -698,17 +719,17 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	notShard("step");
 	stageStimulus(fstim, nf, inidx, icur, ni, false);
 	cudaStream_t stream = STREAM(m_stream);
-	launchBlock(m_cycle, 1);
-	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
-	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
-				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, stream));
-	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	/* the kernel writes the firing bitmap and the error word into mapped
+	 * host memory: no copy after it */
+	launchStep();
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	NEMO_CUDA(cudaGetLastError());
-	checkDeviceError();
+	if(m_stepWords[m_net.nWords] != 0) {
+		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
+	}
 	m_cycle++;
 	m_stateDirty = true;
-	decodeFired(m_hWords, m_fired);
+	decodeFired(m_stepWords, m_fired);
 	return m_fired;
 }
 
@@ -747,7 +768,7 @@ Simulation::shardStep(const unsigned* fstim, size_t nf, const unsigned* inidx, c
 	}
 	stageStimulus(fstim, nf, inidx, icur, ni, true);
 	cudaStream_t stream = STREAM(m_stream);
-	launchBlock(m_cycle, 1, (m_pendingGather ? 1u : 0u) | 2u);
+	launchStep();
 	const uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
 	const uint32_t words = m_shard.warpHi - m_shard.warpLo;
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords + m_shard.warpLo,
@@ -759,7 +780,6 @@ Simulation::shardStep(const unsigned* fstim, size_t nf, const unsigned* inidx, c
 	std::memcpy(localWords, m_hWords, size_t(words) * 4);
 	m_cycle++;
 	m_stateDirty = true;
-	m_pendingGather = true;
 	m_awaitDeliver = true;
 }
 
@@ -785,16 +805,31 @@ Simulation::shardDeliver(const uint32_t* allWords)
 	return m_fired;
 }
 
-/* The pending gathering and learning of a shard's last cycle: one gather
- * phase (carry bit 0, no cycles). */
+/* One cycle as a single phase: the update of cycle m_cycle, overlapped with
+ * the gathering and learning of the cycle before when that is pending (carry
+ * bit 0); this cycle's own gathering waits (carry bit 1) for the next step or
+ * flushPending. Reading the firing never needs it: delivery only affects
+ * later cycles' currents and the STDP accumulators. */
 void
-Simulation::flushShard()
+Simulation::launchStep()
+{
+	m_stepWords[m_net.nWords] = 0u;
+	launchBlock(m_cycle, 1, (m_pendingGather ? 1u : 0u) | 2u, m_stepGlobalAcc, m_dStepWords, &m_inline);
+	m_inline.nf = m_inline.ni = 0;
+	m_pendingGather = true;
+}
+
+/* The pending gathering and learning of the last cycle: one gather phase
+ * (carry bit 0, no cycles). Before anything that reads the accumulators or
+ * launches the multi-cycle kernel. */
+void
+Simulation::flushPending()
 {
 	if(m_awaitDeliver) {
 		fail(NEMO_LOGIC_ERROR, "the last shard step's firing has not been delivered");
 	}
 	if(m_pendingGather) {
-		launchBlock(m_cycle, 0, 1u);
+		launchBlock(m_cycle, 0, 1u, m_stepGlobalAcc);
 		m_pendingGather = false;
 	}
 }
@@ -871,19 +906,17 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
 	}
 
-	launchBlock(m_cycle, 1);
-	uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
-	NEMO_CUDA(cudaMemcpyAsync(m_hWords, m_net.firedRing + size_t(slot) * m_net.nWords,
-				size_t(m_net.nWords) * 4, cudaMemcpyDeviceToHost, stream));
-	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
+	launchStep();
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	NEMO_CUDA(cudaGetLastError());
-	checkDeviceError();
+	if(m_stepWords[m_net.nWords] != 0) {
+		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
+	}
 	m_cycle++;
 	m_stateDirty = true;
 	size_t count = 0;
 	for(uint32_t w = 0; w < m_net.nWords; ++w) {
-		uint32_t bits = m_hWords[w];
+		uint32_t bits = m_stepWords[w];
 		while(bits) {
 			uint32_t b = uint32_t(__builtin_ctz(bits));
 			bits &= bits - 1;
@@ -897,6 +930,7 @@ void
 Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 {
 	notShard("run");
+	flushPending();
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
@@ -962,6 +996,7 @@ void
 Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
 {
 	notShard("runGraph");
+	flushPending();
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
@@ -1023,6 +1058,7 @@ unsigned
 Simulation::autotune(unsigned trialCycles, double ms[3])
 {
 	notShard("autotune");
+	flushPending();
 	if(trialCycles == 0 || trialCycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "autotune: trial cycles must be in 1.." + std::to_string(m_ring));
 	}
@@ -1101,9 +1137,7 @@ Simulation::applyStdp(float reward)
 		msg << "STDP reward rounded down to zero. The smallest valid reward is " << fixToFloat(1, m_fbits);
 		fail(NEMO_INVALID_INPUT, msg.str());
 	}
-	if(m_shardMode) {
-		flushShard();
-	}
+	flushPending();
 	if(m_nrcm) {
 		launchApply(fx);
 	}
@@ -1333,6 +1367,7 @@ void
 Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4])
 {
 	notShard("timedSteps");
+	flushPending();
 	if(cyclesPerStep == 0 || cyclesPerStep > m_ring) {
 		fail(NEMO_INVALID_INPUT, "timed steps: cycles per step must be in 1.." + std::to_string(m_ring));
 	}
@@ -1376,6 +1411,7 @@ void
 Simulation::profile(unsigned cycles, float reward, double out[10])
 {
 	notShard("profile");
+	flushPending();
 	cudaStream_t stream = STREAM(m_stream);
 	cudaEvent_t e0, e1, e2;
 	NEMO_CUDA(cudaEventCreate(&e0));
@@ -1419,6 +1455,7 @@ void
 Simulation::trace(unsigned cycles, double out[14])
 {
 	notShard("trace");
+	flushPending();
 	if(cycles == 0) {
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");
 	}

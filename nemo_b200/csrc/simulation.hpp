@@ -185,13 +185,22 @@ private:
 	Group& groupOfDev(uint32_t dev, uint32_t* i);
 	const Group& groupOfDev(uint32_t dev, uint32_t* i) const;
 	const Aux& aux(synapse_id id) const;
-	void launchBlock(uint64_t first, unsigned cycles, uint32_t carry = 0);
+	/* a step's short stimulus, staged by stageStimulus for the next launchStep */
+	struct InlineStim {
+		uint32_t nf = 0, ni = 0;
+		uint32_t f[INLINE_STIM_MAX];
+		uint32_t i[INLINE_STIM_MAX];
+		float cur[INLINE_STIM_MAX];
+	};
+	void launchBlock(uint64_t first, unsigned cycles, uint32_t carry = 0, bool globalAcc = false,
+			uint32_t* hostWords = nullptr, const InlineStim* inl = nullptr);
+	void launchStep();
 	void stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 			bool ownedOnly);
 	void notShard(const char* what) const;
 	void launchApply(int32_t reward);
 	bool owns(uint32_t dev) const { return dev / 32 >= m_shard.warpLo && dev / 32 < m_shard.warpHi; }
-	void flushShard();
+	void flushPending();
 	void checkDeviceError();
 	void syncStateToHost();
 	void* alloc(size_t bytes);
@@ -240,6 +249,9 @@ private:
 
 	/* pinned staging */
 	uint32_t* m_hWords;        /* one firing bitmap, then the barrier error word */
+	uint32_t* m_stepWords = nullptr;    /* mapped: a step's firing bitmap and error word */
+	InlineStim m_inline;
+	uint32_t* m_dStepWords = nullptr;   /* its device address */
 	uint32_t* m_hStim;         /* fstim + istim indices */
 	float* m_hCur;
 	uint32_t* m_dStim;
@@ -255,10 +267,15 @@ private:
 	std::vector<unsigned> m_batchFired;
 	std::vector<size_t> m_batchOffsets;
 
+	/* the last cycle's gathering and learning wait for the next step or a
+	 * flush (one-cycle steps and shard steps) */
+	bool m_pendingGather = false;
+	/* one-cycle steps run on the global current slots (CycleArgs::globalAcc) */
+	bool m_stepGlobalAcc = true;
+
 	/* sharded simulation */
 	bool m_shardMode = false;
 	ShardSpec m_shard;
-	bool m_pendingGather = false;   /* the last cycle's gathering and learning wait */
 	bool m_awaitDeliver = false;    /* the last cycle's remote firing has not come in */
 	uint32_t* m_dAllWords = nullptr;
 
