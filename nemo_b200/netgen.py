@@ -16,6 +16,10 @@ construction.
 * :func:`ring` — the reference's ring network (src/test/utils.cpp:132-155).
 * :func:`mixed_plugins` — Izhikevich / IF_curr_exp / QIF / HH populations.
 * :func:`batched_sizes` — instance sizes log-uniform in [lo, hi].
+
+A :class:`NetSpec` saves to one file and loads from it (:meth:`NetSpec.save`,
+:meth:`NetSpec.load`), so that a network is generated once and the same file
+is built by the B200 library and by the oracle.
 """
 
 from dataclasses import dataclass, field
@@ -51,6 +55,42 @@ class NetSpec:
     def out_degree(self):
         n = self.neuron_count
         return np.bincount(self.source, minlength=n) if self.source is not None else np.zeros(n, np.int64)
+
+    FORMAT = "nemo-b200-network-v1"
+
+    def save(self, path):
+        """Write the network to one file (numpy .npz: the neuron types in
+        registration order with their indices and per-argument arrays, then
+        the synapses in insertion order), so that every implementation of the
+        C ABI -- the B200 library and the oracle -- builds it from the same
+        file."""
+        arrays = {"format": np.array(self.FORMAT), "types": np.array([p.type_name for p in self.populations])}
+        for k, p in enumerate(self.populations):
+            arrays["idx_%d" % k] = np.asarray(p.idx, np.uint32)
+            arrays["args_%d" % k] = (np.stack([np.asarray(a, np.float32) for a in p.args])
+                                     if p.args else np.zeros((0, p.idx.size), np.float32))
+        if self.synapse_count:
+            arrays.update(source=np.asarray(self.source, np.uint32), target=np.asarray(self.target, np.uint32),
+                          delay=np.asarray(self.delay, np.uint32), weight=np.asarray(self.weight, np.float32),
+                          plastic=np.asarray(self.plastic, np.uint8))
+        with open(path, "wb") as f:
+            np.savez(f, **arrays)
+
+    @classmethod
+    def load(cls, path):
+        """The network a :meth:`save` wrote."""
+        with np.load(path, allow_pickle=False) as z:
+            if "format" not in z.files or str(z["format"]) != cls.FORMAT:
+                raise ValueError("%s is not a %s file" % (path, cls.FORMAT))
+            pops = []
+            for k, name in enumerate(z["types"]):
+                args = z["args_%d" % k]
+                pops.append(Population(str(name), z["idx_%d" % k].copy(), [a.copy() for a in args]))
+            spec = cls(pops)
+            if "source" in z.files:
+                spec.source, spec.target = z["source"].copy(), z["target"].copy()
+                spec.delay, spec.weight, spec.plastic = z["delay"].copy(), z["weight"].copy(), z["plastic"].copy()
+            return spec
 
     def build(self, net):
         """Add the neurons and synapses to a nemo.Network (any library)."""

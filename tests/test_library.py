@@ -61,6 +61,32 @@ def test_network_construction_matches_oracle(oracle_lib):
     assert a.get_neuron_state(150, 0) == b.get_neuron_state(150, 0)
 
 
+def test_network_file_round_trip(tmp_path, oracle_lib):
+    """A generated network written to one file and read back is the same
+    network, and both libraries build identical networks from the file."""
+    spec = netgen.mixed_plugins(n_iz=120, n_lif=80, n_qif=40, n_hh=9, m=20, dmax=10, seed=3)
+    path = tmp_path / "net.npz"
+    spec.save(path)
+    back = netgen.NetSpec.load(path)
+    assert [p.type_name for p in back.populations] == [p.type_name for p in spec.populations]
+    for p, q in zip(spec.populations, back.populations):
+        assert np.array_equal(p.idx, q.idx)
+        assert all(np.array_equal(np.asarray(a, np.float32), b) for a, b in zip(p.args, q.args))
+    for k in ("source", "target", "delay", "weight", "plastic"):
+        assert np.array_equal(getattr(spec, k), getattr(back, k))
+    a, b = back.build(Network(Library())), back.build(Network(oracle_lib))
+    assert a.neuron_count() == b.neuron_count() == spec.neuron_count
+    for src in (0, 100, 230):
+        ids = a.get_synapses_from(src)
+        assert list(ids) == list(b.get_synapses_from(src))
+        for sid in ids:
+            assert a.get_synapse_weight(sid) == b.get_synapse_weight(sid)
+    bad = tmp_path / "other.npz"
+    np.savez(bad, x=np.zeros(3))
+    with pytest.raises(ValueError):
+        netgen.NetSpec.load(bad)
+
+
 @pytest.mark.parametrize("which", ["b200", "oracle"])
 def test_network_errors(which, oracle_lib):
     lib = Library() if which == "b200" else oracle_lib
