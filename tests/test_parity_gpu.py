@@ -281,3 +281,65 @@ def test_every_event_delivered_once(dmax):
     fired, events, delivered = out[1], out[2], out[3]
     assert fired > 0
     assert delivered == events
+
+
+def test_steps_runs_and_applies_interleaved(oracle_lib):
+    """One-phase nemo_step calls (each leaves its cycle's gathering for the
+    next call), with short stimulus carried in the kernel parameters --
+    current stimulus on Hodgkin-Huxley neurons included -- interleaved with
+    device-resident runs, allocation-free steps and applyStdp, which flush
+    the pending gathering first: firing and weights identical to the
+    oracle's every cycle."""
+    f32 = np.float32
+    spec = netgen.mixed_plugins(n_iz=600, n_lif=300, n_qif=200, n_hh=40, m=50, dmax=12, seed=11)
+    spec.plastic = (spec.source < 480).astype(np.uint8)   # excitatory Izhikevich sources
+    n = spec.neuron_count
+    pre, post = netgen.standard_stdp()
+    (_, g), (_, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 1.0, 0.0, -1.0)))
+    lib = g.lib
+    P = ctypes.POINTER
+    lib.dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    lib.dll.nemo_b200_fired_at.argtypes = [ctypes.c_void_p, ctypes.c_uint64, P(P(ctypes.c_uint)), P(ctypes.c_size_t)]
+    lib.dll.nemo_b200_step_noalloc.argtypes = [ctypes.c_void_p, P(ctypes.c_uint), ctypes.c_size_t, P(ctypes.c_uint),
+                                               P(ctypes.c_float), ctypes.c_size_t, P(ctypes.c_uint), ctypes.c_size_t,
+                                               P(ctypes.c_size_t)]
+    rng = np.random.default_rng(7)
+    hh = spec.populations[-1].idx
+    cycle = 0
+
+    def stimulus():
+        fstim = np.sort(rng.choice(n, size=int(rng.integers(0, 8)), replace=False)).astype(np.uint32)
+        ii = np.concatenate([rng.choice(hh, size=4, replace=False), rng.choice(n, size=6, replace=False)])
+        return fstim, [(int(i), float(rng.uniform(5, 30))) for i in np.unique(ii)]
+
+    out = np.zeros(n, np.uint32)
+    cnt = ctypes.c_size_t()
+    for rnd in range(3):
+        for _ in range(40):
+            fstim, istim = stimulus()
+            assert np.array_equal(g.step(fstim=fstim, istim=istim), o.step(fstim=fstim, istim=istim)), cycle
+            cycle += 1
+        for _ in range(10):
+            fstim, istim = stimulus()
+            inidx = np.array([p[0] for p in istim], np.uint32)
+            icur = np.array([p[1] for p in istim], np.float32)
+            lib.call("nemo_b200_step_noalloc", g.handle, fstim.ctypes.data_as(P(ctypes.c_uint)), fstim.size,
+                     inidx.ctypes.data_as(P(ctypes.c_uint)), icur.ctypes.data_as(P(ctypes.c_float)), inidx.size,
+                     out.ctypes.data_as(P(ctypes.c_uint)), out.size, ctypes.byref(cnt))
+            assert np.array_equal(out[:cnt.value], o.step(fstim=fstim, istim=istim)), cycle
+            cycle += 1
+        chunk = 30
+        lib.call("nemo_b200_run", g.handle, chunk, None, None)
+        for k in range(chunk):
+            ref = o.step()
+            ptr = P(ctypes.c_uint)()
+            c2 = ctypes.c_size_t()
+            lib.call("nemo_b200_fired_at", g.handle, cycle + k, ctypes.byref(ptr), ctypes.byref(c2))
+            got = np.ctypeslib.as_array(ptr, shape=(c2.value,)).copy() if c2.value else np.zeros(0, np.uint32)
+            assert np.array_equal(got, ref), cycle + k
+        cycle += chunk
+        g.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+    for src in range(0, 480, 9):
+        for sid in g.get_synapses_from(src):
+            assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid), (src, sid)
