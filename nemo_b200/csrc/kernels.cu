@@ -1096,18 +1096,17 @@ k_stimulus_scratch(NetDev net, const uint32_t* scratch, uint32_t nf, uint32_t ni
  * source's firing history after the last completed cycle (cycleNow - 1):
  * bit k fired at cycleNow-1-k and arrives at cycleNow-1-k+d. */
 __device__ __forceinline__ void applyOne(const NetDev& net, const StdpRule& rule, int32_t reward, uint64_t cycleNow,
-		const uint64_t* rfNow, uint32_t j, uint32_t f, int32_t acc, uint2 syn, uint32_t sd)
+		const uint64_t* rfNow, uint32_t j, uint32_t f, int32_t acc, int32_t wOld, uint32_t target, uint32_t sd)
 {
-	const int32_t wOld = int32_t(syn.y);
 	const int32_t diff = int32_t((int64_t(reward) * int64_t(acc)) >> net.fbits);
 	const int32_t wNew = updatedWeight(wOld, diff, rule);
 	if(wNew != wOld) {
 		net.fcm[f].y = uint32_t(wNew);
+		__stcs(&net.rcmWeight[j], wNew);
 		if(net.deliver) {
 			const uint32_t d = (sd & 63u) + 1u;
 			uint64_t pending = rfNow[sd >> 6] & ((uint64_t(1) << d) - 1u);
 			if(pending) {
-				const uint32_t target = syn.x >> 6;
 				const long long delta = (long long) wNew - (long long) wOld;
 				const int half = wOld >= 0 ? 0 : 1;
 				while(pending) {
@@ -1153,33 +1152,30 @@ k_apply_stdp(NetDev net, StdpRule rule, int32_t reward, uint64_t cycleNow, uint3
 		const uint32_t e = net.rcmStart[t + 1];
 		if(b0 >= e) continue;
 		const uint32_t j = b0 + lane;
-		/* the forward indices are loaded with the accumulators (one round
-		 * trip); only the forward records wait for the accumulator test */
+		/* the accumulators first; a synapse that changes (live) then loads
+		 * its forward index, its weight (the reverse-order copy) and its
+		 * source word together, all coalesced: no forward record is read */
 		int32_t a[APPLY_PER_LANE];
-		uint32_t f[APPLY_PER_LANE];
 		bool live[APPLY_PER_LANE];
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
 			const uint32_t jj = j + 32u * u;
 			a[u] = jj < e ? __ldcs(&net.rcmAcc[jj]) : 0;
-			f[u] = jj < e ? __ldcs(&net.rcmForward[jj]) : 0u;
+			live[u] = jj < e && (a[u] != 0 || !skipZero);
 		}
-#pragma unroll
-		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			live[u] = j + 32u * u < e && (a[u] != 0 || !skipZero);
-		}
-		/* the source words (for the in-flight correction of a changed
-		 * weight) come with the forward records */
-		uint2 syn[APPLY_PER_LANE];
+		uint32_t f[APPLY_PER_LANE];
+		int32_t w[APPLY_PER_LANE];
 		uint32_t sd[APPLY_PER_LANE];
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			syn[u] = live[u] ? net.fcm[f[u]] : make_uint2(0u, 0u);
-			sd[u] = live[u] && net.deliver ? __ldcs(&net.rcmSrcDelay[j + 32u * u]) : 0u;
+			const uint32_t jj = j + 32u * u;
+			f[u] = live[u] ? __ldcs(&net.rcmForward[jj]) : 0u;
+			w[u] = live[u] ? __ldcs(&net.rcmWeight[jj]) : 0;
+			sd[u] = live[u] && net.deliver ? __ldcs(&net.rcmSrcDelay[jj]) : 0u;
 		}
 #pragma unroll
 		for(int u = 0; u < int(APPLY_PER_LANE); ++u) {
-			if(live[u]) applyOne(net, rule, reward, cycleNow, rfNow, j + 32u * u, f[u], a[u], syn[u], sd[u]);
+			if(live[u]) applyOne(net, rule, reward, cycleNow, rfNow, j + 32u * u, f[u], a[u], w[u], t, sd[u]);
 		}
 	}
 }

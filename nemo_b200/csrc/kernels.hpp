@@ -124,6 +124,9 @@ struct NetDev {
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
 	const uint32_t* rcmForward;    /* index into fcm, ascending within a target */
 	int32_t* rcmAcc;
+	/* the plastic weights in reverse order, a copy of the forward records'
+	 * weights that applyStdp reads (coalesced) and writes with them */
+	int32_t* rcmWeight;
 
 	/* glibc-matching correction tables (libm_match.cuh) */
 	const uint32_t* sinTab;

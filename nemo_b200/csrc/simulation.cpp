@@ -366,6 +366,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
 	std::vector<uint32_t> rcmStart;
 	std::vector<uint32_t> rcmSrcDelay, rcmForward;
+	std::vector<int32_t> rcmWeight;
 	uint64_t maxIn = 0;
 	if(m_stdpOn) {
 		rcmStart.assign(size_t(m_nDev) + 1, 0);
@@ -377,6 +378,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		m_nrcm = rcmStart[m_nDev];
 		rcmSrcDelay.resize(m_nrcm);
 		rcmForward.resize(m_nrcm);
+		rcmWeight.resize(m_nrcm);
 		/* filled in forward order, so each target's synapses are sorted by
 		 * their position in the forward matrix */
 		std::vector<uint32_t> fill(rcmStart.begin(), rcmStart.end() - 1);
@@ -386,6 +388,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 			uint32_t j = fill[dtgt[s]]++;
 			rcmSrcDelay[j] = (dsrc[s] << 6) | (net.dly[s] - 1);
 			rcmForward[j] = uint32_t(pos);
+			rcmWeight[j] = wfx[s];
 		}
 	}
 	/* STDP work items (32 x STDP_PER_LANE synapses) per post-spiking target */
@@ -469,6 +472,7 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		m_net.rcmStart = (const uint32_t*) put(rcmStart.data(), rcmStart.size() * 4);
 		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
 		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
+		m_net.rcmWeight = (int32_t*) put(rcmWeight.data(), rcmWeight.size() * 4);
 		m_net.rcmAcc = (int32_t*) alloc(size_t(m_nrcm) * 4);
 	}
 
