@@ -59,6 +59,15 @@ def workload(small=False):
     return dict(name="izhikevich-100k-m1000-stdp", n=100000, m=1000, dmax=20, seed=1)
 
 
+def bench_config(wl, world):
+    """The workload description both arms (B200 and reference) report."""
+    n, m = wl["n"], wl["m"]
+    return {"workload": wl["name"], "neurons": n, "synapses_per_neuron": m, "synapses": n * m,
+            "delays": "U{1..%d}" % wl["dmax"], "stdp": "exc plastic, applyStdp(1.0) every 100 cycles",
+            "cycles_per_step": CYCLES_PER_STEP, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (800 MB forward matrix)"}
+
+
 def build_sim(lib, wl, oracle=False):
     spec = netgen.izhikevich_random(wl["n"], wl["m"], dmax=wl["dmax"], seed=wl["seed"], stdp=True)
     net = spec.build(Network(lib))
@@ -348,10 +357,7 @@ def run_b200(args):
         "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32/int64 fixed point + f32/f64 state",
         "data": "synthetic (seeded generator, numpy PCG64 seed %d)" % wl["seed"],
-        "config": {"workload": wl["name"], "neurons": n, "synapses_per_neuron": m, "synapses": n * m,
-                   "delays": "U{1..%d}" % wl["dmax"], "stdp": "exc plastic, applyStdp(1.0) every 100 cycles",
-                   "cycles_per_step": CYCLES_PER_STEP, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (800 MB forward matrix)"},
+        "config": bench_config(wl, world),
         "sim_ms_per_wall_s": round(CYCLES_PER_STEP * args.steps / (ms_max * 1e-3), 1),
         "fired_per_cycle": round(fired / (CYCLES_PER_STEP * args.steps), 1),
         "delivered_synapses": int(delivered), "build_s": round(t_build, 2),
@@ -390,8 +396,7 @@ def run_reference(args):
         "steps": nsteps, "warmup": args.warmup, "ms_per_step": round(secs * 1000 / nsteps, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/int64 fixed point + f32/f64 state", "data": "synthetic (seeded generator)",
-        "config": {"workload": wl["name"], "neurons": n, "synapses_per_neuron": wl["m"],
-                   "cycles_per_step": CYCLES_PER_STEP},
+        "config": bench_config(wl, 1),
         "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                          "sample": "%d step(s) of 100 cycles + applyStdp after %d warm-up step(s)"
                                    % (nsteps, args.warmup)},
