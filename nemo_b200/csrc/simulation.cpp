@@ -249,10 +249,6 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	 * revolution later can be added */
 	const uint32_t slots = deliver ? m_maxDelay + 1 : 1;
 
-	/* int32 accumulators are exact when no slot can leave the int32 range:
-	 * a slot of target t only ever holds at most one arrival per incoming
-	 * synapse, so it is bounded by the sum of its in-weights, taking each
-	 * plastic weight at its STDP limit if that is larger */
 	/* src/nemo/StdpProcess.cpp:129-137: a weight updatedWeight leaves alone
 	 * when the change is 0 */
 	if(m_stdpOn) {
@@ -264,6 +260,10 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 			else if(w < 0) m_weightsInRange = w >= m_rule.maxI && w <= m_rule.minI;
 		}
 	}
+	/* int32 accumulators are exact when no slot can leave the int32 range:
+	 * a slot of target t only ever holds at most one arrival per incoming
+	 * synapse, so it is bounded by the sum of its in-weights, taking each
+	 * plastic weight at its STDP limit if that is larger */
 	bool acc32 = true;
 	{
 		std::vector<int64_t> pos(m_nDev, 0), neg(m_nDev, 0);
