@@ -37,6 +37,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -65,7 +66,7 @@ def bench_config(wl, world):
     return {"workload": wl["name"], "neurons": n, "synapses_per_neuron": m, "synapses": n * m,
             "delays": "U{1..%d}" % wl["dmax"], "stdp": "exc plastic, applyStdp(1.0) every 100 cycles",
             "cycles_per_step": CYCLES_PER_STEP, "parallelism": "replicas" if world > 1 else "single",
-            "l2": "inputs larger than L2 (800 MB forward matrix)"}
+            "l2": "inputs larger than L2 (%d MB forward matrix)" % (n * m * 8 // 10**6)}
 
 
 def build_sim(lib, wl, oracle=False):
@@ -145,7 +146,9 @@ def oracle_library():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region,
+    into a temporary file (or the file NEMO_B200_CLOCKS_CSV names, which is
+    kept)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -154,7 +157,12 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench.csv")
+        self.keep = bool(os.environ.get("NEMO_B200_CLOCKS_CSV"))
+        if self.keep:
+            self.path = os.path.abspath(os.environ["NEMO_B200_CLOCKS_CSV"])
+        else:
+            fd, self.path = tempfile.mkstemp(prefix="nemo_b200_clocks_", suffix=".csv")
+            os.close(fd)
 
     def __enter__(self):
         try:
@@ -185,8 +193,15 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
-        if self.proc is None or not os.path.exists(self.path):
-            return None
+        try:
+            if self.proc is None or not os.path.exists(self.path):
+                return None
+            return self._summary()
+        finally:
+            if not self.keep and os.path.exists(self.path):
+                os.unlink(self.path)
+
+    def _summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
