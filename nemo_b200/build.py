@@ -85,6 +85,29 @@ def build(verbose=False, clean=False):
     return LIB
 
 
+def build_plugin(src, name=None, plugin_dir=None, extra_flags=()):
+    """Compile a GPU neuron-model plugin (include/nemo_b200_plugin.h) from the
+    CUDA source `src` into <plugin_dir>/b200/lib<name>.so, the place the
+    library looks for it beside <name>.ini (name: the source's base name;
+    plugin_dir: the source's directory). Rebuilt only when the source or the
+    plugin header is newer. Returns the library's path."""
+    name = name or os.path.splitext(os.path.basename(src))[0]
+    plugin_dir = plugin_dir or os.path.dirname(os.path.abspath(src))
+    out = os.path.join(plugin_dir, "b200", "lib%s.so" % name)
+    header = os.path.join(ROOT, "include", "nemo_b200_plugin.h")
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(src), os.path.getmtime(header)):
+        return out
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-fmad=false", "-shared", "-Xcompiler", "-fPIC", "-ccbin", CXX,
+                           "-I" + os.path.join(ROOT, "include"), "-Xlinker", "--exclude-libs,ALL",
+                           *extra_flags, src, "-o", out + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("building plugin %s failed:\n%s%s" % (src, r.stdout, r.stderr))
+    os.replace(out + ".tmp", out)
+    return out
+
+
 def prepare_tables():
     """Write the glibc correction-table cache next to the library."""
     import ctypes

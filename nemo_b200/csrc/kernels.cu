@@ -780,6 +780,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
 						case 2: fired = modelQif(net, G, i, n, E, I, stim); break;
 						case 4: fired = modelPoisson(net, G, i, n, E, I, stim); break;
+						case 6:
+							/* a plugin model: its firing, stimulus included,
+							 * from the bits its update wrote for this cycle */
+							fired = (__ldg(&G.extFired[i >> 5]) >> (i & 31u)) & 1u;
+							break;
 						default: fired = modelInput(net, G, i, n, E, I, stim); break;
 					}
 				}
@@ -1036,6 +1041,30 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	if(A.cycleCounter && b == 0 && tid == 0) {
 		*A.cycleCounter = first + A.cycles;
 	}
+}
+
+/* The currents of one cycle of a plugin model's neurons: slot plus inbox,
+ * summed as the update sums them, saturated and converted (wfxToFloat). */
+__global__ void
+k_export_currents(NetDev net, uint32_t devBase, uint32_t count, uint32_t slot, uint32_t par, float* E, float* I)
+{
+	const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i >= count) return;
+	const size_t n = size_t(devBase) + i;
+	long long e, in;
+	if(net.acc32) {
+		const int2 a = reinterpret_cast<const int2*>(net.acc)[size_t(slot) * net.nDev + n];
+		const int2 b = reinterpret_cast<const int2*>(net.inbox)[size_t(par) * net.nDev + n];
+		e = (long long) b.x + a.x;
+		in = (long long) b.y + a.y;
+	} else {
+		const longlong2 a = reinterpret_cast<const longlong2*>(net.acc)[size_t(slot) * net.nDev + n];
+		const longlong2 b = reinterpret_cast<const longlong2*>(net.inbox)[size_t(par) * net.nDev + n];
+		e = b.x + a.x;
+		in = b.y + a.y;
+	}
+	E[i] = wfxToFloat(e, net.fbits);
+	I[i] = wfxToFloat(in, net.fbits);
 }
 
 /* Firing and current stimulus of this cycle (src/nemo/cpu/Simulation.cpp:
@@ -1468,6 +1497,15 @@ launchShardInject(const NetDev& net, uint64_t t, const uint32_t* allWords, uint3
 	const uint32_t warps = net.nWords;
 	const uint32_t blocks = std::max<uint32_t>(1u, std::min<uint32_t>((warps + 7u) / 8u, uint32_t(smCount()) * 8u));
 	k_shard_inject<<<blocks, 256, 0, S(stream)>>>(net, t, allWords, ownLo, ownHi);
+}
+
+void
+launchExportCurrents(const NetDev& net, uint32_t devBase, uint32_t count, uint64_t cycle, float* E, float* I,
+		void* stream)
+{
+	if(count == 0) return;
+	k_export_currents<<<(count + 255) / 256, 256, 0, S(stream)>>>(net, devBase, count,
+			uint32_t(cycle % net.slots), uint32_t(cycle) & 1u, E, I);
 }
 
 void

@@ -164,6 +164,9 @@ struct GroupDev {
 	uint32_t shift;         /* neuron i at device index devBase + (i << shift):
 	                         * HH neurons take 8 lanes each (shift 3), the
 	                         * other models one */
+	const uint32_t* extFired;  /* a plugin model's firing bits of the cycle
+	                            * (bit i % 32 of word i / 32), written by the
+	                            * plugin before the update; null otherwise */
 };
 
 /* The STDP rule in fixed point (src/nemo/StdpProcess.cpp:20-46) */
@@ -276,6 +279,13 @@ void launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, vo
 /* sharded simulation: the remote firing of cycle t (k_shard_inject) */
 void launchShardInject(const NetDev& net, uint64_t t, const uint32_t* allWords, uint32_t ownLo, uint32_t ownHi,
 		void* stream);
+/* The currents of cycle `cycle` of device neurons devBase .. devBase +
+ * count - 1 (their current slot plus their delay-1 inbox, saturated and
+ * converted), into E[count] and I[count], for a plugin model; not cleared
+ * (the cycle's update clears them). */
+void launchExportCurrents(const NetDev& net, uint32_t devBase, uint32_t count, uint64_t cycle, float* E, float* I,
+		void* stream);
+
 /* counts of mismatches [3] (zeroed by the caller) of the HH constant divisions */
 void launchHhDivCheck(unsigned long long* bad, void* stream);
 int smCount();

@@ -181,6 +181,15 @@ loadNeuronType(const std::string& name)
 	t.history = h == kv.end() ? 1 : parseUnsigned(h->second, "history", file);
 	t.pluginDir = file.substr(0, file.rfind('/'));
 	t.kind = modelKind(name);
+	if(t.kind == MODEL_COUNT) {
+		/* not a built-in model: a GPU plugin beside the .ini, as the
+		 * reference keeps lib<name>.so in <dir>/{cpu,cuda}/ */
+		const std::string lib = t.pluginDir + "/b200/lib" + name + ".so";
+		if(isFile(lib)) {
+			t.kind = MODEL_EXTERNAL;
+			t.b200Plugin = lib;
+		}
+	}
 	return t;
 }
 

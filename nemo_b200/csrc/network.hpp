@@ -29,6 +29,7 @@ enum ModelKind {
 	MODEL_HH,
 	MODEL_POISSON_SOURCE,
 	MODEL_INPUT,
+	MODEL_EXTERNAL,   /* a plugin's kernels (nemo_b200_plugin.h) */
 	MODEL_COUNT
 };
 
@@ -44,6 +45,7 @@ struct NeuronType {
 	bool backendCpu = false, backendCuda = false;
 	std::string pluginDir;
 	ModelKind kind = MODEL_COUNT;
+	std::string b200Plugin;   /* MODEL_EXTERNAL: <pluginDir>/b200/lib<name>.so */
 };
 
 void addPluginPath(const std::string& dir);

@@ -1,0 +1,27 @@
+#ifndef NEMO_B200_PLUGIN_HPP
+#define NEMO_B200_PLUGIN_HPP
+
+/* Loading of GPU neuron-model plugins (include/nemo_b200_plugin.h): the
+ * role of the reference's plugin loader (src/nemo/Plugin.cpp,
+ * src/nemo/cpu/Neurons.cpp:19-20), for the B200 backend's signature. */
+
+#include <string>
+
+#include <nemo_b200_plugin.h>
+
+namespace nemo_b200 {
+
+struct B200Plugin {
+	std::string path;
+	b200_update_neurons_t* update = nullptr;
+	b200_init_neurons_t* init = nullptr;   /* optional */
+};
+
+/* The plugin at `path`, opened once per process and kept open. Fails with
+ * NEMO_DL_ERROR when it cannot be opened and NEMO_INVALID_INPUT when it does
+ * not export b200_update_neurons. */
+const B200Plugin& loadB200Plugin(const std::string& path);
+
+} // namespace nemo_b200
+
+#endif

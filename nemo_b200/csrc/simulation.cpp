@@ -111,10 +111,19 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		uint32_t n = uint32_t(ng.gidx.size());
 		if(n == 0) continue;
 		if(ng.type.kind == MODEL_COUNT) {
-			fail(NEMO_API_UNSUPPORTED, "The B200 backend has no kernel for neuron model " + ng.type.name);
+			fail(NEMO_API_UNSUPPORTED, "The B200 backend has no kernel for neuron model " + ng.type.name
+					+ " (a plugin model needs b200/lib" + ng.type.name + ".so beside its .ini)");
 		}
 		Group g;
 		g.type = ng.type;
+		if(ng.type.kind == MODEL_EXTERNAL) {
+			if(shard) {
+				fail(NEMO_API_UNSUPPORTED, "Shard: neuron model " + ng.type.name
+						+ " is a plugin model; sharded simulations run built-in models only");
+			}
+			g.plugin = &loadB200Plugin(ng.type.b200Plugin);
+			m_external = true;
+		}
 		g.localBase = local;
 		g.devBase = devPos;
 		g.count = n;
@@ -520,6 +529,11 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 		}
 		g.dRng = (uint4*) put(seeds.data(), seeds.size() * 16);
 		needTables = needTables || g.type.kind == MODEL_IZHIKEVICH;
+		if(g.plugin) {
+			g.dExtE = (float*) alloc(size_t(g.count) * 4);
+			g.dExtI = (float*) alloc(size_t(g.count) * 4);
+			g.dExtFired = (uint32_t*) alloc(size_t((g.count + 31) / 32) * 4);
+		}
 	}
 	bool needExp = false;
 	for(const Group& g : m_groups) needExp = needExp || g.type.kind == MODEL_HH;
@@ -547,7 +561,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	m_args.groupWarp[0] = 0;
 	for(size_t gi = 0; gi < m_groups.size(); ++gi) {
 		const Group& g = m_groups[gi];
-		m_args.groups[gi] = GroupDev{g.devBase, g.count, 0u, int(g.type.kind), g.dParam, g.dState, g.dRng, g.shift};
+		m_args.groups[gi] = GroupDev{g.devBase, g.count, 0u, int(g.type.kind), g.dParam, g.dState, g.dRng, g.shift,
+			g.dExtFired};
 		m_args.groupWarp[gi + 1] = m_args.groupWarp[gi] + uint32_t(((uint64_t(g.count) << g.shift) + 31) / 32);
 	}
 	/* a grid barrier that waits this long has lost a block: give up */
@@ -556,6 +571,22 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords + 1) * 4));
 	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, size_t(m_net.nWords + 1) * 4, cudaHostAllocMapped));
 	NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dStepWords, m_stepWords, 0));
+	/* plugin models derive their initial state (b200_init_neurons) */
+	for(const Group& g : m_groups) {
+		if(g.plugin && g.plugin->init) {
+			b200_neuron_batch b;
+			pluginBatch(g, &b);
+			b.cycle = 0;
+			b.current_epsp = b.current_ipsp = nullptr;
+			b.fstim = nullptr;
+			b.fired = nullptr;
+			const int rc = g.plugin->init(&b, m_stream);
+			if(rc != 0) {
+				fail(NEMO_CUDA_INVOCATION_ERROR, "Neuron model plugin " + g.plugin->path + ": b200_init_neurons: "
+						+ cudaGetErrorString(cudaError_t(rc)));
+			}
+		}
+	}
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	m_wallStart = std::chrono::steady_clock::now();
 }
@@ -698,7 +729,7 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 		}
 	}
 	m_inline.nf = m_inline.ni = 0;
-	if(!err && nfOk <= INLINE_STIM_MAX && niOk <= INLINE_STIM_MAX) {
+	if(!err && !m_external && nfOk <= INLINE_STIM_MAX && niOk <= INLINE_STIM_MAX) {
 		/* short: carried in the step kernel's parameters */
 		m_inline.nf = nfOk;
 		m_inline.ni = niOk;
@@ -722,6 +753,7 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 {
 	notShard("step");
 	stageStimulus(fstim, nf, inidx, icur, ni, false);
+	if(m_external) runPlugins();
 	cudaStream_t stream = STREAM(m_stream);
 	/* the kernel writes the firing bitmap and the error word into mapped
 	 * host memory: no copy after it */
@@ -745,6 +777,58 @@ Simulation::launchApply(int32_t reward)
 	launchApplyStdp(m_net, m_rule, reward, m_cycle, m_applyGroups.data(), uint32_t(m_applyGroups.size() - 1),
 			m_weightsInRange, m_stream);
 	m_weightsInRange = true;
+}
+
+/* The batch of a plugin population for the cycle about to run
+ * (nemo_b200_plugin.h): the current of the cycle, the stimulus staged for
+ * it, the firing history before it. */
+void
+Simulation::pluginBatch(const Group& g, b200_neuron_batch* b) const
+{
+	b->count = g.count;
+	b->cycle = (unsigned long long) (m_cycle - m_timerBase);
+	b->param = g.dParam;
+	b->param_stride = g.count;
+	b->state = g.dState;
+	b->state_stride = g.count;
+	b->current_epsp = g.dExtE;
+	b->current_ipsp = g.dExtI;
+	b->current_external = m_net.ext + g.devBase;
+	b->fstim = m_net.fstim + g.devBase / 32;
+	b->recent_firing = m_net.rf + size_t(m_cycle & 1u) * m_nDev + g.devBase;
+	b->fired = g.dExtFired;
+	b->rng = reinterpret_cast<uint32_t*>(g.dRng);
+}
+
+/* Each plugin population's update for the cycle about to run, on the
+ * simulation's stream: its currents of the cycle are complete once the
+ * previous step has run (its delay-1 arrivals are in the slot; the pending
+ * gathering only reaches later cycles), so they are exported, the plugin
+ * writes the firing bits, and the step launch that follows reads them. */
+void
+Simulation::runPlugins()
+{
+	for(const Group& g : m_groups) {
+		if(!g.plugin) continue;
+		launchExportCurrents(m_net, g.devBase, g.count, m_cycle, g.dExtE, g.dExtI, m_stream);
+		NEMO_CUDA(cudaGetLastError());
+		b200_neuron_batch b;
+		pluginBatch(g, &b);
+		const int rc = g.plugin->update(&b, m_stream);
+		if(rc != 0) {
+			fail(NEMO_CUDA_INVOCATION_ERROR, "Neuron model plugin " + g.plugin->path + ": b200_update_neurons: "
+					+ cudaGetErrorString(cudaError_t(rc)));
+		}
+	}
+}
+
+void
+Simulation::notExternal(const char* what) const
+{
+	if(m_external) {
+		fail(NEMO_API_UNSUPPORTED, std::string(what) + ": the network has plugin neuron models, whose updates "
+				"run cycle by cycle; step the simulation with nemo_step");
+	}
 }
 
 void
@@ -909,6 +993,7 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 		NEMO_CUDA(cudaStreamSynchronize(stream));
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(badIdx));
 	}
+	if(m_external) runPlugins();
 
 	launchStep();
 	NEMO_CUDA(cudaStreamSynchronize(stream));
@@ -934,6 +1019,7 @@ void
 Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 {
 	notShard("run");
+	notExternal("run");
 	flushPending();
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
@@ -1000,6 +1086,7 @@ void
 Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
 {
 	notShard("runGraph");
+	notExternal("runGraph");
 	flushPending();
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
@@ -1062,6 +1149,7 @@ unsigned
 Simulation::autotune(unsigned trialCycles, double ms[3])
 {
 	notShard("autotune");
+	notExternal("autotune");
 	flushPending();
 	if(trialCycles == 0 || trialCycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "autotune: trial cycles must be in 1.." + std::to_string(m_ring));
@@ -1371,6 +1459,7 @@ void
 Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float reward, double out[4])
 {
 	notShard("timedSteps");
+	notExternal("timedSteps");
 	flushPending();
 	if(cyclesPerStep == 0 || cyclesPerStep > m_ring) {
 		fail(NEMO_INVALID_INPUT, "timed steps: cycles per step must be in 1.." + std::to_string(m_ring));
@@ -1415,6 +1504,7 @@ void
 Simulation::profile(unsigned cycles, float reward, double out[10])
 {
 	notShard("profile");
+	notExternal("profile");
 	flushPending();
 	cudaStream_t stream = STREAM(m_stream);
 	cudaEvent_t e0, e1, e2;
@@ -1459,6 +1549,7 @@ void
 Simulation::trace(unsigned cycles, double out[14])
 {
 	notShard("trace");
+	notExternal("trace");
 	flushPending();
 	if(cycles == 0) {
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");

@@ -13,6 +13,7 @@
 
 #include "kernels.hpp"
 #include "network.hpp"
+#include "plugin.hpp"
 
 namespace nemo_b200 {
 
@@ -172,6 +173,12 @@ private:
 		float* dParam = nullptr;
 		float* dState = nullptr;
 		uint4* dRng = nullptr;
+		/* a plugin model (MODEL_EXTERNAL): its update, the currents it is
+		 * given and the firing bits it writes, per cycle */
+		const B200Plugin* plugin = nullptr;
+		float* dExtE = nullptr;
+		float* dExtI = nullptr;
+		uint32_t* dExtFired = nullptr;
 	};
 
 	struct Aux {            /* per synapse, in per-source id order */
@@ -198,6 +205,9 @@ private:
 	void stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 			bool ownedOnly);
 	void notShard(const char* what) const;
+	void notExternal(const char* what) const;
+	void runPlugins();
+	void pluginBatch(const Group& g, b200_neuron_batch* b) const;
 	void launchApply(int32_t reward);
 	bool owns(uint32_t dev) const { return dev / 32 >= m_shard.warpLo && dev / 32 < m_shard.warpHi; }
 	void flushPending();
@@ -272,6 +282,10 @@ private:
 	bool m_pendingGather = false;
 	/* one-cycle steps run on the global current slots (CycleArgs::globalAcc) */
 	bool m_stepGlobalAcc = true;
+
+	/* the network has plugin models: every cycle runs their updates
+	 * between the current export and the step launch */
+	bool m_external = false;
 
 	/* sharded simulation */
 	bool m_shardMode = false;

@@ -301,7 +301,10 @@ class Simulation:
             raise ValueError("network and configuration are bound to different libraries")
         self.handle = self.lib.dll.nemo_new_simulation(net.handle, conf.handle)
         if not self.handle:
-            raise NemoError(-1, self.lib.dll.nemo_strerror().decode(errors="replace"))
+            # the constructor returns NULL; the status of the failure, where
+            # the library reports it
+            status = self.lib.dll.nemo_b200_last_status() if hasattr(self.lib.dll, "nemo_b200_last_status") else -1
+            raise NemoError(status, self.lib.dll.nemo_strerror().decode(errors="replace"))
         self._fired = POINTER(c_uint)()
         self._nfired = c_size_t()
 

@@ -1,0 +1,166 @@
+"""Neuron models supplied as GPU plugins (include/nemo_b200_plugin.h): a
+model whose name is not built in is loaded from <dir>/b200/lib<Name>.so
+beside <Name>.ini, as the reference loads lib<Name>.so from <dir>/{cpu,cuda}/
+(src/nemo/NeuronType.cpp:48-73). tests/plugins/QIFPlugin.cu restates the
+QIF update as a user's plugin; a network using it must fire and evolve
+exactly as the oracle's network with the built-in QIF."""
+import copy
+import ctypes
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from nemo_b200 import build as nb_build
+from nemo_b200 import netgen
+from nemo_b200.nemo import Configuration, Library, NemoError, Network, Simulation
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PLUGIN_DIR = os.path.join(ROOT, "tests", "plugins")
+
+NEMO_CUDA_INVOCATION_ERROR = 1
+NEMO_CUDA_ERROR = 4
+NEMO_API_UNSUPPORTED = 5
+NEMO_INVALID_INPUT = 6
+NEMO_DL_ERROR = 12
+
+
+@pytest.fixture(scope="module")
+def plugin_lib():
+    nb_build.build_plugin(os.path.join(PLUGIN_DIR, "QIFPlugin.cu"))
+    lib = Library()
+    lib.dll.nemo_add_plugin_path(PLUGIN_DIR.encode())
+    return lib
+
+
+def _spec(n_iz=700, n_qif=300, m=60, seed=4, stdp=False):
+    """Izhikevich and QIF populations, m synapses per neuron; with stdp the
+    excitatory Izhikevich sources' synapses are plastic."""
+    spec = netgen.mixed_plugins(n_iz=n_iz, n_lif=0, n_qif=n_qif, n_hh=0, m=m, dmax=8, seed=seed)
+    if stdp:
+        n_exc = int(n_iz * 0.8)
+        spec.plastic = (spec.source < n_exc).astype(np.uint8)
+    return spec
+
+
+def _as_plugin(spec):
+    s = copy.deepcopy(spec)
+    for p in s.populations:
+        if p.type_name == "QIF":
+            p.type_name = "QIFPlugin"
+    return s
+
+
+def test_plugin_header_compiles_as_c_and_cpp(tmp_path):
+    src = tmp_path / "use.c"
+    src.write_text('#include <nemo_b200_plugin.h>\n'
+                   'static b200_update_neurons_t* f;\n'
+                   'int main(void) { b200_neuron_batch b; b.count = 0; (void) b; (void) f; return 0; }\n')
+    for compiler, flags in (("gcc", ["-std=c99"]), ("g++", ["-std=c++11", "-x", "c++"])):
+        exe = shutil.which(compiler)
+        if exe is None:
+            pytest.skip("%s not found" % compiler)
+        subprocess.check_call([exe] + flags + ["-Wall", "-Werror", "-fsyntax-only", "-I",
+                                               os.path.join(ROOT, "include"), str(src)])
+
+
+def test_plugin_exports_update(plugin_lib):
+    so = ctypes.CDLL(os.path.join(PLUGIN_DIR, "b200", "libQIFPlugin.so"))
+    assert hasattr(so, "b200_update_neurons")
+
+
+def _simulation_status(lib, type_name, plugin_path=None):
+    if plugin_path:
+        lib.dll.nemo_add_plugin_path(plugin_path.encode())
+    net = Network(lib)
+    t = net.add_neuron_type(type_name)
+    net.add_neuron(t, 0, 0.04, 0.0)   # parameter a, state v (QIFPlugin.ini)
+    try:
+        Simulation(net, Configuration(lib))
+    except NemoError as e:
+        return e.status, str(e)
+    return 0, ""
+
+
+def test_unknown_model_without_plugin_is_unsupported(tmp_path):
+    """A model with a descriptor but neither a built-in kernel nor a plugin
+    library: the simulation is refused before any device work."""
+    (tmp_path / "NoKernel.ini").write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
+    status, msg = _simulation_status(Library(), "NoKernel", str(tmp_path))
+    assert status == NEMO_API_UNSUPPORTED, msg
+    assert "b200/libNoKernel.so" in msg
+
+
+def test_plugin_without_update_symbol_is_rejected(tmp_path):
+    """A plugin library that does not export b200_update_neurons."""
+    (tmp_path / "NoUpdate.ini").write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
+    (tmp_path / "b200").mkdir()
+    src = tmp_path / "noupdate.c"
+    src.write_text("int b200_something_else(void) { return 0; }\n")
+    subprocess.check_call(["gcc", "-shared", "-fPIC", "-o", str(tmp_path / "b200" / "libNoUpdate.so"), str(src)])
+    status, msg = _simulation_status(Library(), "NoUpdate", str(tmp_path))
+    assert status == NEMO_INVALID_INPUT, msg
+    assert "b200_update_neurons" in msg
+
+
+def test_plugin_that_cannot_load_is_a_dl_error(tmp_path):
+    (tmp_path / "Broken.ini").write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
+    (tmp_path / "b200").mkdir()
+    (tmp_path / "b200" / "libBroken.so").write_bytes(b"not an ELF file")
+    status, msg = _simulation_status(Library(), "Broken", str(tmp_path))
+    assert status == NEMO_DL_ERROR, msg
+
+
+@pytest.mark.gpu
+def test_plugin_model_matches_builtin(plugin_lib, oracle_lib):
+    """Izhikevich + plugin QIF on the B200 against Izhikevich + built-in QIF
+    on the oracle: identical firing every cycle (firing and current stimulus
+    on both populations), identical v bits of every QIF neuron, STDP applied
+    every 50 cycles."""
+    spec = _spec(stdp=True)
+    pspec = _as_plugin(spec)
+    pre, post = netgen.standard_stdp()
+    sims = []
+    for lib, s in ((plugin_lib, pspec), (oracle_lib, spec)):
+        net = s.build(Network(lib))
+        conf = Configuration(lib)
+        conf.set_stdp_function(pre, post, 0.0, 1.0, 0.0, -1.0)
+        if lib is oracle_lib:
+            conf.set_cpu_backend()
+        sims.append((net, Simulation(net, conf)))
+    (_, g), (_, o) = sims
+    n = spec.neuron_count
+    qif = [p for p in spec.populations if p.type_name == "QIF"][0].idx
+    rng = np.random.default_rng(11)
+    fired_qif = 0
+    for c in range(200):
+        fstim = np.sort(rng.choice(n, 8, replace=False)).astype(np.uint32)
+        ii = rng.choice(n, 40, replace=False)
+        istim = [(int(i), float(rng.normal(40, 20))) for i in ii]
+        a, b = g.step(fstim=fstim, istim=istim), o.step(fstim=fstim, istim=istim)
+        assert np.array_equal(a, b), "cycle %d" % c
+        fired_qif += int(np.isin(a, qif).sum())
+        if c % 50 == 49:
+            g.apply_stdp(1.0)
+            o.apply_stdp(1.0)
+    assert fired_qif > 100
+    for i in qif:
+        assert np.float32(g.get_membrane_potential(int(i))).view(np.uint32) == \
+            np.float32(o.get_membrane_potential(int(i))).view(np.uint32), i
+
+
+@pytest.mark.gpu
+def test_plugin_model_refuses_multi_cycle_runs(plugin_lib):
+    """Plugin updates run cycle by cycle: the device-resident multi-cycle
+    entry points refuse such a network with NEMO_API_UNSUPPORTED."""
+    net = _as_plugin(_spec(n_iz=64, n_qif=64, m=8)).build(Network(plugin_lib))
+    sim = Simulation(net, Configuration(plugin_lib))
+    sim.step()
+    P = ctypes.POINTER
+    plugin_lib.dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    with pytest.raises(NemoError) as e:
+        plugin_lib.call("nemo_b200_run", sim.handle, 10, None, None)
+    assert e.value.status == NEMO_API_UNSUPPORTED
+    sim.step()
