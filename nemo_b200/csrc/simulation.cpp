@@ -585,6 +585,8 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 				fail(NEMO_CUDA_INVOCATION_ERROR, "Neuron model plugin " + g.plugin->path + ": b200_init_neurons: "
 						+ cudaGetErrorString(cudaError_t(rc)));
 			}
+			/* the device state is ahead of the host copy */
+			m_stateDirty = true;
 		}
 	}
 	NEMO_CUDA(cudaStreamSynchronize(stream));

@@ -5,9 +5,9 @@
  * as a plain CUDA kernel with the reference's float operation order. A
  * network using it must behave exactly like one using the built-in QIF.
  *
- * Built with: nvcc -shared -Xcompiler -fPIC -gencode
- * arch=compute_100a,code=sm_100a -fmad=false -I include
- * -o tests/plugins/b200/libQIFPlugin.so tests/plugins/QIFPlugin.cu */
+ * Built by nemo_b200.build.build_plugin into b200/libQIFPlugin.so, and with
+ * QIF_PLUGIN_INIT defined into b200/libQIFPluginInit.so, which also exports
+ * b200_init_neurons (initial v = 5 a, replacing the state given). */
 
 #include <cuda_runtime.h>
 
@@ -69,3 +69,24 @@ b200_update_neurons(const b200_neuron_batch* batch, void* stream)
 	k_qif_plugin<<<(batch->count + 255u) / 256u, 256, 0, (cudaStream_t) stream>>>(*batch);
 	return (int) cudaGetLastError();
 }
+
+#ifdef QIF_PLUGIN_INIT
+__global__ void
+k_qif_plugin_init(b200_neuron_batch b)
+{
+	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i < b.count) {
+		b.state[i] = __fmul_rn(b.param[i], 5.0f);
+	}
+}
+
+extern "C" int
+b200_init_neurons(const b200_neuron_batch* batch, void* stream)
+{
+	if(batch->count == 0) {
+		return 0;
+	}
+	k_qif_plugin_init<<<(batch->count + 255u) / 256u, 256, 0, (cudaStream_t) stream>>>(*batch);
+	return (int) cudaGetLastError();
+}
+#endif

@@ -27,9 +27,15 @@ NEMO_INVALID_INPUT = 6
 NEMO_DL_ERROR = 12
 
 
+def build_test_plugins():
+    src = os.path.join(PLUGIN_DIR, "QIFPlugin.cu")
+    nb_build.build_plugin(src)
+    nb_build.build_plugin(src, name="QIFPluginInit", extra_flags=["-DQIF_PLUGIN_INIT"])
+
+
 @pytest.fixture(scope="module")
 def plugin_lib():
-    nb_build.build_plugin(os.path.join(PLUGIN_DIR, "QIFPlugin.cu"))
+    build_test_plugins()
     lib = Library()
     lib.dll.nemo_add_plugin_path(PLUGIN_DIR.encode())
     return lib
@@ -45,11 +51,11 @@ def _spec(n_iz=700, n_qif=300, m=60, seed=4, stdp=False):
     return spec
 
 
-def _as_plugin(spec):
+def _as_plugin(spec, name="QIFPlugin"):
     s = copy.deepcopy(spec)
     for p in s.populations:
         if p.type_name == "QIF":
-            p.type_name = "QIFPlugin"
+            p.type_name = name
     return s
 
 
@@ -164,3 +170,29 @@ def test_plugin_model_refuses_multi_cycle_runs(plugin_lib):
         plugin_lib.call("nemo_b200_run", sim.handle, 10, None, None)
     assert e.value.status == NEMO_API_UNSUPPORTED
     sim.step()
+
+
+@pytest.mark.gpu
+def test_plugin_init_sets_initial_state(plugin_lib, oracle_lib):
+    """b200_init_neurons runs once when the simulation is created: the
+    QIFPluginInit population starts from v = 5 a whatever state it was given,
+    and then fires like built-in QIF neurons that were given v = 5 a."""
+    spec = _spec(n_iz=500, n_qif=200, m=40, seed=9)
+    pspec = _as_plugin(spec, "QIFPluginInit")
+    q = [p for p in spec.populations if p.type_name == "QIF"][0]
+    q.args[1] = (np.asarray(q.args[0], np.float32) * np.float32(5)).astype(np.float32)
+    g = Simulation(pspec.build(Network(plugin_lib)), Configuration(plugin_lib))
+    conf = Configuration(oracle_lib)
+    conf.set_cpu_backend()
+    o = Simulation(spec.build(Network(oracle_lib)), conf)
+    v0 = np.float32(0.04) * np.float32(5)
+    for i in q.idx[::17]:
+        assert np.float32(g.get_membrane_potential(int(i))).view(np.uint32) == v0.view(np.uint32), i
+    rng = np.random.default_rng(2)
+    n = spec.neuron_count
+    for c in range(100):
+        istim = [(int(i), float(rng.normal(40, 20))) for i in rng.choice(n, 30, replace=False)]
+        assert np.array_equal(g.step(istim=istim), o.step(istim=istim)), "cycle %d" % c
+    for i in q.idx:
+        assert np.float32(g.get_membrane_potential(int(i))).view(np.uint32) == \
+            np.float32(o.get_membrane_potential(int(i))).view(np.uint32), i

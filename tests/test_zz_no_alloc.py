@@ -135,3 +135,32 @@ def test_noalloc_limits_and_errors():
     assert na.status(fstim=bad) == NEMO_INVALID_INPUT
     for _ in range(30):
         assert np.array_equal(ref.step(), na.step())
+
+
+def test_noalloc_with_plugin_model():
+    """A network with a GPU plugin population (tests/plugins/QIFPlugin): the
+    allocation-free step runs the plugin's update like nemo_step does."""
+    import copy
+    import os
+    from nemo_b200 import build as nb_build
+    plugin_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "plugins")
+    nb_build.build_plugin(os.path.join(plugin_dir, "QIFPlugin.cu"))
+    lib = Library()
+    lib.dll.nemo_add_plugin_path(plugin_dir.encode())
+    spec = netgen.mixed_plugins(n_iz=400, n_lif=0, n_qif=300, n_hh=0, m=40, dmax=8, seed=3)
+    spec = copy.deepcopy(spec)
+    for p in spec.populations:
+        if p.type_name == "QIF":
+            p.type_name = "QIFPlugin"
+    a = Simulation(spec.build(Network(lib)), Configuration(lib))
+    b = Simulation(spec.build(Network(lib)), Configuration(lib))
+    n = spec.neuron_count
+    na = NoAlloc(lib, b, n)
+    rng = np.random.default_rng(8)
+    for c in range(60):
+        fstim = np.sort(rng.choice(n, 5, replace=False)).astype(np.uint32)
+        istim = [(int(i), float(rng.normal(40, 20))) for i in rng.choice(n, 30, replace=False)]
+        assert np.array_equal(a.step(fstim=fstim, istim=istim), na.step(fstim=fstim, istim=istim)), c
+    for i in range(400, 700, 7):
+        assert np.float32(a.get_membrane_potential(i)).view(np.uint32) == \
+            np.float32(b.get_membrane_potential(i)).view(np.uint32), i
