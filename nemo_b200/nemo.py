@@ -129,6 +129,12 @@ class Library:
     def version(self):
         return self.dll.nemo_version().decode()
 
+    def add_plugin_path(self, path):
+        """Search `path` for neuron-model descriptors <Name>.ini (and GPU plugins
+        b200/lib<Name>.so beside them) before the default directories
+        (nemo_add_plugin_path, src/nemo.h)."""
+        self.call("nemo_add_plugin_path", os.fsencode(os.path.abspath(path)))
+
 
 def _u32(a):
     return np.ascontiguousarray(np.asarray(a, dtype=np.uint32).reshape(-1))

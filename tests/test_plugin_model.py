@@ -37,7 +37,7 @@ def build_test_plugins():
 def plugin_lib():
     build_test_plugins()
     lib = Library()
-    lib.dll.nemo_add_plugin_path(PLUGIN_DIR.encode())
+    lib.add_plugin_path(PLUGIN_DIR)
     return lib
 
 
@@ -79,7 +79,7 @@ def test_plugin_exports_update(plugin_lib):
 
 def _simulation_status(lib, type_name, plugin_path=None):
     if plugin_path:
-        lib.dll.nemo_add_plugin_path(plugin_path.encode())
+        lib.add_plugin_path(plugin_path)
     net = Network(lib)
     t = net.add_neuron_type(type_name)
     net.add_neuron(t, 0, 0.04, 0.0)   # parameter a, state v (QIFPlugin.ini)

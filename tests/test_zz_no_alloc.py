@@ -146,7 +146,7 @@ def test_noalloc_with_plugin_model():
     plugin_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "plugins")
     nb_build.build_plugin(os.path.join(plugin_dir, "QIFPlugin.cu"))
     lib = Library()
-    lib.dll.nemo_add_plugin_path(plugin_dir.encode())
+    lib.add_plugin_path(plugin_dir)
     spec = netgen.mixed_plugins(n_iz=400, n_lif=0, n_qif=300, n_hh=0, m=40, dmax=8, seed=3)
     spec = copy.deepcopy(spec)
     for p in spec.populations:
