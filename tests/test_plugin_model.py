@@ -31,6 +31,7 @@ def build_test_plugins():
     src = os.path.join(PLUGIN_DIR, "QIFPlugin.cu")
     nb_build.build_plugin(src)
     nb_build.build_plugin(src, name="QIFPluginInit", extra_flags=["-DQIF_PLUGIN_INIT"])
+    nb_build.build_plugin(os.path.join(PLUGIN_DIR, "LIFPlugin.cu"))
 
 
 @pytest.fixture(scope="module")
@@ -196,3 +197,40 @@ def test_plugin_init_sets_initial_state(plugin_lib, oracle_lib):
     for i in q.idx:
         assert np.float32(g.get_membrane_potential(int(i))).view(np.uint32) == \
             np.float32(o.get_membrane_potential(int(i))).view(np.uint32), i
+
+
+@pytest.mark.gpu
+def test_two_plugin_models_with_strided_state(plugin_lib, oracle_lib):
+    """Two plugin populations in one network, LIFPlugin (nine parameters,
+    four state variables through the batch's strides) and QIFPlugin, beside
+    Izhikevich: identical firing to the oracle's IF_curr_exp and QIF every
+    cycle, and identical bits of every state variable afterwards."""
+    spec = netgen.mixed_plugins(n_iz=600, n_lif=400, n_qif=200, n_hh=0, m=50, dmax=6, seed=12)
+    pspec = copy.deepcopy(spec)
+    names = {"IF_curr_exp": "LIFPlugin", "QIF": "QIFPlugin"}
+    for p in pspec.populations:
+        p.type_name = names.get(p.type_name, p.type_name)
+    g = Simulation(pspec.build(Network(plugin_lib)), Configuration(plugin_lib))
+    conf = Configuration(oracle_lib)
+    conf.set_cpu_backend()
+    o = Simulation(spec.build(Network(oracle_lib)), conf)
+    n = spec.neuron_count
+    rng = np.random.default_rng(5)
+    fired = {k: 0 for k in names}
+    for c in range(150):
+        fstim = np.sort(rng.choice(n, 6, replace=False)).astype(np.uint32)
+        istim = [(int(i), float(rng.normal(30, 15))) for i in rng.choice(n, 40, replace=False)]
+        a, b = g.step(fstim=fstim, istim=istim), o.step(fstim=fstim, istim=istim)
+        assert np.array_equal(a, b), "cycle %d" % c
+        for p in spec.populations:
+            if p.type_name in fired:
+                fired[p.type_name] += int(np.isin(a, p.idx).sum())
+    assert min(fired.values()) > 20, fired
+    for p in spec.populations:
+        if p.type_name not in names:
+            continue
+        nstate = 4 if p.type_name == "IF_curr_exp" else 1
+        for var in range(nstate):
+            for i in p.idx:
+                assert np.float32(g.get_neuron_state(int(i), var)).view(np.uint32) == \
+                    np.float32(o.get_neuron_state(int(i), var)).view(np.uint32), (p.type_name, var, i)
