@@ -78,9 +78,11 @@ def build_sim(lib, wl, oracle=False):
     conf.set_write_only_synapses()
     if oracle:
         conf.set_cpu_backend()
+    t = time.perf_counter()
     sim = Simulation(net, conf)
+    build_s = time.perf_counter() - t
     del net
-    return sim, spec
+    return sim, spec, build_s
 
 
 def stim_stream(n, cycles, seed=7):
@@ -120,7 +122,7 @@ def run_oracle_steps(wl, warmup, steps, budget_s=None):
     cores) on the workload: `warmup` untimed steps, then up to `steps` timed
     steps of 100 cycles + applyStdp, stopping early after budget_s seconds."""
     lib = Library(oracle_library())
-    sim, spec = build_sim(lib, wl, oracle=True)
+    sim, spec, build_s = build_sim(lib, wl, oracle=True)
     m = wl["m"]
     for s in range(warmup):
         e2e_steps(sim, wl["n"], 1, seed=100 + s)
@@ -135,7 +137,7 @@ def run_oracle_steps(wl, warmup, steps, budget_s=None):
         if budget_s is not None and time.perf_counter() - t_start > budget_s:
             break
     total = sum(times)
-    return events / total, done, total
+    return events / total, done, total, build_s
 
 
 def oracle_library():
@@ -389,10 +391,11 @@ def run_b200(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         del sim
-        v, nsteps, secs = run_oracle_steps(wl, 0, args.cpu_steps, budget_s=args.cpu_seconds)
+        v, nsteps, secs, o_build = run_oracle_steps(wl, 0, args.cpu_steps, budget_s=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                 "sample": "%d step(s) of 100 cycles + applyStdp from a fresh network, %.1f s, "
-                                          "e2e protocol" % (nsteps, secs)}
+                                          "e2e protocol" % (nsteps, secs),
+                                "build_s": round(o_build, 2)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -404,11 +407,12 @@ def run_reference(args):
     if rank != 0:
         return
     wl = workload(args.small)
-    v, nsteps, secs = run_oracle_steps(wl, args.warmup, args.steps, budget_s=args.cpu_seconds * 6)
+    v, nsteps, secs, build_s = run_oracle_steps(wl, args.warmup, args.steps, budget_s=args.cpu_seconds * 6)
     n = wl["n"]
     line = {
         "metric": METRIC, "value": round(v, 1), "unit": UNIT, "impl": "reference", "n_gpus": 0,
         "steps": nsteps, "warmup": args.warmup, "ms_per_step": round(secs * 1000 / nsteps, 2),
+        "build_s": round(build_s, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/int64 fixed point + f32/f64 state", "data": "synthetic (seeded generator)",
         "config": bench_config(wl, 1),

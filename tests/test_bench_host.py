@@ -78,6 +78,7 @@ def test_reference_arm_line():
     assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["kind"] == "port"
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+    assert line["build_s"] > 0
     assert line["config"]["workload"] == "izhikevich-20k-m1000-stdp"
     assert line["config"]["synapses"] == 20000 * 1000
     assert "160 MB" in line["config"]["l2"]
