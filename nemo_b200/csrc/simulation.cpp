@@ -87,6 +87,19 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 	m_dCur(nullptr),
 	m_stimCap(0)
 {
+	/* the destructor does not run for a constructor that throws: release
+	 * what the construction allocated before passing the error on */
+	try {
+		construct(net, conf, shard);
+	} catch(...) {
+		release();
+		throw;
+	}
+}
+
+void
+Simulation::construct(const Network& net, const Configuration& conf, const ShardSpec* shard)
+{
 	std::memset(&m_net, 0, sizeof(m_net));
 	std::memset(&m_rule, 0, sizeof(m_rule));
 	std::memset(&m_args, 0, sizeof(m_args));
@@ -595,9 +608,16 @@ Simulation::Simulation(const Network& net, const Configuration& conf, const Shar
 
 Simulation::~Simulation()
 {
+	release();
+}
+
+void
+Simulation::release()
+{
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
 	destroyGraph();
 	for(void* p : m_allocs) cudaFree(p);
+	m_allocs.clear();
 	if(m_hWords) cudaFreeHost(m_hWords);
 	if(m_stepWords) cudaFreeHost(m_stepWords);
 	if(m_hStim) cudaFreeHost(m_hStim);
@@ -605,6 +625,14 @@ Simulation::~Simulation()
 	if(m_dStim) cudaFree(m_dStim);
 	if(m_dCur) cudaFree(m_dCur);
 	if(m_stream) cudaStreamDestroy(STREAM(m_stream));
+	m_hWords = nullptr;
+	m_stepWords = nullptr;
+	m_dStepWords = nullptr;
+	m_hStim = nullptr;
+	m_hCur = nullptr;
+	m_dStim = nullptr;
+	m_dCur = nullptr;
+	m_stream = nullptr;
 }
 
 uint32_t

@@ -204,6 +204,8 @@ private:
 	void launchStep();
 	void stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 			bool ownedOnly);
+	void construct(const Network& net, const Configuration& conf, const ShardSpec* shard);
+	void release();
 	void notShard(const char* what) const;
 	void notExternal(const char* what) const;
 	void runPlugins();

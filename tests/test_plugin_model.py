@@ -234,3 +234,50 @@ def test_two_plugin_models_with_strided_state(plugin_lib, oracle_lib):
             for i in p.idx:
                 assert np.float32(g.get_neuron_state(int(i), var)).view(np.uint32) == \
                     np.float32(o.get_neuron_state(int(i), var)).view(np.uint32), (p.type_name, var, i)
+
+
+def _failing_plugin(tmp_path, name, body):
+    """A plugin library (plain C, no kernels) named `name` with the given
+    entry points, and its descriptor."""
+    (tmp_path / (name + ".ini")).write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
+    (tmp_path / "b200").mkdir(exist_ok=True)
+    src = tmp_path / (name + ".c")
+    src.write_text(body)
+    subprocess.check_call(["gcc", "-shared", "-fPIC", "-o", str(tmp_path / "b200" / ("lib%s.so" % name)), str(src)])
+
+
+@pytest.mark.gpu
+def test_plugin_update_error_is_reported(tmp_path):
+    """An update that returns a CUDA error code (here 1, cudaErrorInvalidValue,
+    without launching anything): nemo_step fails with
+    NEMO_CUDA_INVOCATION_ERROR naming the plugin's entry point."""
+    _failing_plugin(tmp_path, "FailingUpdate",
+                    "int b200_update_neurons(const void* batch, void* stream) { return 1; }\n")
+    lib = Library()
+    lib.add_plugin_path(str(tmp_path))
+    net = Network(lib)
+    t = net.add_neuron_type("FailingUpdate")
+    net.add_neuron(t, 0, 0.04, 0.0)
+    sim = Simulation(net, Configuration(lib))
+    with pytest.raises(NemoError) as e:
+        sim.step()
+    assert e.value.status == NEMO_CUDA_INVOCATION_ERROR
+    assert "b200_update_neurons" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_plugin_init_error_is_reported(tmp_path):
+    """An initialisation that returns a CUDA error code: the simulation is
+    not created, with NEMO_CUDA_INVOCATION_ERROR naming b200_init_neurons."""
+    _failing_plugin(tmp_path, "FailingInit",
+                    "int b200_update_neurons(const void* batch, void* stream) { return 0; }\n"
+                    "int b200_init_neurons(const void* batch, void* stream) { return 1; }\n")
+    lib = Library()
+    lib.add_plugin_path(str(tmp_path))
+    net = Network(lib)
+    t = net.add_neuron_type("FailingInit")
+    net.add_neuron(t, 0, 0.04, 0.0)
+    with pytest.raises(NemoError) as e:
+        Simulation(net, Configuration(lib))
+    assert e.value.status == NEMO_CUDA_INVOCATION_ERROR
+    assert "b200_init_neurons" in str(e.value)
