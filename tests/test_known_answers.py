@@ -25,6 +25,21 @@ def add_excitatory(net, t, idx, sigma=0.0):
     net.add_neuron(t, idx, np.float32(0.02) + np.float32(0.08) * r, b, v, 2.0, sigma, b * v, v)
 
 
+# ---- neuron count: src/test/test.cpp:155-177 (network construction only,
+# so both libraries run it on the host) ----
+
+@pytest.mark.parametrize("which", ["oracle", "b200"])
+@pytest.mark.parametrize("start,step", [(0, 1), (1000, 1), (0, 5), (1000, 5)])
+def test_neuron_count(which, start, step):
+    from conftest import ensure_oracle
+    from nemo_b200.nemo import Library
+    lib = Library(ensure_oracle()) if which == "oracle" else Library()
+    net = Network(lib)
+    for i in range(2000):
+        net.add_neuron_iz(start + i * step, 0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7)
+    assert net.neuron_count() == 2000
+
+
 # ---- ring networks: src/test/test.cpp:302-328, 474-490 ----
 
 @pytest.mark.parametrize("ncount,delay", [(1000, 1), (1024, 1), (2000, 1), (4000, 1), (2000, 20), (2000, 63)])

@@ -32,6 +32,7 @@ def build_test_plugins():
     nb_build.build_plugin(src)
     nb_build.build_plugin(src, name="QIFPluginInit", extra_flags=["-DQIF_PLUGIN_INIT"])
     nb_build.build_plugin(os.path.join(PLUGIN_DIR, "LIFPlugin.cu"))
+    nb_build.build_plugin(os.path.join(PLUGIN_DIR, "IzhikevichRS.cu"))
 
 
 @pytest.fixture(scope="module")
@@ -281,3 +282,24 @@ def test_plugin_init_error_is_reported(tmp_path):
         Simulation(net, Configuration(lib))
     assert e.value.status == NEMO_CUDA_INVOCATION_ERROR
     assert "b200_init_neurons" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_no_parameter_plugin_model(plugin_lib):
+    """src/test/test.cpp:988-1006 (plugins/no_parameters): 1000 neurons of
+    IzhikevichRS, a model with no parameters that the reference ships only as
+    a CUDA kernel, run here as a B200 plugin; 100 cycles without synapses
+    leave u and v finite. Then a current of 100 in one cycle makes the
+    stimulated neurons fire and reset (v = -65); the others stay at rest."""
+    net = Network(plugin_lib)
+    rs = net.add_neuron_type("IzhikevichRS")
+    for n in range(1000):
+        net.add_neuron(rs, n, -13.0, -65.0)
+    sim = Simulation(net, Configuration(plugin_lib))
+    for _ in range(100):
+        sim.step()
+        u, v = sim.get_neuron_state(100, 0), sim.get_neuron_state(100, 1)
+        assert np.isfinite(u) and np.isfinite(v)
+    fired = sim.step(istim=[(n, 100.0) for n in range(0, 1000, 3)])
+    assert np.array_equal(fired, np.arange(0, 1000, 3, dtype=np.uint32))
+    assert sim.get_membrane_potential(0) == -65.0 and sim.get_membrane_potential(1) != -65.0
