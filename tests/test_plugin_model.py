@@ -303,3 +303,22 @@ def test_no_parameter_plugin_model(plugin_lib):
     fired = sim.step(istim=[(n, 100.0) for n in range(0, 1000, 3)])
     assert np.array_equal(fired, np.arange(0, 1000, 3, dtype=np.uint32))
     assert sim.get_membrane_potential(0) == -65.0 and sim.get_membrane_potential(1) != -65.0
+
+
+def test_build_plugin_places_and_rebuilds(tmp_path):
+    """nemo_b200.build.build_plugin compiles <dir>/<Name>.cu into
+    <dir>/b200/lib<Name>.so, exporting the entry point, and rebuilds only when
+    the source is newer than the library."""
+    src = tmp_path / "Tiny.cu"
+    src.write_text('#include <nemo_b200_plugin.h>\n'
+                   'extern "C" int b200_update_neurons(const b200_neuron_batch* b, void* s) { return 0; }\n')
+    out = nb_build.build_plugin(str(src))
+    assert out == str(tmp_path / "b200" / "libTiny.so")
+    assert hasattr(ctypes.CDLL(out), "b200_update_neurons")
+    t0 = os.path.getmtime(out)
+    assert nb_build.build_plugin(str(src)) == out and os.path.getmtime(out) == t0
+    os.utime(src, (t0 + 10, t0 + 10))
+    nb_build.build_plugin(str(src))
+    assert os.path.getmtime(out) > t0
+    other = nb_build.build_plugin(str(src), name="Renamed", plugin_dir=str(tmp_path / "elsewhere"))
+    assert other == str(tmp_path / "elsewhere" / "b200" / "libRenamed.so") and os.path.exists(other)
