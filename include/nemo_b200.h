@@ -16,7 +16,9 @@ extern "C" {
 
 /* Run `cycles` cycles (<= 1024 per call) without stimulus, entirely on the
  * device in one persistent launch of the step kernel (spike gather, neuron
- * update and STDP accumulation per cycle, one grid barrier per cycle).
+ * update and STDP accumulation per cycle, one grid barrier per cycle); a
+ * network with plugin neuron models (nemo_b200_plugin.h) instead queues
+ * each cycle's plugin updates and step launch without host synchronisation.
  * Equivalent to `cycles` calls of nemo_step with empty stimulus. fired_counts[k] / events[k] (each may be NULL) receive the
  * number of neurons fired in cycle k and the synaptic events those firings
  * generate (fired neurons x out-degree, the throughput unit of the

@@ -1049,16 +1049,29 @@ void
 Simulation::run(unsigned cycles, uint32_t* firedCounts, uint64_t* events)
 {
 	notShard("run");
-	notExternal("run");
 	flushPending();
 	if(cycles == 0) return;
 	if(cycles > m_ring) {
 		fail(NEMO_INVALID_INPUT, "run: at most " + std::to_string(m_ring) + " cycles per call");
 	}
 	cudaStream_t stream = STREAM(m_stream);
-	launchBlock(m_cycle, cycles);
 	uint64_t first = m_cycle;
-	m_cycle += cycles;
+	if(m_external) {
+		/* plugin models update between the kernel's phases: every cycle's
+		 * current export, plugin updates and one-phase step launch are
+		 * queued on the stream without waiting, as nemo_step runs them; a
+		 * barrier timeout in any of them stays in the barrier's error word */
+		for(unsigned k = 0; k < cycles; ++k) {
+			runPlugins();
+			launchBlock(m_cycle, 1, (m_pendingGather ? 1u : 0u) | 2u, m_stepGlobalAcc);
+			m_pendingGather = true;
+			m_cycle++;
+		}
+		flushPending();
+	} else {
+		launchBlock(m_cycle, cycles);
+		m_cycle += cycles;
+	}
 	m_stateDirty = true;
 	std::vector<uint32_t> fc(m_ring);
 	std::vector<uint64_t> ev(m_ring);

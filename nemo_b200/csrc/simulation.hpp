@@ -59,8 +59,10 @@ public:
 			unsigned* firedOut, size_t firedCapacity);
 
 	/* Device-resident run of `cycles` cycles without stimulus in one
-	 * persistent launch; per-cycle fired counts and synaptic events (fired x
-	 * out-degree) are returned when the pointers are non-null. */
+	 * persistent launch (for a network with plugin models, one launch
+	 * sequence per cycle, queued without waiting); per-cycle fired counts
+	 * and synaptic events (fired x out-degree) are returned when the
+	 * pointers are non-null. */
 	void run(unsigned cycles, uint32_t* firedCounts, uint64_t* events);
 
 	/* Fired neurons of one of the last cycles run (device firing ring). */

@@ -160,18 +160,58 @@ def test_plugin_model_matches_builtin(plugin_lib, oracle_lib):
 
 
 @pytest.mark.gpu
-def test_plugin_model_refuses_multi_cycle_runs(plugin_lib):
-    """Plugin updates run cycle by cycle: the device-resident multi-cycle
-    entry points refuse such a network with NEMO_API_UNSUPPORTED."""
+def test_plugin_model_refuses_persistent_multi_cycle_calls(plugin_lib):
+    """Plugin updates run between the kernel's cycles: the calls that need
+    one persistent launch over many cycles (timed steps, graph runs) refuse
+    such a network with NEMO_API_UNSUPPORTED, and the simulation goes on."""
     net = _as_plugin(_spec(n_iz=64, n_qif=64, m=8)).build(Network(plugin_lib))
     sim = Simulation(net, Configuration(plugin_lib))
     sim.step()
-    P = ctypes.POINTER
-    plugin_lib.dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    plugin_lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                                     ctypes.c_float, ctypes.c_double * 4]
+    out = (ctypes.c_double * 4)()
     with pytest.raises(NemoError) as e:
-        plugin_lib.call("nemo_b200_run", sim.handle, 10, None, None)
+        plugin_lib.call("nemo_b200_timed_steps", sim.handle, 1, 10, 0, ctypes.c_float(0), out)
     assert e.value.status == NEMO_API_UNSUPPORTED
     sim.step()
+
+
+@pytest.mark.gpu
+def test_plugin_model_device_resident_run(plugin_lib):
+    """nemo_b200_run on a network with plugin models (the cycles queued
+    without host synchronisation) fires exactly as nemo_step cycle by cycle
+    on a second copy: per-cycle counts, fired lists and final potentials."""
+    spec = _as_plugin(_spec(n_iz=600, n_qif=300, m=50, seed=21))
+    iz = [p for p in spec.populations if p.type_name == "Izhikevich"][0]
+    iz.args[4] = np.full(iz.idx.size, 5.0, np.float32)   # thalamic noise: firing every cycle
+    a = Simulation(spec.build(Network(plugin_lib)), Configuration(plugin_lib))
+    b = Simulation(spec.build(Network(plugin_lib)), Configuration(plugin_lib))
+    P = ctypes.POINTER
+    dll = plugin_lib.dll
+    dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    dll.nemo_b200_fired_at.argtypes = [ctypes.c_void_p, ctypes.c_uint64, P(P(ctypes.c_uint)), P(ctypes.c_size_t)]
+    n = spec.neuron_count
+    rng = np.random.default_rng(4)
+    cycle = 0
+    for chunk in (50, 120):
+        # a stimulated cycle before each run, so that there is activity
+        fstim = np.sort(rng.choice(n, 200, replace=False)).astype(np.uint32)
+        assert np.array_equal(a.step(fstim=fstim), b.step(fstim=fstim))
+        cycle += 1
+        counts = np.zeros(chunk, np.uint32)
+        plugin_lib.call("nemo_b200_run", a.handle, chunk, counts.ctypes.data_as(P(ctypes.c_uint32)), None)
+        for k in range(chunk):
+            expected = b.step()
+            assert counts[k] == expected.size, (chunk, k)
+            ptr, cnt = P(ctypes.c_uint)(), ctypes.c_size_t()
+            plugin_lib.call("nemo_b200_fired_at", a.handle, cycle + k, ctypes.byref(ptr), ctypes.byref(cnt))
+            got = np.ctypeslib.as_array(ptr, (cnt.value,)).copy() if cnt.value else np.zeros(0, np.uint32)
+            assert np.array_equal(got, expected), (chunk, k)
+        cycle += chunk
+        assert counts.sum() > chunk, counts.sum()
+    for i in range(0, n, 11):
+        assert np.float32(a.get_membrane_potential(i)).view(np.uint32) == \
+            np.float32(b.get_membrane_potential(i)).view(np.uint32), i
 
 
 @pytest.mark.gpu
