@@ -19,6 +19,7 @@
 #include <sstream>
 #include <thread>
 
+#include "compile.hpp"
 #include "libm_match.cuh"
 #include "libm_tables.hpp"
 
@@ -45,6 +46,20 @@ static bool
 fitsFix(float f, unsigned fbits)
 {
 	return !(std::abs(int(f)) >= 1 << (31 - fbits));
+}
+
+/* networks of at least this many synapses build their matrices on the
+ * device (NEMO_B200_DEVICE_BUILD_MIN overrides it; 0 builds every network
+ * there) */
+static size_t
+deviceBuildMinSynapses()
+{
+	if(const char* env = getenv("NEMO_B200_DEVICE_BUILD_MIN")) {
+		char* end = nullptr;
+		const unsigned long long v = strtoull(env, &end, 10);
+		if(end != env) return size_t(v);
+	}
+	return size_t(1) << 22;
 }
 
 static float
@@ -329,17 +344,53 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	const uint32_t B = m_blocks;
 	const uint32_t ownN = ownWarps * 32;
 
+	/* the simulation's stream; the device build of the layout runs on it */
+	cudaStream_t stream;
+	NEMO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+	m_stream = stream;
+
+	/* a large network builds its forward and reverse matrices on the
+	 * device (compile.cu), a small one on the host below; the two builds
+	 * are equal element for element */
+	const bool onDevice = S >= deviceBuildMinSynapses() && layoutOnDevice(S, m_nDev, B);
+	LayoutOut dev;
+	if(onDevice) {
+		LayoutIn li;
+		li.S = S;
+		li.nDev = m_nDev;
+		li.blocks = B;
+		li.warpLo = warpLo;
+		li.ownedWarps = uint32_t(ownerOfWarp.size());
+		li.stdp = m_stdpOn;
+		li.wantFcmPos = !m_writeOnly;
+		li.src = dsrc.data();
+		li.tgt = dtgt.data();
+		li.wfx = wfx.data();
+		li.dly = net.dly.data();
+		li.plastic = net.plastic.data();
+		li.ownerOfWarp = ownerOfWarp.data();
+		buildLayoutOnDevice(li, [this](size_t bytes) { return alloc(bytes); }, &dev, m_stream);
+	}
+
 	/* ---- forward matrix: the synapses of delay >= 2 partitioned by target
 	 * owner (region b holds, source by source, those whose target block b
 	 * owns, in insertion order within a segment), then the delay-1
 	 * synapses grouped by source (pushed at firing) ---- */
-	std::vector<uint64_t> regionBase(size_t(B) + 1, 0);
-	std::vector<uint32_t> segOff((size_t(m_nDev) + 1) * B, 0);
-	std::vector<uint32_t> d1Start(size_t(m_nDev) + 1, 0);
-	std::vector<uint2> fcm(S);
-	std::vector<uint32_t> fcmPos(S);
-	std::vector<uint32_t> synAt(S);   /* synapse at each forward position */
-	{
+	std::vector<uint64_t> regionBase;
+	std::vector<uint32_t> segOff, d1Start;
+	std::vector<uint2> fcm;
+	std::vector<uint32_t> fcmPos;
+	std::vector<uint32_t> synAt;   /* synapse at each forward position */
+	if(onDevice) {
+		regionBase = dev.regionBase;
+		fcmPos.swap(dev.fcmPos);
+	} else {
+		regionBase.assign(size_t(B) + 1, 0);
+		segOff.assign((size_t(m_nDev) + 1) * B, 0);
+		d1Start.assign(size_t(m_nDev) + 1, 0);
+		fcm.resize(S);
+		fcmPos.resize(S);
+		synAt.resize(S);
 		/* cursor[b][s]: count, then next free offset within region b */
 		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
@@ -390,7 +441,10 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	std::vector<uint32_t> rcmSrcDelay, rcmForward;
 	std::vector<int32_t> rcmWeight;
 	uint64_t maxIn = 0;
-	if(m_stdpOn) {
+	if(m_stdpOn && onDevice) {
+		m_nrcm = dev.nrcm;
+		maxIn = dev.maxIn;
+	} else if(m_stdpOn) {
 		rcmStart.assign(size_t(m_nDev) + 1, 0);
 		for(size_t s = 0; s < S; ++s) if(net.plastic[s]) rcmStart[dtgt[s] + 1]++;
 		for(uint32_t n = 0; n < m_nDev; ++n) {
@@ -438,10 +492,6 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	}
 
 	/* ---- device ---- */
-	cudaStream_t stream;
-	NEMO_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-	m_stream = stream;
-
 	auto put = [&](const void* host, size_t bytes) -> void* {
 		void* d = alloc(bytes);
 		if(bytes) NEMO_CUDA(cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, stream));
@@ -461,11 +511,11 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.ownStart = (const uint32_t*) put(ownStart.data(), ownStart.size() * 4);
 	m_net.warpBase = warpLo;
 	m_net.smemAcc = smemAcc ? 1 : 0;
-	m_net.fcm = (uint2*) put(fcm.data(), fcm.size() * 8);
+	m_net.fcm = onDevice ? dev.fcm : (uint2*) put(fcm.data(), fcm.size() * 8);
 	m_net.regionBase = (const uint64_t*) put(regionBase.data(), regionBase.size() * 8);
-	m_net.segOff = (const uint32_t*) put(segOff.data(), segOff.size() * 4);
+	m_net.segOff = onDevice ? dev.segOff : (const uint32_t*) put(segOff.data(), segOff.size() * 4);
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
-	m_net.d1Start = (const uint32_t*) put(d1Start.data(), d1Start.size() * 4);
+	m_net.d1Start = onDevice ? dev.d1Start : (const uint32_t*) put(d1Start.data(), d1Start.size() * 4);
 	m_net.d1Base = regionBase[B];
 	m_net.inbox = alloc(size_t(2) * m_nDev * (acc32 ? 8 : 16));
 	m_net.acc = alloc(size_t(slots) * m_nDev * (acc32 ? 8 : 16));
@@ -491,10 +541,17 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
-		m_net.rcmStart = (const uint32_t*) put(rcmStart.data(), rcmStart.size() * 4);
-		m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
-		m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
-		m_net.rcmWeight = (int32_t*) put(rcmWeight.data(), rcmWeight.size() * 4);
+		if(onDevice) {
+			m_net.rcmStart = dev.rcmStart;
+			m_net.rcmSrcDelay = dev.rcmSrcDelay;
+			m_net.rcmForward = dev.rcmForward;
+			m_net.rcmWeight = dev.rcmWeight;
+		} else {
+			m_net.rcmStart = (const uint32_t*) put(rcmStart.data(), rcmStart.size() * 4);
+			m_net.rcmSrcDelay = (const uint32_t*) put(rcmSrcDelay.data(), rcmSrcDelay.size() * 4);
+			m_net.rcmForward = (const uint32_t*) put(rcmForward.data(), rcmForward.size() * 4);
+			m_net.rcmWeight = (int32_t*) put(rcmWeight.data(), rcmWeight.size() * 4);
+		}
 		m_net.rcmAcc = (int32_t*) alloc(size_t(m_nrcm) * 4);
 	}
 
