@@ -362,3 +362,21 @@ def test_build_plugin_places_and_rebuilds(tmp_path):
     assert os.path.getmtime(out) > t0
     other = nb_build.build_plugin(str(src), name="Renamed", plugin_dir=str(tmp_path / "elsewhere"))
     assert other == str(tmp_path / "elsewhere" / "b200" / "libRenamed.so") and os.path.exists(other)
+
+
+def test_plugin_batch_layout(tmp_path):
+    """The binary layout of b200_neuron_batch on LP64 (the plugin ABI): field
+    offsets and size as compiled plugins see them, from a C compiler."""
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include <nemo_b200_plugin.h>\n'
+                   '#define F(x) printf("%s %zu\\n", #x, offsetof(b200_neuron_batch, x));\n'
+                   'int main(void) { F(count) F(cycle) F(param) F(param_stride) F(state) F(state_stride)\n'
+                   ' F(current_epsp) F(current_ipsp) F(current_external) F(fstim) F(recent_firing) F(fired) F(rng)\n'
+                   ' printf("size %zu\\n", sizeof(b200_neuron_batch)); return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = dict(line.split() for line in subprocess.check_output([str(exe)], text=True).splitlines())
+    expected = {"count": 0, "cycle": 8, "param": 16, "param_stride": 24, "state": 32, "state_stride": 40,
+                "current_epsp": 48, "current_ipsp": 56, "current_external": 64, "fstim": 72,
+                "recent_firing": 80, "fired": 88, "rng": 96, "size": 104}
+    assert {k: int(v) for k, v in got.items()} == expected
