@@ -140,6 +140,18 @@ def run_oracle_steps(wl, warmup, steps, budget_s=None):
     return events / total, done, total, build_s
 
 
+def cpu_model():
+    """The host CPU's model name (stated beside every CPU figure)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def oracle_library():
     path = os.path.join(ROOT, "oracle", "_build", "libnemo_oracle.so")
     if not os.path.exists(path):
@@ -392,7 +404,7 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         del sim
         v, nsteps, secs, o_build = run_oracle_steps(wl, 0, args.cpu_steps, budget_s=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+        line["cpu_baseline"] = {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "cpu_model": cpu_model(), "kind": "port",
                                 "sample": "%d step(s) of 100 cycles + applyStdp from a fresh network, %.1f s, "
                                           "e2e protocol" % (nsteps, secs),
                                 "build_s": round(o_build, 2)}
@@ -416,7 +428,7 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/int64 fixed point + f32/f64 state", "data": "synthetic (seeded generator)",
         "config": bench_config(wl, 1),
-        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+        "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": os.cpu_count(), "cpu_model": cpu_model(), "kind": "port",
                          "sample": "%d step(s) of 100 cycles + applyStdp after %d warm-up step(s)"
                                    % (nsteps, args.warmup)},
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -643,7 +655,7 @@ def run_bptt(args):
         secs = time.perf_counter() - c0
         scale = (steps / t_s) * (trials / b_s)
         line["cpu_baseline"] = {"value": round(1.0 / (secs * scale), 8), "unit": "grad steps/s",
-                                "cores": torch.get_num_threads(), "kind": "port",
+                                "cores": torch.get_num_threads(), "cpu_model": cpu_model(), "kind": "port",
                                 "sample": "float64 PyTorch reference (autograd, surrogate gradient), %d of %d trials x "
                                           "%d of %d steps in %.2f s, scaled linearly to the full grad step"
                                           % (b_s, trials, t_s, steps, secs)}
@@ -782,7 +794,7 @@ def run_mixed(args):
         osecs = sum(p[0] for p in oper)
         oev = sum(p[1] for p in oper)
         gsecs = sum(p[0] for p in per[:k])
-        line["cpu_baseline"] = {"value": round(oev / osecs, 1), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+        line["cpu_baseline"] = {"value": round(oev / osecs, 1), "unit": UNIT, "cores": os.cpu_count(), "cpu_model": cpu_model(), "kind": "port",
                                 "sample": "first %d cycles of the same run, %.1f s" % (k, osecs),
                                 "sim_ms_per_wall_s": round(k / osecs, 3),
                                 "gpu_same_cycles": round(oev / gsecs, 1),

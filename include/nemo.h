@@ -144,21 +144,6 @@ nemo_status_t nemo_reset_timer(nemo_simulation_t);
 
 const char* nemo_strerror(void);
 
-/* ---- Bulk construction (no counterpart in the reference C ABI; they are the
- * C form of the vector overloads of the reference Python binding,
- * src/api/python/nemo_py.cpp:733-806). Semantics are exactly those of calling
- * nemo_add_neuron / nemo_add_synapse once per element, in array order; on an
- * error the elements before the failing one stay added. ---- */
-
-/* args is row-major: count rows of nargs floats (parameters, then state). */
-nemo_status_t nemo_add_neurons(nemo_network_t, unsigned type, size_t count,
-		const unsigned idx[], unsigned nargs, const float args[]);
-
-/* plastic may be NULL (all static); ids may be NULL. */
-nemo_status_t nemo_add_synapses(nemo_network_t, size_t count,
-		const unsigned source[], const unsigned target[], const unsigned delay[],
-		const float weight[], const unsigned char plastic[], synapse_id ids[]);
-
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,21 @@ typedef struct b200_neuron_batch {
 	uint32_t* rng;
 } b200_neuron_batch;
 
+/* The binary layout of b200_neuron_batch and of the calls below. Every
+ * source that includes this header defines `b200_plugin_abi_version` (a weak,
+ * exported constant; define NEMO_B200_PLUGIN_HOST before the include to leave
+ * it out), so a plugin carries the layout it was compiled against, and the
+ * simulation refuses a plugin whose version is missing or differs from its
+ * own with NEMO_DL_ERROR instead of running it with wrong field offsets. */
+#define NEMO_B200_PLUGIN_ABI_VERSION 1u
+
+#if !defined(NEMO_B200_PLUGIN_HOST)
+#ifdef __cplusplus
+extern   /* a const at namespace scope has internal linkage in C++ otherwise */
+#endif
+__attribute__((weak, visibility("default"))) const unsigned b200_plugin_abi_version = NEMO_B200_PLUGIN_ABI_VERSION;
+#endif
+
 /* Update one population for one cycle. `stream` is the simulation's
  * cudaStream_t. Returns 0 (cudaSuccess) or a CUDA error code, which the
  * simulation reports as NEMO_CUDA_INVOCATION_ERROR. Exported by the plugin

@@ -1086,18 +1086,22 @@ k_stimulus(NetDev net, StimDev s)
 /* Stimulus of the allocation-free step, read from the per-device scratch
  * below: [0, nf) firing-stimulus device indices, [NOALLOC_STIM_MAX,
  * +ni) current-stimulus device indices, [2 NOALLOC_STIM_MAX, +ni) their
- * currents (float bits). One warp walks the current stimulus in order, 32
- * entries at a time; of equal indices within a group the highest lane writes,
- * and __syncwarp orders the groups, so the last entry for a neuron wins as in
- * the reference (cpu/Simulation.cpp:140-163). */
+ * currents (float bits). The firing stimulus is one entry per thread of the
+ * grid (bit sets commute). The current stimulus is walked in order by the
+ * first warp of block 0, 32 entries at a time; of equal indices within a
+ * group the highest lane writes, and __syncwarp orders the groups, so the
+ * last entry for a neuron wins as in the reference (cpu/Simulation.cpp:
+ * 140-163). */
 __global__ void
 k_stimulus_scratch(NetDev net, const uint32_t* scratch, uint32_t nf, uint32_t ni)
 {
-	const uint32_t lane = threadIdx.x;
-	for(uint32_t i = lane; i < nf; i += 32) {
-		uint32_t n = scratch[i];
+	const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+	if(g < nf) {
+		const uint32_t n = scratch[g];
 		atomicOr(&net.fstim[n >> 5], 1u << (n & 31u));
 	}
+	if(blockIdx.x != 0 || threadIdx.x >= 32u) return;
+	const uint32_t lane = threadIdx.x;
 	const uint32_t* idx = scratch + NOALLOC_STIM_MAX;
 	const float* cur = reinterpret_cast<const float*>(scratch + 2 * NOALLOC_STIM_MAX);
 	for(uint32_t base = 0; base < ni; base += 32) {
@@ -1369,7 +1373,8 @@ void
 launchStimulusScratch(const NetDev& net, const uint32_t* scratch, uint32_t nf, uint32_t ni, void* stream)
 {
 	if(nf + ni == 0) return;
-	k_stimulus_scratch<<<1, 32, 0, S(stream)>>>(net, scratch, nf, ni);
+	const uint32_t blocks = std::max<uint32_t>(1u, (nf + 255u) / 256u);
+	k_stimulus_scratch<<<blocks, 256, 0, S(stream)>>>(net, scratch, nf, ni);
 }
 
 /* The step kernel's plan: one 1024-thread block per SM (its registers allow

@@ -5,6 +5,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 
 #include "common.hpp"
 
@@ -34,6 +35,16 @@ loadB200Plugin(const std::string& path)
 	if(p->update == nullptr) {
 		dlclose(h);
 		fail(NEMO_INVALID_INPUT, "Neuron model plugin " + path + " does not export b200_update_neurons");
+	}
+	/* a plugin compiled against another layout of the batch would read
+	 * the wrong fields */
+	const unsigned* abi = reinterpret_cast<const unsigned*>(dlsym(h, "b200_plugin_abi_version"));
+	if(abi == nullptr || *abi != NEMO_B200_PLUGIN_ABI_VERSION) {
+		const std::string got = abi == nullptr ? std::string("no b200_plugin_abi_version") : std::to_string(*abi);
+		dlclose(h);
+		fail(NEMO_DL_ERROR, "Neuron model plugin " + path + " was built for plugin ABI version " + got
+				+ "; this library expects version " + std::to_string(NEMO_B200_PLUGIN_ABI_VERSION)
+				+ " (rebuild it against include/nemo_b200_plugin.h)");
 	}
 	const B200Plugin& ref = *p;
 	g_plugins.emplace(path, std::move(p));

@@ -7,6 +7,8 @@
 
 #include <string>
 
+/* the library reads plugins' layout version; it defines none of its own */
+#define NEMO_B200_PLUGIN_HOST
 #include <nemo_b200_plugin.h>
 
 namespace nemo_b200 {
@@ -18,8 +20,10 @@ struct B200Plugin {
 };
 
 /* The plugin at `path`, opened once per process and kept open. Fails with
- * NEMO_DL_ERROR when it cannot be opened and NEMO_INVALID_INPUT when it does
- * not export b200_update_neurons. */
+ * NEMO_DL_ERROR when it cannot be opened, NEMO_INVALID_INPUT when it does
+ * not export b200_update_neurons, and NEMO_DL_ERROR when its
+ * b200_plugin_abi_version is missing or is not NEMO_B200_PLUGIN_ABI_VERSION
+ * (a plugin compiled against another layout of b200_neuron_batch). */
 const B200Plugin& loadB200Plugin(const std::string& path);
 
 } // namespace nemo_b200

@@ -777,15 +777,25 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 	cudaStream_t stream = STREAM(m_stream);
 	size_t need = nf + ni;
 	if(need > m_stimCap) {
+		/* the old buffers go first; a failed allocation leaves the ones
+		 * not yet made null and the capacity 0, so that the next call
+		 * allocates again and release() frees only what exists */
+		cudaStreamSynchronize(stream);
 		if(m_hStim) cudaFreeHost(m_hStim);
 		if(m_hCur) cudaFreeHost(m_hCur);
 		if(m_dStim) cudaFree(m_dStim);
 		if(m_dCur) cudaFree(m_dCur);
-		m_stimCap = std::max<size_t>(need, 1024);
-		NEMO_CUDA(cudaMallocHost((void**) &m_hStim, m_stimCap * 4));
-		NEMO_CUDA(cudaMallocHost((void**) &m_hCur, m_stimCap * 4));
-		NEMO_CUDA(cudaMalloc((void**) &m_dStim, m_stimCap * 4));
-		NEMO_CUDA(cudaMalloc((void**) &m_dCur, m_stimCap * 4));
+		m_hStim = nullptr;
+		m_hCur = nullptr;
+		m_dStim = nullptr;
+		m_dCur = nullptr;
+		m_stimCap = 0;
+		const size_t cap = std::max<size_t>(need, 1024);
+		NEMO_CUDA(cudaMallocHost((void**) &m_hStim, cap * 4));
+		NEMO_CUDA(cudaMallocHost((void**) &m_hCur, cap * 4));
+		NEMO_CUDA(cudaMalloc((void**) &m_dStim, cap * 4));
+		NEMO_CUDA(cudaMalloc((void**) &m_dCur, cap * 4));
+		m_stimCap = cap;
 	}
 	uint32_t nfOk = 0, niOk = 0;
 	int err = 0;

@@ -5,6 +5,11 @@
  * semantics, step() helper order). */
 
 #include <nemo.h>
+/* the bulk construction calls (nemo_add_neurons / nemo_add_synapses) and the
+ * bulk weight read are declared with the B200 library's extensions; the
+ * oracle defines them too, so that a network file builds through the same
+ * calls on both libraries and the tests read weights the same way */
+#include <nemo_b200.h>
 
 #include <cstring>
 #include <string>

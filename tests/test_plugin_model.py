@@ -113,6 +113,31 @@ def test_plugin_without_update_symbol_is_rejected(tmp_path):
     assert "b200_update_neurons" in msg
 
 
+@pytest.mark.parametrize("version", [None, 0, 99])
+def test_plugin_of_another_abi_version_is_rejected(tmp_path, version):
+    """A plugin library whose b200_plugin_abi_version is missing (built
+    against an older header) or differs from the library's: refused with
+    NEMO_DL_ERROR before anything runs, so that no kernel reads the batch
+    with wrong field offsets."""
+    name = "Abi%s" % ("None" if version is None else version)
+    (tmp_path / ("%s.ini" % name)).write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
+    (tmp_path / "b200").mkdir()
+    src = tmp_path / "abi.c"
+    body = "int b200_update_neurons(const void* b, void* s) { return 0; }\n"
+    if version is not None:
+        body += "const unsigned b200_plugin_abi_version = %du;\n" % version
+    src.write_text(body)
+    subprocess.check_call(["gcc", "-shared", "-fPIC", "-o", str(tmp_path / "b200" / ("lib%s.so" % name)), str(src)])
+    status, msg = _simulation_status(Library(), name, str(tmp_path))
+    assert status == NEMO_DL_ERROR, msg
+    assert "ABI version" in msg
+
+
+def test_plugin_built_from_the_header_carries_its_abi_version(plugin_lib):
+    so = ctypes.CDLL(os.path.join(PLUGIN_DIR, "b200", "libQIFPlugin.so"))
+    assert ctypes.c_uint.in_dll(so, "b200_plugin_abi_version").value == 1
+
+
 def test_plugin_that_cannot_load_is_a_dl_error(tmp_path):
     (tmp_path / "Broken.ini").write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
     (tmp_path / "b200").mkdir()

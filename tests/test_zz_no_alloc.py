@@ -164,3 +164,27 @@ def test_noalloc_with_plugin_model():
     for i in range(400, 700, 7):
         assert np.float32(a.get_membrane_potential(i)).view(np.uint32) == \
             np.float32(b.get_membrane_potential(i)).view(np.uint32), i
+
+
+def test_noalloc_step_allocates_nothing():
+    """The promise itself: once a first call at the size limit has set up
+    the scratch, further calls (at the limit, short, empty) leave the
+    device's free memory unchanged -- the entry point grows no staging buffer
+    and allocates nothing else."""
+    import torch
+    torch.cuda.mem_get_info()   # torch's own context set-up happens before the count
+    lib, spec, ref, sut = _sims(n=2000, m=50, seed=11)
+    n = spec.neuron_count
+    na = NoAlloc(lib, sut, n)
+    full = np.arange(STIM_MAX, dtype=np.uint32) % n
+    istim = [(int(i), 1.5) for i in full]
+    na.step(full, istim)
+    na.step()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for k in range(4):
+        na.step(full[k:], istim[:STIM_MAX - 3 * k])
+        na.step()
+        na.step(full[:10], istim[:7])
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
