@@ -257,6 +257,34 @@ def load_traffic(kernel, workload_name):
     return None
 
 
+def parity_check(wl, cycles_before=100, cycles_after=50):
+    """The headline workload on a fresh B200 simulation and a fresh oracle
+    simulation: `cycles_before` cycles in one device-resident launch (the
+    timed path), applyStdp(1.0), `cycles_after` more; the fired list of every
+    cycle compared. The firing after the apply depends on every weight the
+    apply changed."""
+    lib = Library()
+    sim, _, _ = build_sim(lib, wl)
+    osim, _, _ = build_sim(Library(oracle_library()), wl, oracle=True)
+    bad = firings = 0
+    cycle = 0
+    for block in (cycles_before, cycles_after):
+        lib.dll.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p]
+        lib.call("nemo_b200_run", sim.handle, block, None, None)
+        for k in range(block):
+            want = osim.step()
+            got = sim.fired_at(cycle + k)
+            bad += 0 if np.array_equal(got, want) else 1
+            firings += want.size
+        cycle += block
+        if block == cycles_before:
+            sim.apply_stdp(REWARD)
+            osim.apply_stdp(REWARD)
+    return {"cycles_checked": cycle, "applies": 1, "mismatched_cycles": bad, "firings": firings,
+            "against": "oracle (reference CPU backend restated), fired list of every cycle",
+            "path": "device-resident launches, as timed"}
+
+
 def roofline(sim, lib, wl):
     """Device times of one step's two kernels — the persistent step kernel
     (100 cycles of update, spike push and STDP accumulation) and applyStdp —
@@ -365,9 +393,10 @@ def run_b200(args):
         ms_max, events_all = ms, events
     value = events_all / (ms_max * 1e-3)
 
-    # end to end through the C ABI (host buffers, per-cycle copies)
-    e2e_s, e2e_fired = e2e_steps(sim, n, max(1, min(args.steps, 3)), seed=11)
-    e2e_steps_n = max(1, min(args.steps, 3))
+    # end to end through the C ABI (host buffers, per-cycle copies), the
+    # same number of steps as the device-timed loop
+    e2e_steps_n = max(1, args.steps)
+    e2e_s, e2e_fired = e2e_steps(sim, n, e2e_steps_n, seed=11)
     e2e_value = e2e_fired * m / e2e_s
     nwords = (n + 31) // 32
 
@@ -408,6 +437,8 @@ def run_b200(args):
                                 "sample": "%d step(s) of 100 cycles + applyStdp from a fresh network, %.1f s, "
                                           "e2e protocol" % (nsteps, secs),
                                 "build_s": round(o_build, 2)}
+    if rank == 0 and world == 1 and not args.no_parity:
+        line["parity"] = parity_check(wl)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -886,6 +917,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--small", action="store_true", help="20k-neuron variant (profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison of the headline workload")
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--batched", action="store_true",

@@ -29,6 +29,12 @@ nemo_status_t nemo_add_synapses(nemo_network_t, size_t count,
 		const unsigned source[], const unsigned target[], const unsigned delay[],
 		const float weight[], const unsigned char plastic[], synapse_id ids[]);
 
+/* The vector form of nemo_get_synapse_weight_s (src/nemo.h:478-486; no
+ * counterpart in the reference C ABI): weights[k] = the current weight of
+ * synapse ids[k], for k < count. Errors as the single query: the first
+ * invalid id fails the call (the weights before it are written). */
+nemo_status_t nemo_b200_get_weights(nemo_simulation_t sim, const synapse_id ids[], size_t count, float weights[]);
+
 /* Run `cycles` cycles (<= 1024 per call) without stimulus, entirely on the
  * device in one persistent launch of the step kernel (spike gather, neuron
  * update and STDP accumulation per cycle, one grid barrier per cycle); a

@@ -352,6 +352,11 @@ nemo_status_t nemo_get_synapse_delay_n(nemo_network_t n, synapse_id id, unsigned
 nemo_status_t nemo_get_synapse_delay_s(nemo_simulation_t s, synapse_id id, unsigned* d) { RETURN_CALL(*d = s->sim.getSynapseDelay(id)); }
 nemo_status_t nemo_get_synapse_weight_n(nemo_network_t n, synapse_id id, float* w) { RETURN_CALL(*w = n->net.wgt[n->net.synapsePosition(id)]); }
 nemo_status_t nemo_get_synapse_weight_s(nemo_simulation_t s, synapse_id id, float* w) { RETURN_CALL(*w = s->sim.getSynapseWeight(id)); }
+nemo_status_t
+nemo_b200_get_weights(nemo_simulation_t s, const synapse_id ids[], size_t count, float weights[])
+{
+	RETURN_CALL(s->sim.getWeights(ids, count, weights));
+}
 nemo_status_t nemo_get_synapse_plastic_n(nemo_network_t n, synapse_id id, unsigned char* p) { RETURN_CALL(*p = n->net.plastic[n->net.synapsePosition(id)]); }
 nemo_status_t nemo_get_synapse_plastic_s(nemo_simulation_t s, synapse_id id, unsigned char* p) { RETURN_CALL(*p = s->sim.getSynapsePlastic(id)); }
 

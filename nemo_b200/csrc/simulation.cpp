@@ -1518,6 +1518,42 @@ Simulation::getSynapseWeight(synapse_id id)
 	return fixToFloat(int32_t(m_fcmHost[a.fcmPos].y), m_fbits);
 }
 
+/* getSynapseWeight over many ids: the per-source lookup is made once per run
+ * of ids from the same source */
+void
+Simulation::getWeights(const synapse_id* ids, size_t n, float* out)
+{
+	if(m_writeOnly) {
+		fail(NEMO_INVALID_INPUT, "Cannot read synapse state if simulation configured with write-only synapses");
+	}
+	if(!m_auxSid.empty()) {
+		for(size_t k = 0; k < n; ++k) out[k] = getSynapseWeight(ids[k]);
+		return;
+	}
+	if(n) (void) getSynapseWeight(ids[0]);   /* the host copy of the forward matrix */
+	bool have = false;
+	uint32_t last = 0;
+	size_t first = 0, count = 0;
+	for(size_t k = 0; k < n; ++k) {
+		const uint32_t neuron = uint32_t(ids[k] >> 32);
+		if(!have || neuron != last) {
+			auto it = m_auxRange.find(neuron);
+			if(it == m_auxRange.end()) {
+				fail(NEMO_INVALID_INPUT, "Non-existing neuron id (" + std::to_string(neuron) + ") in synapse query");
+			}
+			first = it->second.first;
+			count = it->second.second;
+			last = neuron;
+			have = true;
+		}
+		const uint32_t idx = uint32_t(ids[k] & 0xffffffffu);
+		if(idx >= count) {
+			throw std::out_of_range("synapse index out of range");
+		}
+		out[k] = fixToFloat(int32_t(m_fcmHost[m_aux[first + idx].fcmPos].y), m_fbits);
+	}
+}
+
 unsigned long
 Simulation::elapsedWallclock() const
 {

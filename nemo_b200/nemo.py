@@ -385,6 +385,37 @@ class Simulation:
     def get_synapse_plastic(self, sid):
         return _query(self.lib, "nemo_get_synapse_plastic_s", self.handle, sid, c_ubyte)
 
+    def run(self, cycles):
+        """Device-resident run of `cycles` cycles without stimulus
+        (nemo_b200_run); returns the fired count of each cycle."""
+        counts = np.zeros(cycles, dtype=np.uint32)
+        fn = self.lib.dll.nemo_b200_run
+        fn.argtypes = [c_void_p, c_uint, POINTER(ctypes.c_uint32), POINTER(c_uint64)]
+        self.lib.call("nemo_b200_run", self.handle, cycles, counts.ctypes.data_as(POINTER(ctypes.c_uint32)), None)
+        return counts
+
+    def fired_at(self, cycle):
+        """Fired neurons of one of the last 1024 cycles (nemo_b200_fired_at),
+        in nemo_step's order."""
+        ptr = POINTER(c_uint)()
+        n = c_size_t()
+        fn = self.lib.dll.nemo_b200_fired_at
+        fn.argtypes = [c_void_p, c_uint64, POINTER(POINTER(c_uint)), POINTER(c_size_t)]
+        self.lib.call("nemo_b200_fired_at", self.handle, cycle, byref(ptr), byref(n))
+        if n.value == 0:
+            return np.zeros(0, dtype=np.uint32)
+        return np.ctypeslib.as_array(ptr, shape=(n.value,)).astype(np.uint32)
+
+    def get_weights(self, ids):
+        """Weights of many synapses at once (nemo_b200_get_weights)."""
+        ids = np.ascontiguousarray(np.asarray(ids, dtype=np.uint64))
+        out = np.empty(ids.size, dtype=np.float32)
+        fn = self.lib.dll.nemo_b200_get_weights
+        fn.argtypes = [c_void_p, POINTER(c_uint64), c_size_t, POINTER(c_float)]
+        self.lib.call("nemo_b200_get_weights", self.handle, ids.ctypes.data_as(POINTER(c_uint64)), ids.size,
+                      out.ctypes.data_as(POINTER(c_float)))
+        return out
+
     def elapsed_wallclock(self):
         e = c_ulong()
         self.lib.call("nemo_elapsed_wallclock", self.handle, byref(e))

@@ -28,40 +28,57 @@ class _Spike(torch.autograd.Function):
         return g / (a * a), None, None, None
 
 
-def counts(net, w, in_spikes, trials, relaxed=False, spikes=None):
+def counts(net, w, in_spikes, trials, relaxed=False, spikes=None, segment=None):
     """Spike counts [trials][bins] in float64. w: float64 tensor (synapse
-    order of net); in_spikes: bool [T][C][trials]; spikes: bool [T][N][trials]
-    (exact mode; None: thresholds computed here)."""
+    order of net); in_spikes: bool [T][C][>= trials]; spikes: bool
+    [T][N][>= trials] (exact mode; None: thresholds computed here); only the
+    first `trials` trials are used. segment: recompute the steps of each
+    segment of this many steps in the backward pass instead of keeping them
+    (torch.utils.checkpoint), for networks whose per-step tensors do not all
+    fit in memory; the values are the same."""
+    import torch.utils.checkpoint as ckpt
     n, T = net.n, in_spikes.shape[0]
     pre = torch.as_tensor(net.pres)
     tgt = torch.as_tensor(net.targets)
-    rec = pre < n
-    inp = ~rec
+    rec = torch.nonzero(pre < n).flatten()
+    inp = torch.nonzero(pre >= n).flatten()
+    pre_rec, tgt_rec = pre[rec], tgt[rec]
+    pre_inp, tgt_inp = pre[inp] - n, tgt[inp]
     beta, theta, kappa = net.beta, net.theta, net.kappa
     B = trials
+
+    def run(t0, t1, w, v, s_prev):
+        """steps [t0, t1) from state (v, s_prev): the new state and the
+        population spike sums of each step [t1 - t0][B]"""
+        w_rec, w_inp = w[rec], w[inp]
+        sums = []
+        for t in range(t0, t1):
+            ins = torch.as_tensor(in_spikes[t][:, :trials].T.astype(np.float64))     # [B][C]
+            I = torch.zeros(B, n, dtype=torch.float64).index_add(1, tgt_rec, s_prev[:, pre_rec] * w_rec)
+            I = I.index_add(1, tgt_inp, ins[:, pre_inp] * w_inp)
+            u = beta * v + I
+            if relaxed:
+                d = u - theta
+                s = d / (1.0 + kappa * d.abs())
+            else:
+                given = (u >= theta).double() if spikes is None else \
+                    torch.as_tensor(spikes[t][:, :trials].T.astype(np.float64))
+                s = _Spike.apply(u, given, theta, kappa)
+            v = u - theta * s
+            sums.append(s.sum(1))
+            s_prev = s
+        return v, s_prev, torch.stack(sums)
+
     v = torch.zeros(B, n, dtype=torch.float64)
     s_prev = torch.zeros(B, n, dtype=torch.float64)
-    bins = T // net.bin_steps
-    out = []
-    acc = torch.zeros(B, dtype=torch.float64)
-    ins = torch.as_tensor(in_spikes[:, :, :trials].astype(np.float64))
-    for t in range(T):
-        x = torch.zeros(B, pre.numel(), dtype=torch.float64)
-        x[:, rec] = s_prev[:, pre[rec]]
-        x[:, inp] = ins[t][pre[inp] - n].T
-        I = torch.zeros(B, n, dtype=torch.float64).index_add(1, tgt, x * w)
-        u = beta * v + I
-        if relaxed:
-            d = u - theta
-            s = d / (1.0 + kappa * d.abs())
+    seg = T if segment is None else int(segment)
+    parts = []
+    for t0 in range(0, T, seg):
+        t1 = min(T, t0 + seg)
+        if segment is None:
+            v, s_prev, sums = run(t0, t1, w, v, s_prev)
         else:
-            given = (u >= theta).double() if spikes is None else \
-                torch.as_tensor(spikes[t].T.astype(np.float64))
-            s = _Spike.apply(u, given, theta, kappa)
-        v = u - theta * s
-        acc = acc + s.sum(1)
-        if (t + 1) % net.bin_steps == 0:
-            out.append(acc)
-            acc = torch.zeros(B, dtype=torch.float64)
-        s_prev = s
-    return torch.stack(out, 1)
+            v, s_prev, sums = ckpt.checkpoint(run, t0, t1, w, v, s_prev, use_reentrant=False)
+        parts.append(sums)
+    per_step = torch.cat(parts)                   # [T][B]
+    return per_step.reshape(T // net.bin_steps, net.bin_steps, B).sum(1).T

@@ -220,6 +220,7 @@ public:
 	unsigned getSynapseTarget(synapse_id id) const;
 	unsigned getSynapseDelay(synapse_id id) const;
 	float getSynapseWeight(synapse_id id) const;
+	void getWeights(const synapse_id* ids, size_t n, float* out) const;
 	unsigned char getSynapsePlastic(synapse_id id) const;
 
 	unsigned long elapsedWallclock() const;

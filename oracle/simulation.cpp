@@ -486,6 +486,35 @@ Simulation::getSynapseWeight(synapse_id id) const
 	return fx_toFloat(m_terminals[m_rowStart[addressOf(src, s.delay)] + s.idx].weight, m_fbits);
 }
 
+/* getSynapseWeight over many ids, with the per-source lookups made once per
+ * run of ids from the same source (the tests read every weight of large
+ * networks) */
+void
+Simulation::getWeights(const synapse_id* ids, size_t n, float* out) const
+{
+	bool have = false;
+	unsigned last = 0, src = 0;
+	size_t first = 0, count = 0;
+	for(size_t k = 0; k < n; ++k) {
+		const unsigned neuron = unsigned(ids[k] >> 32);
+		if(!have || neuron != last) {
+			(void) aux(ids[k] & ~uint64_t(0xffffffffu));   /* errors of the single query */
+			auto it = m_auxRange.find(neuron);
+			first = it->second.first;
+			count = it->second.second;
+			src = localIdx(neuron);
+			last = neuron;
+			have = true;
+		}
+		const size_t idx = size_t(ids[k] & 0xffffffffu);
+		if(idx >= count) {
+			throw std::out_of_range("synapse index out of range");
+		}
+		const Aux& a = m_aux[first + idx];
+		out[k] = fx_toFloat(m_terminals[m_rowStart[addressOf(src, a.delay)] + a.idx].weight, m_fbits);
+	}
+}
+
 unsigned char
 Simulation::getSynapsePlastic(synapse_id id) const
 {
