@@ -8,8 +8,13 @@
 2. The same runs against tests/golden/plugins.npz, which
    tests/golden/make_golden.py wrote from those compiled reference plugins, so
    the pin holds where the reference sources are absent.
-3. The fixed-point and RNG-seeding restatements against values derived from
-   their published definitions.
+3. The fixed-point conversions (fx_toFix, fx_toFloat, wfx_toFloat, fx_mul)
+   and the STDP process (potentiation/depression bits, weightChange,
+   updatedWeight) against the reference's own src/nemo/{fixedpoint,
+   StdpFunction,StdpProcess}.cpp compiled into oracle/_ref/libnemo_stdp_ref.so,
+   and against tests/golden/stdp_fixedpoint.npz written from that build.
+4. The RNG-seeding restatement against values derived from its published
+   definition.
 """
 
 import ctypes
@@ -19,7 +24,7 @@ import numpy as np
 import pytest
 
 from conftest import ORACLE_REF_DIR, ROOT, ensure_oracle
-from plugin_harness import MODELS, PIN_N, UPDATE_T, _Run, drive_inputs, pin_cycles, run_digest
+from plugin_harness import MODELS, PIN_N, UPDATE_T, _Run, drive_inputs, pin_cycles, pin_outputs, run_digest
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "plugins.npz")
 
@@ -65,6 +70,29 @@ def test_restated_update_matches_golden_vectors(model):
     assert np.array_equal(state.view(np.uint32), g[model + "/state"].view(np.uint32))
     assert np.array_equal(rf, g[model + "/rf"])
     assert np.array_equal(rng, g[model + "/rng"])
+
+
+def _compare_pins(mine, theirs):
+    assert set(mine) == set(theirs)
+    for key in sorted(mine):
+        bad = np.nonzero(np.asarray(mine[key]) != np.asarray(theirs[key]))[0]
+        assert bad.size == 0, "%s: %d of %d differ (first at %d)" % (key, bad.size, np.asarray(mine[key]).size, bad[0])
+
+
+def test_fixed_point_and_stdp_match_reference_sources():
+    path = os.path.join(ORACLE_REF_DIR, "libnemo_stdp_ref.so")
+    if not os.path.exists(path):
+        pytest.skip("reference sources were not available when oracle/_ref was built")
+    ours = pin_outputs(ctypes.CDLL(ensure_oracle()))
+    _compare_pins(ours, pin_outputs(ctypes.CDLL(path)))
+    # the inputs reach every branch: overflow, saturation, both windows
+    assert any(ours[k].any() for k in ours if k.startswith("to_fix_threw"))
+    assert any(np.any(ours[k] != 0) for k in ours if k.startswith("weight_change"))
+
+
+def test_fixed_point_and_stdp_match_golden_vectors():
+    g = np.load(os.path.join(ROOT, "tests", "golden", "stdp_fixedpoint.npz"))
+    _compare_pins(pin_outputs(ctypes.CDLL(ensure_oracle())), {k: g[k] for k in g.files})
 
 
 def test_rng_seeds_follow_mt19937():
