@@ -291,14 +291,17 @@ def roofline(sim, lib, wl):
     and the dominant one's algorithmic bytes / time against the measured HBM
     copy bandwidth. Algorithmic bytes: spike push 8 B per pushed synapse
     (packed target/delay + i32 weight); Izhikevich update 92 B per neuron per
-    cycle; STDP accumulation 20 B per visited synapse; applyStdp 20 B per
-    plastic synapse."""
-    out = (ctypes.c_double * 10)()
-    lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 10]
+    cycle; STDP accumulation 4 B per visited synapse (its source/delay word)
+    plus 12 B per visit whose source fired in the last 64 cycles (the 8 B
+    source history and the 4 B accumulator; for the others the kernel's
+    recent-firing bitmap shows that the change is 0) plus 4 B per
+    accumulator written; applyStdp 20 B per plastic synapse."""
+    out = (ctypes.c_double * 12)()
+    lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 12]
     lib.call("nemo_b200_profile", sim.handle, CYCLES_PER_STEP, ctypes.c_float(REWARD), out)
-    tcyc, blocks, _, pushed, fired, visits, updates, tapply, nplastic, generated = list(out)
+    tcyc, blocks, _, pushed, fired, visits, updates, tapply, nplastic, generated, hist, accw = list(out)
     kernels = {
-        "k_cycles": (8.0 * pushed + 92.0 * updates + 20.0 * visits, tcyc, 1),
+        "k_cycles": (8.0 * pushed + 92.0 * updates + 4.0 * visits + 12.0 * hist + 4.0 * accw, tcyc, 1),
         "k_apply_stdp": (20.0 * nplastic, tapply, 1),
     }
     peak, peak_kind = measured_peaks()
@@ -318,7 +321,8 @@ def roofline(sim, lib, wl):
             "per_kernel": {k: {kk: (round(vv, 5) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                            for k, v in table.items()},
             "work_per_step": {"cycles": CYCLES_PER_STEP, "pushed_synapses": int(pushed), "fired": int(fired),
-                              "stdp_visits": int(visits), "neuron_updates": int(updates),
+                              "stdp_visits": int(visits), "stdp_history_reads": int(hist),
+                              "stdp_accumulator_writes": int(accw), "neuron_updates": int(updates),
                               "plastic_synapses": int(nplastic), "grid_blocks": int(blocks)}}
     return roof
 
@@ -909,6 +913,25 @@ def run_sharded(args):
         dist.destroy_process_group()
 
 
+def run_ncu_case(args):
+    """A bounded case for ncu: the workload (--small: the 20k-neuron one)
+    built, --warmup steps of 100 cycles + applyStdp, then --steps more, all
+    through nemo_b200_timed_steps; k_cycles launches: warmup + steps, each
+    followed by the applyStdp launches. Prints the device time of the last
+    steps."""
+    wl = workload(args.small)
+    lib = Library()
+    sim, _, build_s = build_sim(lib, wl)
+    lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                              ctypes.c_float, ctypes.c_double * 4]
+    out = (ctypes.c_double * 4)()
+    lib.call("nemo_b200_timed_steps", sim.handle, max(args.warmup, 1), CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
+    lib.call("nemo_b200_timed_steps", sim.handle, max(args.steps, 1), CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
+    print(json.dumps({"case": wl["name"], "steps": max(args.steps, 1), "warmup": max(args.warmup, 1),
+                      "ms_per_step": round(out[0] / max(args.steps, 1), 4), "build_s": round(build_s, 2),
+                      "apply_launches_per_step": apply_launches(sim, lib)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -932,8 +955,12 @@ def main():
     ap.add_argument("--mixed", action="store_true",
                     help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
     ap.add_argument("--mixed-cycles", type=int, default=1000)
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="a bounded run of the headline (or --small) workload for ncu captures")
     args = ap.parse_args()
-    if args.random1k:
+    if args.ncu_case:
+        run_ncu_case(args)
+    elif args.random1k:
         run_random1k(args)
     elif args.sharded:
         run_sharded(args)

@@ -167,6 +167,37 @@ nemo_status_t nemo_b200_shard_step(nemo_simulation_t sim, unsigned fstim_nidx[],
 nemo_status_t nemo_b200_shard_deliver(nemo_simulation_t sim, const uint32_t all_words[], unsigned* fired[],
 		size_t* fired_count);
 
+/* The same cycle with the fired words kept in device memory, for an exchange
+ * by a collective on the GPUs (NCCL over NVLink) instead of through host
+ * memory. Nothing waits on the host:
+ *
+ *   nemo_b200_shard_step_async     queues the stimulus, the update and a
+ *                                  copy of the shard's own words (`words`
+ *                                  of shard_range) into local_words_dev
+ *                                  (device memory), and makes `stream` (a
+ *                                  cudaStream_t; NULL: the legacy default
+ *                                  stream) wait for that copy;
+ *   (the caller all-gathers the words into all_words_dev on `stream`)
+ *   nemo_b200_shard_deliver_async  makes the simulation wait for the work
+ *                                  queued on `stream` so far, then brings
+ *                                  the other shards' firing in from
+ *                                  all_words_dev (device, total_words).
+ *
+ * Both buffers must stay allocated until the simulation's work that reads
+ * them has run (nemo_b200_stream_wait orders a stream after it). The cycle's
+ * fired neurons are read with nemo_b200_fired_at. No counterpart in the
+ * reference (the MPI worker exchanges through host messages,
+ * src/mpi/Worker.cpp:265-292). */
+nemo_status_t nemo_b200_shard_step_async(nemo_simulation_t sim, const unsigned fstim_nidx[], size_t fstim_count,
+		const unsigned istim_nidx[], const float istim_current[], size_t istim_count, uint32_t* local_words_dev,
+		void* stream);
+nemo_status_t nemo_b200_shard_deliver_async(nemo_simulation_t sim, const uint32_t* all_words_dev, void* stream);
+
+/* Make `stream` (a cudaStream_t; NULL: the legacy default stream) wait for
+ * every piece of work queued on the simulation so far, without waiting on the
+ * host. */
+nemo_status_t nemo_b200_stream_wait(nemo_simulation_t sim, void* stream);
+
 /* Number of networks of a batch (1 for an ordinary simulation). */
 nemo_status_t nemo_b200_batch_instances(nemo_simulation_t sim, size_t* count);
 
@@ -255,8 +286,10 @@ nemo_status_t nemo_b200_timed_steps(nemo_simulation_t sim, unsigned steps, unsig
  * simulated). out[0] = step-kernel ms, out[1] = its grid blocks, out[2] = 0,
  * out[3] = synapses pushed, out[4] = neurons fired, out[5] = STDP synapse
  * visits, out[6] = neuron updates, out[7] = applyStdp ms, out[8] = plastic
- * synapses, out[9] = synaptic events generated. */
-nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[10]);
+ * synapses, out[9] = synaptic events generated, out[10] = STDP visits that
+ * read the source's firing history (the others' sources fired in none of the
+ * last 64 cycles), out[11] = STDP accumulators written. */
+nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[12]);
 
 /* Phase timing of the step kernel over `cycles` cycles (one traced launch;
  * the cycles are simulated). Means over cycles, in ns: out[0] whole phase,

@@ -2,12 +2,13 @@
  * (CUB) reproduce the constructor's host counting sorts exactly.
  *
  * Forward matrix. Each synapse gets the key of its bucket: a delay >= 2
- * synapse goes to (owner block of its target) x nDev + source, a delay-1
- * synapse to blocks x nDev + source, after every region. A stable sort of
- * (key, insertion index) puts the synapses in forward order: by region, in a
- * region by source, in a segment by insertion order, as the host fills them.
- * The exclusive sum of the bucket counts gives the regions' bases, the
- * segments' offsets and the delay-1 starts.
+ * synapse whose target block b belongs to block group g goes to
+ * groupFirst[g] x nDev + source x blocks(g) + (b - groupFirst[g]), a delay-1
+ * synapse to blocks x nDev + source, after every group. A stable sort of
+ * (key, insertion index) puts the synapses in forward order: by group, in a
+ * group by source, for a source by block, in a bucket by insertion order, as
+ * the host fills them. The exclusive sum of the bucket counts gives the
+ * bucket starts and the delay-1 starts.
  *
  * Reverse matrix. Walking the forward order, a plastic synapse gets the key
  * of its target and any other the key nDev (after all targets); a stable sort
@@ -62,8 +63,9 @@ bitsFor(uint64_t x)
 }
 
 __global__ void
-k_forward_keys(size_t S, uint32_t nDev, uint32_t B, uint32_t warpLo, uint32_t ownedWarps,
+k_forward_keys(size_t S, uint32_t nDev, uint32_t B, uint32_t warpLo, uint32_t ownedWarps, uint32_t G,
 		const uint32_t* src, const uint32_t* tgt, const uint32_t* dly, const uint32_t* ownerOfWarp,
+		const uint32_t* groupFirst, const uint32_t* groupOf,
 		unsigned long long* key, uint32_t* val, uint32_t* cnt, uint32_t* bad)
 {
 	for(size_t s = blockIdx.x * size_t(blockDim.x) + threadIdx.x; s < S; s += size_t(gridDim.x) * blockDim.x) {
@@ -77,7 +79,11 @@ k_forward_keys(size_t S, uint32_t nDev, uint32_t B, uint32_t warpLo, uint32_t ow
 			ok = tw >= warpLo && tw - warpLo < ownedWarps;
 			const uint32_t b = ok ? ownerOfWarp[tw - warpLo] : 0u;
 			ok = ok && b < B;
-			k = (unsigned long long) b * nDev + a;
+			const uint32_t g = ok ? groupOf[b] : 0u;
+			ok = ok && g < G;
+			const uint32_t g0 = ok ? groupFirst[g] : 0u, g1 = ok ? groupFirst[g + 1] : 1u;
+			ok = ok && g0 <= b && b < g1 && g1 <= B;
+			k = ok ? (unsigned long long) g0 * nDev + (unsigned long long) a * (g1 - g0) + (b - g0) : 0ull;
 		}
 		if(ok) {
 			atomicAdd(&cnt[k], 1u);
@@ -105,23 +111,15 @@ k_forward_fill(size_t S, const uint32_t* synAt, const uint32_t* tgt, const uint3
 	}
 }
 
-/* start: exclusive sum of the bucket counts, B x nDev + nDev + 1 entries */
+/* start: exclusive sum of the bucket counts, B x nDev + nDev + 1 entries:
+ * the first B x nDev + 1 are the bucket starts, the rest (less the first
+ * delay-1 position) the delay-1 starts */
 __global__ void
-k_forward_offsets(const uint32_t* start, uint32_t nDev, uint32_t B, uint32_t* segOff, uint32_t* d1Start,
-		unsigned long long* regionBase)
+k_forward_offsets(const uint32_t* start, uint32_t nDev, uint32_t B, uint32_t* d1Start)
 {
-	const size_t row = size_t(nDev) + 1;
-	const size_t total = (size_t(B) + 1) * row;
-	for(size_t x = blockIdx.x * size_t(blockDim.x) + threadIdx.x; x < total; x += size_t(gridDim.x) * blockDim.x) {
-		const uint32_t b = uint32_t(x / row), a = uint32_t(x - size_t(b) * row);
-		const uint32_t base = start[size_t(b) * nDev];
-		const uint32_t v = start[size_t(b) * nDev + a] - base;
-		if(b < B) {
-			segOff[x] = v;
-		} else {
-			d1Start[a] = v;
-		}
-		if(a == 0u) regionBase[b] = base;
+	const size_t base = size_t(B) * nDev;
+	for(size_t a = blockIdx.x * size_t(blockDim.x) + threadIdx.x; a <= nDev; a += size_t(gridDim.x) * blockDim.x) {
+		d1Start[a] = start[base + a] - start[base];
 	}
 }
 
@@ -174,7 +172,8 @@ buildLayoutOnDevice(const LayoutIn& in, const std::function<void*(size_t)>& keep
 
 	/* inputs */
 	Temp src(S * 4, st), tgt(S * 4, st), wfx(S * 4, st), dly(S * 4, st), plastic(S, st),
-		owner(size_t(in.ownedWarps) * 4, st), bad(4, st);
+		owner(size_t(in.ownedWarps) * 4, st), bad(4, st), gFirst((size_t(in.groups) + 1) * 4, st),
+		gOf(size_t(B) * 4, st);
 	NEMO_CUDA(cudaMemcpyAsync(src.p, in.src, S * 4, cudaMemcpyHostToDevice, st));
 	NEMO_CUDA(cudaMemcpyAsync(tgt.p, in.tgt, S * 4, cudaMemcpyHostToDevice, st));
 	NEMO_CUDA(cudaMemcpyAsync(wfx.p, in.wfx, S * 4, cudaMemcpyHostToDevice, st));
@@ -183,15 +182,17 @@ buildLayoutOnDevice(const LayoutIn& in, const std::function<void*(size_t)>& keep
 	if(in.ownedWarps) {
 		NEMO_CUDA(cudaMemcpyAsync(owner.p, in.ownerOfWarp, size_t(in.ownedWarps) * 4, cudaMemcpyHostToDevice, st));
 	}
+	NEMO_CUDA(cudaMemcpyAsync(gFirst.p, in.groupFirst, (size_t(in.groups) + 1) * 4, cudaMemcpyHostToDevice, st));
+	NEMO_CUDA(cudaMemcpyAsync(gOf.p, in.groupOf, size_t(B) * 4, cudaMemcpyHostToDevice, st));
 	NEMO_CUDA(cudaMemsetAsync(bad.p, 0, 4, st));
 
 	/* ---- forward matrix ---- */
 	Temp cnt(buckets * 4, st), start(buckets * 4, st);
 	NEMO_CUDA(cudaMemsetAsync(cnt.p, 0, buckets * 4, st));
 	Temp keyIn(S * 8, st), keyOut(S * 8, st), valIn(S * 4, st), synAt(S * 4, st);
-	k_forward_keys<<<gridFor(S), 256, 0, st>>>(S, nDev, B, in.warpLo, in.ownedWarps, src.as<uint32_t>(),
-			tgt.as<uint32_t>(), dly.as<uint32_t>(), owner.as<uint32_t>(), keyIn.as<unsigned long long>(),
-			valIn.as<uint32_t>(), cnt.as<uint32_t>(), bad.as<uint32_t>());
+	k_forward_keys<<<gridFor(S), 256, 0, st>>>(S, nDev, B, in.warpLo, in.ownedWarps, in.groups, src.as<uint32_t>(),
+			tgt.as<uint32_t>(), dly.as<uint32_t>(), owner.as<uint32_t>(), gFirst.as<uint32_t>(), gOf.as<uint32_t>(),
+			keyIn.as<unsigned long long>(), valIn.as<uint32_t>(), cnt.as<uint32_t>(), bad.as<uint32_t>());
 	NEMO_CUDA(cudaGetLastError());
 	{
 		size_t bytes = 0;
@@ -209,21 +210,21 @@ buildLayoutOnDevice(const LayoutIn& in, const std::function<void*(size_t)>& keep
 		NEMO_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, bytes, cnt.as<uint32_t>(), start.as<uint32_t>(), buckets, st));
 	}
 	out->fcm = static_cast<uint2*>(keep(S * 8));
-	out->segOff = static_cast<uint32_t*>(keep(size_t(B) * (size_t(nDev) + 1) * 4));
+	const size_t segEntries = size_t(B) * nDev + 1;
+	out->segOff = static_cast<uint32_t*>(keep(segEntries * 4));
 	out->d1Start = static_cast<uint32_t*>(keep((size_t(nDev) + 1) * 4));
-	Temp regionBase((size_t(B) + 1) * 8, st);
 	Temp fcmPos(in.wantFcmPos ? S * 4 : 16, st);
 	k_forward_fill<<<gridFor(S), 256, 0, st>>>(S, synAt.as<uint32_t>(), tgt.as<uint32_t>(), dly.as<uint32_t>(),
 			wfx.as<int32_t>(), out->fcm, in.wantFcmPos ? fcmPos.as<uint32_t>() : nullptr, bad.as<uint32_t>());
 	NEMO_CUDA(cudaGetLastError());
-	k_forward_offsets<<<gridFor((size_t(B) + 1) * (size_t(nDev) + 1)), 256, 0, st>>>(start.as<uint32_t>(), nDev, B,
-			out->segOff, out->d1Start, regionBase.as<unsigned long long>());
+	NEMO_CUDA(cudaMemcpyAsync(out->segOff, start.p, segEntries * 4, cudaMemcpyDeviceToDevice, st));
+	k_forward_offsets<<<gridFor(size_t(nDev) + 1), 256, 0, st>>>(start.as<uint32_t>(), nDev, B, out->d1Start);
 	NEMO_CUDA(cudaGetLastError());
-	uint32_t hBad = 0;
-	out->regionBase.assign(size_t(B) + 1, 0);
+	uint32_t hBad = 0, hD1 = 0;
 	NEMO_CUDA(cudaMemcpyAsync(&hBad, bad.p, 4, cudaMemcpyDeviceToHost, st));
-	NEMO_CUDA(cudaMemcpyAsync(out->regionBase.data(), regionBase.p, (size_t(B) + 1) * 8, cudaMemcpyDeviceToHost, st));
+	NEMO_CUDA(cudaMemcpyAsync(&hD1, start.as<uint32_t>() + size_t(B) * nDev, 4, cudaMemcpyDeviceToHost, st));
 	NEMO_CUDA(cudaStreamSynchronize(st));
+	out->d1Base = hD1;
 	if(hBad) {
 		fail(NEMO_LOGIC_ERROR, "device layout build: a synapse's neuron, delay or owner is out of range");
 	}

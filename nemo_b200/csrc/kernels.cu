@@ -38,12 +38,29 @@ __device__ __forceinline__ unsigned long long globalTimer()
 }
 
 /* wfx_toFloat: saturate the int64 sum to int32, convert, scale
- * (src/nemo/fixedpoint.cpp:40-49) */
+ * (src/nemo/fixedpoint.cpp:40-49). The reference divides by 2^f; the
+ * product with 2^-f is the same float (both are exact: the quotient of an
+ * integer-valued float of magnitude >= 1 by a power of two <= 2^31 is a
+ * normal float), and a multiplication has no slow path. */
 __device__ __forceinline__ float wfxToFloat(long long v, uint32_t fbits)
 {
 	v = v > 2147483647LL ? 2147483647LL : v;
 	v = v < -2147483648LL ? -2147483648LL : v;
-	return __fdiv_rn(__ll2float_rn(v), float(1u << fbits));
+	return __fmul_rn(__ll2float_rn(v), __int_as_float(int((127u - fbits) << 23)));
+}
+
+/* Bring the bytes [lo, hi) of global memory into L2 ahead of their use: one
+ * bulk prefetch through the copy engine (cp.async.bulk.prefetch.L2; a hint,
+ * nothing waits for it), over the range rounded out to 16-byte boundaries.
+ * The arrays it is used on start on a 256-byte boundary and carry 256 bytes
+ * of padding, so the rounded range stays inside the allocation. */
+__device__ __forceinline__ void prefetchL2(const void* lo, const void* hi)
+{
+	const size_t a = __cvta_generic_to_global(lo) & ~size_t(15);
+	const size_t e = (__cvta_generic_to_global(hi) + 15u) & ~size_t(15);
+	if(e > a) {
+		asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(a), "r"(uint32_t(e - a)) : "memory");
+	}
 }
 
 /* xorshift128 (src/nemo/RNG.cpp:10-18) */
@@ -524,41 +541,41 @@ __device__ __forceinline__ int32_t updatedWeight(int32_t wOld, int32_t wDiff, co
 
 /* ---------------- grid barrier with a bounded wait ---------------- */
 
-/* Sense-reversal barrier over all blocks of the cooperative launch. A block
- * that waits longer than timeoutNs sets the error word and returns false;
- * every waiting block also gives up as soon as it sees the error word, so the
- * kernel always terminates. */
-__device__ __forceinline__ bool gridSync(unsigned* bar, unsigned long long timeoutNs)
+/* Barrier over all blocks of the cooperative launch. bar[0] counts arrivals
+ * and never goes back: the i-th barrier of a launch that started at count
+ * `base` (bar[1], read by every block before its first arrival) is passed
+ * once the count reaches base + i * gridDim.x. Arriving is one release
+ * reduction, so the last block's arrival is visible to the waiting blocks
+ * after a single trip through L2. A block that waits longer than timeoutNs
+ * sets the error word and returns false; every waiting block also gives up
+ * as soon as it sees the error word, so the kernel always terminates. */
+__device__ __forceinline__ bool gridSync(unsigned* bar, unsigned target, unsigned long long timeoutNs)
 {
 	__shared__ int ok;
 	__syncthreads();
 	if(threadIdx.x == 0) {
-		cuda::atomic_ref<unsigned, cuda::thread_scope_device> count(bar[0]);
-		cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(bar[1]);
-		cuda::atomic_ref<unsigned, cuda::thread_scope_device> err(bar[2]);
 		int good = 1;
-		unsigned g = gen.load(cuda::memory_order_relaxed);
-		/* publish the block's writes (ordered before this thread by the
-		 * __syncthreads above) to the whole device */
-		cuda::atomic_thread_fence(cuda::memory_order_acq_rel, cuda::thread_scope_device);
-		unsigned arrived = count.fetch_add(1u, cuda::memory_order_acq_rel);
-		if(arrived == gridDim.x - 1) {
-			count.store(0u, cuda::memory_order_relaxed);
-			gen.fetch_add(1u, cuda::memory_order_release);
-		} else {
-			unsigned long long start = globalTimer();
-			unsigned spins = 0;
-			while(gen.load(cuda::memory_order_acquire) == g) {
-				if((++spins & 1023u) == 0) {
-					if(err.load(cuda::memory_order_relaxed)) {
-						good = 0;
-						break;
-					}
-					if(globalTimer() - start > timeoutNs) {
-						err.store(1u, cuda::memory_order_relaxed);
-						good = 0;
-						break;
-					}
+		/* the block's writes are ordered before this thread's by the
+		 * __syncthreads above; the release makes them visible with the
+		 * arrival */
+		const size_t gbar = __cvta_generic_to_global(bar);
+		asm volatile("red.release.gpu.global.add.u32 [%0], 1;" :: "l"(gbar) : "memory");
+		unsigned long long start = 0;
+		unsigned spins = 0;
+		for(;;) {
+			unsigned v;
+			asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(gbar) : "memory");
+			if(int(v - target) >= 0) break;
+			if((++spins & 255u) == 0) {
+				if(start == 0) start = globalTimer();
+				if(*(volatile unsigned*) &bar[2]) {
+					good = 0;
+					break;
+				}
+				if(globalTimer() - start > timeoutNs) {
+					*(volatile unsigned*) &bar[2] = 1u;
+					good = 0;
+					break;
 				}
 			}
 		}
@@ -634,7 +651,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	__shared__ uint32_t sPreF[MAX_BLOCKS + 2];    /* + the remote list of a shard */
 	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
 	__shared__ uint32_t sNFired, sNPost, sWork;
-	__shared__ unsigned long long sEvents, sPushed, sVisits;
+	__shared__ unsigned long long sEvents, sPushed, sVisits, sHist, sAccW;
 
 	const NetDev& net = A.net;
 	const uint32_t tid = threadIdx.x;
@@ -653,11 +670,18 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t updWarps = min(myWarps, warpsPerBlock);
 	const size_t listStride = size_t(B) * ownN;  /* one parity of the lists */
 	int2* acc32 = reinterpret_cast<int2*>(net.acc);
-	const uint2* region = net.fcm + net.regionBase[b];
+	/* this block's buckets of the forward matrix: bucket of source s =
+	 * segKey0 + s * segStride */
+	const uint32_t grp = net.groupOf[b];
+	const uint32_t grpFirst = net.groupFirst[grp];
+	const uint32_t segStride = net.groupFirst[grp + 1] - grpFirst;
+	const size_t segKey0 = size_t(grpFirst) * nDev + (b - grpFirst);
 
 	/* the first cycle: a kernel parameter, or (for launches replayed from a
 	 * CUDA graph) a device counter that block 0 advances at the end */
 	const uint64_t first = A.cycleCounter ? *A.cycleCounter : A.firstCycle;
+	/* arrivals at the grid barrier when the launch started */
+	const unsigned barBase = *(volatile unsigned*) &net.barrier[1];
 
 	if(SMEM) {
 		const uint32_t total = net.slots * ownN;
@@ -668,7 +692,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		}
 	}
 
-	const uint32_t phases = A.cycles + ((A.carry & 2u) ? 0u : 1u);
+	/* carry bit 1: the launch ends with its last update phase; the cycle's
+	 * gathering waits for the next launch, and nothing follows that phase,
+	 * so it needs no grid barrier after it (a one-cycle step has none at
+	 * all and runs as an ordinary launch) */
+	const bool lastPending = (A.carry & 2u) != 0u;
+	const uint32_t phases = A.cycles + (lastPending ? 0u : 1u);
+	const uint32_t barriers = lastPending && A.cycles ? A.cycles - 1u : A.cycles;
 	for(uint32_t k = 0; k < phases; ++k) {
 		const uint64_t t64 = first + k;
 		const uint32_t t = uint32_t(t64);
@@ -683,6 +713,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			sEvents = 0;
 			sPushed = 0;
 			sVisits = 0;
+			sHist = 0;
+			sAccW = 0;
 			if(doUpdate && b == 0) {
 				net.firedCountRing[(t + 1) & net.ringMask] = 0;
 				net.eventsRing[(t + 1) & net.ringMask] = 0;
@@ -723,10 +755,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				/* a neuron at this device index (not one of an HH neuron's
 				 * seven helper lanes) */
 				const bool valid = (rel & ((1u << G.shift) - 1u)) == 0u && i < G.count;
-				/* the firing-stimulus word is cleared after the model has
-				 * issued its loads, so that nothing orders them behind it */
-				uint32_t stimWord = lane == 0 ? net.fstim[dw] : 0u;
-				stimWord = __shfl_sync(FULL, stimWord, 0);
+				/* the firing-stimulus word (every lane loads it: one
+				 * transaction, and nothing waits for it before the model
+				 * needs it); cleared after the model has issued its loads,
+				 * so that nothing orders them behind it */
+				uint32_t stimWord = net.fstim[dw];
 				if(k == 0 && (A.inlineNf | A.inlineNi)) {
 					/* a step's short stimulus, from the parameters: this warp's
 					 * firing bits, and the currents of its own neurons (read
@@ -799,6 +832,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					if(A.hostWords) A.hostWords[dw] = word;
 				}
 				if(net.stdp) {
+					const uint32_t rec = __ballot_sync(FULL, rfNew != 0ull && valid);
+					if(lane == 0) net.recentWords[size_t((t + 1u) & 1u) * net.nWords + dw] = rec;
+				}
+				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
 					const bool post = valid && ((rfNew >> net.postShift) & 1ull);
 					const uint32_t pm = __ballot_sync(FULL, post);
@@ -808,6 +845,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						base = __shfl_sync(FULL, base, 0);
 						if(post) {
 							postOut[base + __popc(pm & lt)] = make_uint2(rcm.x, rcm.y - rcm.x);
+							/* the next phase's STDP accumulation walks this
+							 * target's reverse range: into L2 now */
+							prefetchL2(net.rcmSrcDelay + rcm.x, net.rcmSrcDelay + rcm.y);
+							prefetchL2(net.rcmAcc + rcm.x, net.rcmAcc + rcm.y);
 						}
 					}
 				}
@@ -823,6 +864,23 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					if(net.deliver) {
 						const uint32_t np = pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
 						pushed += lane == 0 ? np : 0u;   /* warp total, counted once */
+						/* every block gathers these sources next phase: their
+						 * chunk of each block group, and the bucket starts of
+						 * the chunk, into L2 now; one (source, group) pair per
+						 * lane */
+						const uint32_t G = net.groups;
+						const uint32_t pairs = uint32_t(__popc(word)) * G;
+						for(uint32_t q = lane; q < pairs; q += 32u) {
+							const uint32_t f = q / G, g = q - f * G;
+							const uint32_t src = dw * 32u + uint32_t(__fns(word, 0u, int(f) + 1));
+							const uint32_t g0 = __ldg(&net.groupFirst[g]);
+							const uint32_t bg = __ldg(&net.groupFirst[g + 1]) - g0;
+							const size_t k0 = size_t(g0) * nDev + size_t(src) * bg;
+							prefetchL2(net.segOff + k0, net.segOff + k0 + bg + 1u);
+							const uint32_t c0 = __ldg(&net.srcChunk[size_t(src) * G + g]);
+							const uint32_t c1 = __ldg(&net.srcChunk[size_t(src + 1u) * G + g]);
+							prefetchL2(net.fcm + c0, net.fcm + c1);
+						}
 					}
 				}
 				/* in the first phase the noise of the next cycle is drawn by
@@ -859,9 +917,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const uint32_t* flist = net.firedList + par * listStride;
 			const uint2* plist = net.postList + par * listStride;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
+			const uint32_t* recent = net.recentWords + size_t(t & 1u) * net.nWords;
 			const uint32_t slotPrev = uint32_t((t64 - 1u) % net.slots);
 			uint32_t pushed = 0;
-			uint64_t visited = 0;
+			uint64_t visited = 0, histReads = 0, accWrites = 0;
 			for(;;) {
 				uint32_t u = 0;
 				if(lane == 0) u = atomicAdd(&sWork, 1u);
@@ -878,7 +937,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						const uint32_t bb = findList(sPreF, nLists, j);
 						const uint32_t s = bb < B ? flist[size_t(bb) * ownN + (j - sPreF[bb])]
 							: net.remoteList[size_t(par) * nDev + (j - sPreF[B])];
-						const uint32_t* row = net.segOff + size_t(b) * (nDev + 1u) + s;
+						const uint32_t* row = net.segOff + segKey0 + size_t(s) * segStride;
 						beg = row[0];
 						cnt = row[1] - beg;
 					}
@@ -905,7 +964,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							}
 							const uint32_t eL = __shfl_sync(FULL, excl, lo);
 							const uint32_t bL = __shfl_sync(FULL, beg, lo);
-							r[x] = idx < total ? __ldcs(&region[bL + (idx - eL)]) : make_uint2(0u, 0u);
+							r[x] = idx < total ? __ldcs(&net.fcm[bL + (idx - eL)]) : make_uint2(0u, 0u);
 						}
 #pragma unroll
 						for(int x = 0; x < GATHER_PER_LANE; ++x) {
@@ -941,29 +1000,39 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						const uint32_t b0 = range.x + off;
 						const uint32_t cnt = range.y - off < item ? range.y - off : item;
 						visited += cnt;
-						/* the accumulators do not depend on the sources: load
-						 * them with the source words, before the histories */
 						uint32_t sd[STDP_PER_LANE];
-						int32_t old[STDP_PER_LANE];
 #pragma unroll
 						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
 							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
-							old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
+						}
+						/* a source whose history is 0 contributes nothing
+						 * (weightChange(0) = 0): only the others' histories
+						 * and accumulators are read */
+						bool hot[STDP_PER_LANE];
+#pragma unroll
+						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+							const uint32_t jj = lane + 32u * x;
+							const uint32_t src = sd[x] >> 6;
+							hot[x] = jj < cnt && ((recent[src >> 5] >> (src & 31u)) & 1u);
 						}
 						uint64_t pre[STDP_PER_LANE];
+						int32_t old[STDP_PER_LANE];
 #pragma unroll
 						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
-							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
+							pre[x] = hot[x] ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
+							old[x] = hot[x] ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
+							histReads += hot[x] ? 1u : 0u;
 						}
 #pragma unroll
 						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
-							if(jj < cnt) {
+							if(hot[x]) {
 								const int32_t dw = weightChange(pre[x], A.rule);
 								if(dw != 0) {
 									__stcs(&net.rcmAcc[b0 + jj], int32_t(uint32_t(old[x]) + uint32_t(dw)));
+									accWrites++;
 								}
 							}
 						}
@@ -978,9 +1047,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				}
 			}
 			pushed = __reduce_add_sync(FULL, pushed);
+			histReads = __reduce_add_sync(FULL, uint32_t(histReads));
+			accWrites = __reduce_add_sync(FULL, uint32_t(accWrites));
 			if(lane == 0) {
 				if(pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
 				if(visited) atomicAdd(&sVisits, (unsigned long long) visited);
+				if(histReads) atomicAdd(&sHist, (unsigned long long) histReads);
+				if(accWrites) atomicAdd(&sAccW, (unsigned long long) accWrites);
 			}
 		}
 		__syncthreads();
@@ -998,10 +1071,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			}
 			if(sPushed) atomicAdd(&net.stats[0], sPushed);
 			if(sVisits) atomicAdd(&net.stats[1], sVisits);
+			if(sHist) atomicAdd(&net.stats[4], sHist);
+			if(sAccW) atomicAdd(&net.stats[5], sAccW);
 		}
 		if(trace && tid == 0) trace[3] = globalTimer();
-		if(k < A.cycles) {
-			if(!gridSync(net.barrier, A.timeoutNs)) {
+		if(k < barriers) {
+			if(!gridSync(net.barrier, barBase + (k + 1u) * B, A.timeoutNs)) {
 				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
 				return;
 			}
@@ -1010,8 +1085,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	}
 
 	/* the delay-1 arrivals for the cycle after the launch go into its slot,
-	 * so that between launches every spike fired is in the current slots */
-	{
+	 * so that between launches every spike fired is in the current slots
+	 * (a launch that leaves its last cycle pending leaves them in the inbox,
+	 * which every reader of the cycle's currents adds: the update, the
+	 * plugin current export and applyStdp's arrival-slot correction) */
+	if(!lastPending) {
 		__syncthreads();
 		const uint64_t tEnd = first + A.cycles;
 		const uint32_t slotEnd = uint32_t(tEnd % net.slots);
@@ -1038,8 +1116,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			if(l < myN) acc32[size_t(s) * nDev + n] = sAcc[x];
 		}
 	}
-	if(A.cycleCounter && b == 0 && tid == 0) {
-		*A.cycleCounter = first + A.cycles;
+	if(b == 0 && tid == 0) {
+		if(A.cycleCounter) *A.cycleCounter = first + A.cycles;
+		/* every block has read barBase: they all arrived at this launch's
+		 * barriers, which block 0 has passed (a launch without barriers
+		 * leaves the count as it found it) */
+		if(barriers) *(volatile unsigned*) &net.barrier[1] = barBase + barriers * B;
 	}
 }
 
@@ -1271,8 +1353,13 @@ k_shard_inject(NetDev net, uint64_t t64, const uint32_t* allWords, uint32_t ownL
 		const uint32_t word = allWords[w];
 		const uint32_t n = w * 32u + lane;
 		const bool fired = (word >> lane) & 1u;
-		rfOut[n] = (rfIn[n] << 1) | uint64_t(fired);
+		const uint64_t rfNew = (rfIn[n] << 1) | uint64_t(fired);
+		rfOut[n] = rfNew;
 		if(lane == 0) net.firedRing[size_t(t & net.ringMask) * net.nWords + w] = word;
+		if(net.stdp) {
+			const uint32_t rec = __ballot_sync(FULL, rfNew != 0ull);
+			if(lane == 0) net.recentWords[size_t(par ^ 1u) * net.nWords + w] = rec;
+		}
 		if(word) {
 			uint32_t base = 0;
 			if(lane == 0) base = atomicAdd(&net.remoteCnt[par], uint32_t(__popc(word)));
@@ -1289,6 +1376,22 @@ k_shard_inject(NetDev net, uint64_t t64, const uint32_t* allWords, uint32_t ownL
 	if(lane == 0) {
 		if(events) atomicAdd(&net.stats[3], events);
 		if(pushed) atomicAdd(&net.stats[0], pushed);
+	}
+}
+
+/* net.srcChunk from net.segOff: entry s * groups + g is the bucket start of
+ * (source s, the first block of group g), the start of source s's chunk in
+ * the group; s = nDev gives the group's end */
+__global__ void
+k_source_chunks(NetDev net, uint32_t* out)
+{
+	const size_t G = net.groups;
+	const size_t total = (size_t(net.nDev) + 1) * G;
+	for(size_t x = blockIdx.x * size_t(blockDim.x) + threadIdx.x; x < total; x += size_t(gridDim.x) * blockDim.x) {
+		const size_t src = x / G;
+		const uint32_t g = uint32_t(x - src * G);
+		const uint32_t g0 = net.groupFirst[g], bg = net.groupFirst[g + 1] - g0;
+		out[x] = net.segOff[size_t(g0) * net.nDev + src * bg];
 	}
 }
 
@@ -1426,6 +1529,21 @@ static cudaError_t
 launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
 {
 	const NetDev& net = args.net;
+	if(args.cycles <= 1u && (args.carry & 2u)) {
+		/* one update phase and no grid barrier: the blocks never wait for one
+		 * another, so they need not be co-resident */
+		switch(net.threads) {
+			case 256:
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 256>, dim3(net.blocks), dim3(256), params, bytes,
+						stream);
+			case 512:
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 512>, dim3(net.blocks), dim3(512), params, bytes,
+						stream);
+			default:
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 1024>, dim3(net.blocks), dim3(1024), params,
+						bytes, stream);
+		}
+	}
 	switch(net.threads) {
 		case 256:
 			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 256>, dim3(net.blocks), dim3(256), params,
@@ -1493,6 +1611,14 @@ launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* s
 {
 	if(n == 0) return;
 	k_exp_eval<<<smCount() * 8, 256, 0, S(stream)>>>(first, n, out, net);
+}
+
+void
+launchSourceChunks(const NetDev& net, uint32_t* srcChunk, void* stream)
+{
+	const size_t total = (size_t(net.nDev) + 1) * net.groups;
+	const uint32_t blocks = uint32_t(std::min<size_t>((total + 255) / 256, size_t(smCount()) * 16));
+	k_source_chunks<<<std::max<uint32_t>(blocks, 1u), 256, 0, S(stream)>>>(net, srcChunk);
 }
 
 void

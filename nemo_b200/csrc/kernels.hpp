@@ -85,14 +85,27 @@ struct NetDev {
 	uint32_t warpBase;
 	int smemAcc;            /* current slots of the owned neurons in shared memory */
 
-	/* forward connectivity. Delays >= 2, partitioned by target owner:
-	 * region b = [regionBase[b], regionBase[b+1]); within it the synapses of
-	 * source s are [segOff[b][s], segOff[b][s + 1]) (rows of nDev + 1, so
-	 * that a segment's two ends share a line).
+	/* forward connectivity. Delays >= 2: the owner blocks form `groups`
+	 * consecutive block groups (group g: blocks [groupFirst[g],
+	 * groupFirst[g + 1])); the synapses whose target a block of group g
+	 * owns follow one another in group order, inside a group by source, for
+	 * a source by owner block, for a (source, block) pair in insertion order.
+	 * The segment of (source s, block b) is bucket
+	 *   k = groupFirst[g] * nDev + s * (blocks of g) + (b - groupFirst[g])
+	 * = [segOff[k], segOff[k + 1]) (absolute positions): the buckets of one
+	 * source in one group are consecutive, so a fired source's synapses in a
+	 * group are one contiguous chunk, and its bucket starts for all the
+	 * group's blocks share a line. segOff has blocks * nDev + 1 entries.
 	 * Delay 1, by source: [d1Base + d1Start[s], d1Base + d1Start[s+1]) */
 	uint2* fcm;                    /* {target << 6 | (delay - 1), int32 weight} */
-	const uint64_t* regionBase;    /* [blocks + 1] */
-	const uint32_t* segOff;        /* [blocks][nDev + 1] */
+	const uint32_t* segOff;        /* [blocks * nDev + 1] */
+	uint32_t groups;
+	const uint32_t* groupFirst;    /* [groups + 1] */
+	const uint32_t* groupOf;       /* [blocks] the group of each block */
+	/* the chunk of source s in group g: [srcChunk[s * groups + g],
+	 * srcChunk[(s + 1) * groups + g]) ((nDev + 1) * groups entries, derived
+	 * from segOff by launchSourceChunks) */
+	const uint32_t* srcChunk;
 	const uint32_t* outDegree;     /* [nDev] synapses per source */
 	const uint32_t* d1Start;       /* [nDev + 1] */
 	uint64_t d1Base;
@@ -117,6 +130,11 @@ struct NetDev {
 
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
+	/* [2][nWords] by the parity of rf: bit n % 32 of word n / 32 is set when
+	 * neuron n's firing history (rf of the same parity) is not 0. A synapse
+	 * whose source's bit is clear has no spike in its STDP window, so the
+	 * accumulation skips it without reading the history */
+	uint32_t* recentWords;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
 	uint32_t stdpChunks;           /* STDP items per target (max in-degree / (32 x STDP_PER_LANE)) */
 	uint32_t applyChunks;          /* (32 x APPLY_PER_LANE)-synapse chunks per target */
@@ -146,10 +164,15 @@ struct NetDev {
 	uint32_t* remoteCnt;
 
 	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
-	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */
+	 * [2] neurons fired, [3] synaptic events (fired x out-degree), [4] STDP
+	 * visits that read the source's history (and the accumulator), [5]
+	 * accumulators written; [6], [7] unused */
 	unsigned long long* stats;
 
-	/* grid barrier: [0] arrivals, [1] generation, [2] error (timeout) */
+	/* grid barrier: [0] arrivals since the simulation was created (every
+	 * block adds 1 at every barrier), [1] the arrival count when the current
+	 * launch started (written by block 0 at the end of each launch), [2]
+	 * error (timeout) */
 	unsigned* barrier;
 };
 
@@ -276,6 +299,8 @@ void launchNrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t
 void launchLibmEval(float* sinOut, float* logOut, const uint32_t* sinTab, const uint32_t* logTab, void* stream);
 /* device expf (glibc-matching) of the floats with bits [first, first + n) */
 void launchExpEval(uint32_t first, uint32_t n, float* out, const NetDev& net, void* stream);
+/* fill net.srcChunk from net.segOff (construction) */
+void launchSourceChunks(const NetDev& net, uint32_t* srcChunk, void* stream);
 /* sharded simulation: the remote firing of cycle t (k_shard_inject) */
 void launchShardInject(const NetDev& net, uint64_t t, const uint32_t* allWords, uint32_t ownLo, uint32_t ownHi,
 		void* stream);

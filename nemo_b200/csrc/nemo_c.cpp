@@ -325,6 +325,27 @@ nemo_b200_shard_deliver(nemo_simulation_t s, const uint32_t all_words[], unsigne
 }
 
 nemo_status_t
+nemo_b200_shard_step_async(nemo_simulation_t s, const unsigned fstim_nidx[], size_t fstim_count,
+		const unsigned istim_nidx[], const float istim_current[], size_t istim_count, uint32_t* local_words_dev,
+		void* stream)
+{
+	RETURN_CALL(s->sim.shardStepAsync(fstim_nidx, fstim_count, istim_nidx, istim_current, istim_count,
+				local_words_dev, stream));
+}
+
+nemo_status_t
+nemo_b200_shard_deliver_async(nemo_simulation_t s, const uint32_t* all_words_dev, void* stream)
+{
+	RETURN_CALL(s->sim.shardDeliverAsync(all_words_dev, stream));
+}
+
+nemo_status_t
+nemo_b200_stream_wait(nemo_simulation_t s, void* stream)
+{
+	RETURN_CALL(s->sim.streamWait(stream));
+}
+
+nemo_status_t
 nemo_step(nemo_simulation_t s, unsigned fstim_nidx[], size_t fstim_count,
 		unsigned istim_nidx[], float istim_current[], size_t istim_count,
 		unsigned* fired[], size_t* fired_count)
@@ -438,7 +459,7 @@ nemo_b200_timed_steps(nemo_simulation_t s, unsigned steps, unsigned cycles_per_s
 }
 
 nemo_status_t
-nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out[10])
+nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out[12])
 {
 	RETURN_CALL(s->sim.profile(cycles, reward, out));
 }

@@ -72,7 +72,9 @@ void*
 Simulation::alloc(size_t bytes)
 {
 	void* p = nullptr;
-	if(bytes == 0) bytes = 16;
+	/* 256 bytes of padding: the step kernel's L2 prefetches round ranges
+	 * out to 16-byte boundaries */
+	bytes += 256;
 	NEMO_CUDA(cudaMalloc(&p, bytes));
 	m_allocs.push_back(p);
 	NEMO_CUDA(cudaMemsetAsync(p, 0, bytes, STREAM(m_stream)));
@@ -203,22 +205,16 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 			m_d2group[g.devBase + (i << g.shift)] = int32_t(gi);
 		}
 	}
-	/* dense user -> device table when the user indices are compact */
+	/* dense user -> device table when the user indices are compact (kept:
+	 * every step maps its stimulus through it) */
 	uint32_t lo = ~0u, hi = 0;
 	for(const auto& kv : m_g2d) { lo = std::min(lo, kv.first); hi = std::max(hi, kv.first); }
-	bool dense = uint64_t(hi) - lo + 1 <= std::max<uint64_t>(uint64_t(m_nNeurons) * 4, 1u << 20);
-	std::vector<uint32_t> denseMap;
-	if(dense) {
-		denseMap.assign(size_t(hi) - lo + 1, ~0u);
-		for(const auto& kv : m_g2d) denseMap[kv.first - lo] = kv.second;
+	if(uint64_t(hi) - lo + 1 <= std::max<uint64_t>(uint64_t(m_nNeurons) * 4, 1u << 20)) {
+		m_g2dLo = lo;
+		m_g2dDense.assign(size_t(hi) - lo + 1, ~0u);
+		for(const auto& kv : m_g2d) m_g2dDense[kv.first - lo] = kv.second;
 	}
-	auto map = [&](uint32_t gidx) -> uint32_t {
-		if(dense) {
-			return (gidx >= lo && gidx <= hi) ? denseMap[gidx - lo] : ~0u;
-		}
-		auto it = m_g2d.find(gidx);
-		return it == m_g2d.end() ? ~0u : it->second;
-	};
+	auto map = [&](uint32_t gidx) -> uint32_t { return toDev(gidx); };
 
 	/* ---- STDP constants (src/nemo/StdpProcess.cpp:20-46) ---- */
 	if(m_stdpOn) {
@@ -343,6 +339,30 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	}
 	const uint32_t B = m_blocks;
 	const uint32_t ownN = ownWarps * 32;
+	if(uint64_t(B) * m_nDev + m_nDev + 1 >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most " + std::to_string((uint64_t(1) << 32) / (B + 1))
+				+ " neurons per simulation on this device");
+	}
+
+	/* block groups of the forward matrix: consecutive owner blocks whose
+	 * delay >= 2 synapses together stay within APPLY_GROUP_SYNAPSES (the
+	 * records one applyStdp launch rewrites, kept in L2) */
+	std::vector<uint32_t> groupFirst(1, 0), groupOf(B, 0);
+	{
+		std::vector<uint64_t> perBlock(size_t(B) + 1, 0);
+		for(size_t s = 0; s < S; ++s) {
+			if(net.dly[s] != 1) perBlock[size_t(ownerOfWarp[dtgt[s] / 32 - warpLo]) + 1]++;
+		}
+		for(uint32_t b = 0; b < B; ++b) perBlock[b + 1] += perBlock[b];
+		for(uint32_t b = 0; b < B;) {
+			uint32_t e = b + 1;
+			while(e < B && perBlock[e + 1] - perBlock[b] <= APPLY_GROUP_SYNAPSES) ++e;
+			for(uint32_t x = b; x < e; ++x) groupOf[x] = uint32_t(groupFirst.size() - 1);
+			groupFirst.push_back(e);
+			b = e;
+		}
+	}
+	const uint32_t G = uint32_t(groupFirst.size() - 1);
 
 	/* the simulation's stream; the device build of the layout runs on it */
 	cudaStream_t stream;
@@ -369,56 +389,52 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		li.dly = net.dly.data();
 		li.plastic = net.plastic.data();
 		li.ownerOfWarp = ownerOfWarp.data();
+		li.groupFirst = groupFirst.data();
+		li.groupOf = groupOf.data();
+		li.groups = G;
 		buildLayoutOnDevice(li, [this](size_t bytes) { return alloc(bytes); }, &dev, m_stream);
 	}
 
-	/* ---- forward matrix: the synapses of delay >= 2 partitioned by target
-	 * owner (region b holds, source by source, those whose target block b
-	 * owns, in insertion order within a segment), then the delay-1
-	 * synapses grouped by source (pushed at firing) ---- */
-	std::vector<uint64_t> regionBase;
+	/* ---- forward matrix: the synapses of delay >= 2 by block group, in a
+	 * group by source, for a source by owner block of the target (bucket
+	 * groupFirst[g] * nDev + source * blocks(g) + (b - groupFirst[g])), in
+	 * insertion order within a bucket; then the delay-1 synapses grouped by
+	 * source (pushed at firing) ---- */
 	std::vector<uint32_t> segOff, d1Start;
 	std::vector<uint2> fcm;
 	std::vector<uint32_t> fcmPos;
 	std::vector<uint32_t> synAt;   /* synapse at each forward position */
+	uint64_t d1Base = 0;
 	if(onDevice) {
-		regionBase = dev.regionBase;
+		d1Base = dev.d1Base;
 		fcmPos.swap(dev.fcmPos);
 	} else {
-		regionBase.assign(size_t(B) + 1, 0);
-		segOff.assign((size_t(m_nDev) + 1) * B, 0);
+		const size_t buckets = size_t(B) * m_nDev;
+		auto bucket = [&](size_t s) -> size_t {
+			const uint32_t b = ownerOfWarp[dtgt[s] / 32 - warpLo];
+			const uint32_t g0 = groupFirst[groupOf[b]], bg = groupFirst[groupOf[b] + 1] - g0;
+			return size_t(g0) * m_nDev + size_t(dsrc[s]) * bg + (b - g0);
+		};
+		segOff.assign(buckets + 1, 0);
 		d1Start.assign(size_t(m_nDev) + 1, 0);
 		fcm.resize(S);
 		fcmPos.resize(S);
 		synAt.resize(S);
-		/* cursor[b][s]: count, then next free offset within region b */
-		std::vector<uint32_t> cursor(size_t(B) * m_nDev, 0);
 		for(size_t s = 0; s < S; ++s) {
 			if(net.dly[s] == 1) d1Start[dsrc[s] + 1]++;
-			else cursor[size_t(ownerOfWarp[dtgt[s] / 32 - warpLo]) * m_nDev + dsrc[s]]++;
+			else segOff[bucket(s) + 1]++;
 		}
-		for(uint32_t b = 0; b < B; ++b) {
-			uint32_t* c = &cursor[size_t(b) * m_nDev];
-			uint64_t run = 0;
-			for(uint32_t src = 0; src < m_nDev; ++src) {
-				segOff[size_t(b) * (m_nDev + 1) + src] = uint32_t(run);
-				uint32_t k = c[src];
-				c[src] = uint32_t(run);
-				run += k;
-			}
-			segOff[size_t(b) * (m_nDev + 1) + m_nDev] = uint32_t(run);
-			regionBase[b + 1] = regionBase[b] + run;
-		}
+		for(size_t k = 0; k < buckets; ++k) segOff[k + 1] += segOff[k];
+		d1Base = segOff[buckets];
 		for(uint32_t n = 0; n < m_nDev; ++n) d1Start[n + 1] += d1Start[n];
+		std::vector<uint32_t> cursor(segOff.begin(), segOff.end() - 1);
 		std::vector<uint32_t> d1Fill(d1Start.begin(), d1Start.end() - 1);
-		const uint64_t d1Base = regionBase[B];
 		for(size_t s = 0; s < S; ++s) {
 			uint64_t pos;
 			if(net.dly[s] == 1) {
 				pos = d1Base + d1Fill[dsrc[s]]++;
 			} else {
-				const uint32_t b = ownerOfWarp[dtgt[s] / 32 - warpLo];
-				pos = regionBase[b] + cursor[size_t(b) * m_nDev + dsrc[s]]++;
+				pos = cursor[bucket(s)]++;
 			}
 			fcm[pos] = make_uint2((dtgt[s] << 6) | (net.dly[s] - 1), uint32_t(wfx[s]));
 			fcmPos[s] = uint32_t(pos);
@@ -426,14 +442,12 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		}
 	}
 
-	/* applyStdp launches: consecutive owner blocks grouped until their
-	 * regions hold APPLY_GROUP_SYNAPSES synapses, as target ranges */
+	/* applyStdp launches: one per block group, as target ranges (a
+	 * target's plastic synapses of delay >= 2 all lie in its group's part
+	 * of the forward matrix) */
 	m_applyGroups.assign(1, warpLo * 32u);
-	for(uint32_t b = 0; b < B;) {
-		uint32_t e = b + 1;
-		while(e < B && regionBase[e + 1] - regionBase[b] <= APPLY_GROUP_SYNAPSES) ++e;
-		m_applyGroups.push_back(std::min((warpLo + ownStart[e]) * 32u, m_nDev));
-		b = e;
+	for(uint32_t g = 0; g < G; ++g) {
+		m_applyGroups.push_back(std::min((warpLo + ownStart[groupFirst[g + 1]]) * 32u, m_nDev));
 	}
 
 	/* ---- reverse matrix of plastic synapses, grouped by target ---- */
@@ -512,11 +526,19 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.warpBase = warpLo;
 	m_net.smemAcc = smemAcc ? 1 : 0;
 	m_net.fcm = onDevice ? dev.fcm : (uint2*) put(fcm.data(), fcm.size() * 8);
-	m_net.regionBase = (const uint64_t*) put(regionBase.data(), regionBase.size() * 8);
 	m_net.segOff = onDevice ? dev.segOff : (const uint32_t*) put(segOff.data(), segOff.size() * 4);
+	m_net.groups = G;
+	m_net.groupFirst = (const uint32_t*) put(groupFirst.data(), groupFirst.size() * 4);
+	m_net.groupOf = (const uint32_t*) put(groupOf.data(), groupOf.size() * 4);
+	{
+		uint32_t* chunks = (uint32_t*) alloc((size_t(m_nDev) + 1) * G * 4);
+		launchSourceChunks(m_net, chunks, m_stream);
+		NEMO_CUDA(cudaGetLastError());
+		m_net.srcChunk = chunks;
+	}
 	m_net.outDegree = (const uint32_t*) put(outDegree.data(), outDegree.size() * 4);
 	m_net.d1Start = onDevice ? dev.d1Start : (const uint32_t*) put(d1Start.data(), d1Start.size() * 4);
-	m_net.d1Base = regionBase[B];
+	m_net.d1Base = d1Base;
 	m_net.inbox = alloc(size_t(2) * m_nDev * (acc32 ? 8 : 16));
 	m_net.acc = alloc(size_t(slots) * m_nDev * (acc32 ? 8 : 16));
 	m_net.rf = (uint64_t*) alloc(size_t(2) * m_nDev * 8);
@@ -526,7 +548,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
 	m_net.noise = (float*) alloc(size_t(2) * m_nDev * 4);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
-	m_net.stats = (unsigned long long*) alloc(4 * 8);
+	m_net.stats = (unsigned long long*) alloc(8 * 8);
 	m_net.barrier = (unsigned*) alloc(4 * 4);
 	m_net.firedList = (uint32_t*) alloc(size_t(2) * B * ownN * 4);
 	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
@@ -537,6 +559,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		m_net.remoteCnt = (uint32_t*) alloc(2 * 4);
 	}
 	m_net.stdp = m_stdpOn ? 1 : 0;
+	if(m_stdpOn) m_net.recentWords = (uint32_t*) alloc(size_t(2) * m_net.nWords * 4);
 	m_net.stdpChunks = uint32_t(stdpChunks);
 	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
 	if(m_stdpOn) {
@@ -673,6 +696,11 @@ Simulation::release()
 {
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
 	destroyGraph();
+	for(void** ev : {&m_evOut, &m_evIn, &m_evStaged}) {
+		if(*ev) cudaEventDestroy(static_cast<cudaEvent_t>(*ev));
+		*ev = nullptr;
+	}
+	m_stagedPending = false;
 	for(void* p : m_allocs) cudaFree(p);
 	m_allocs.clear();
 	if(m_hWords) cudaFreeHost(m_hWords);
@@ -695,11 +723,11 @@ Simulation::release()
 uint32_t
 Simulation::devIndex(unsigned gidx) const
 {
-	auto it = m_g2d.find(gidx);
-	if(it == m_g2d.end()) {
+	const uint32_t d = toDev(gidx);
+	if(d == ~0u) {
 		fail(NEMO_INVALID_INPUT, "Non-existing neuron index " + std::to_string(gidx));
 	}
-	return it->second;
+	return d;
 }
 
 Simulation::Group&
@@ -775,6 +803,12 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 		bool ownedOnly)
 {
 	cudaStream_t stream = STREAM(m_stream);
+	/* the pinned buffers are the source of the last staged copy, which a
+	 * call that did not wait for its step may still have queued */
+	if(m_stagedPending) {
+		NEMO_CUDA(cudaEventSynchronize(static_cast<cudaEvent_t>(m_evStaged)));
+		m_stagedPending = false;
+	}
 	size_t need = nf + ni;
 	if(need > m_stimCap) {
 		/* the old buffers go first; a failed allocation leaves the ones
@@ -801,25 +835,34 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 	int err = 0;
 	unsigned badIdx = 0;
 	for(size_t k = 0; k < nf; ++k) {
-		auto it = m_g2d.find(fstim[k]);
-		if(it == m_g2d.end()) { err = 1; badIdx = fstim[k]; break; }
-		if(ownedOnly && !owns(it->second)) continue;
-		m_hStim[nfOk++] = it->second;
+		const uint32_t d = toDev(fstim[k]);
+		if(d == ~0u) { err = 1; badIdx = fstim[k]; break; }
+		if(ownedOnly && !owns(d)) continue;
+		m_hStim[nfOk++] = d;
 	}
 	if(!err && ni) {
-		/* last write wins for repeated neurons */
-		std::unordered_map<uint32_t, uint32_t> seen;
+		/* last write wins for repeated neurons: the entry of a neuron seen
+		 * before in this call (m_stimEntry[d], valid when m_stimEpoch[d] is
+		 * this call's epoch) is overwritten */
+		if(m_stimEpoch.empty()) {
+			m_stimEpoch.assign(m_nDev, 0u);
+			m_stimEntry.assign(m_nDev, 0u);
+		}
+		if(++m_epoch == 0u) {
+			std::fill(m_stimEpoch.begin(), m_stimEpoch.end(), 0u);
+			m_epoch = 1u;
+		}
 		uint32_t* idx = m_hStim + nfOk;
 		for(size_t k = 0; k < ni; ++k) {
-			auto it = m_g2d.find(inidx[k]);
-			if(it == m_g2d.end()) { err = 1; badIdx = inidx[k]; break; }
-			if(ownedOnly && !owns(it->second)) continue;
-			auto s = seen.find(it->second);
-			if(s != seen.end()) {
-				m_hCur[s->second] = icur[k];
+			const uint32_t d = toDev(inidx[k]);
+			if(d == ~0u) { err = 1; badIdx = inidx[k]; break; }
+			if(ownedOnly && !owns(d)) continue;
+			if(m_stimEpoch[d] == m_epoch) {
+				m_hCur[m_stimEntry[d]] = icur[k];
 			} else {
-				seen.emplace(it->second, niOk);
-				idx[niOk] = it->second;
+				m_stimEpoch[d] = m_epoch;
+				m_stimEntry[d] = niOk;
+				idx[niOk] = d;
 				m_hCur[niOk] = icur[k];
 				niOk++;
 			}
@@ -836,6 +879,8 @@ Simulation::stageStimulus(const unsigned* fstim, size_t nf, const unsigned* inid
 	} else if(nfOk + niOk) {
 		NEMO_CUDA(cudaMemcpyAsync(m_dStim, m_hStim, size_t(nfOk + niOk) * 4, cudaMemcpyHostToDevice, stream));
 		if(niOk) NEMO_CUDA(cudaMemcpyAsync(m_dCur, m_hCur, size_t(niOk) * 4, cudaMemcpyHostToDevice, stream));
+		NEMO_CUDA(cudaEventRecord(static_cast<cudaEvent_t>(event(&m_evStaged)), stream));
+		m_stagedPending = true;
 		StimDev sd{m_dStim, nfOk, m_dStim + nfOk, m_dCur, niOk};
 		launchStimulus(m_net, sd, m_stream);
 	}
@@ -990,6 +1035,65 @@ Simulation::shardDeliver(const uint32_t* allWords)
 	return m_fired;
 }
 
+void*
+Simulation::event(void** ev)
+{
+	if(*ev == nullptr) {
+		cudaEvent_t e;
+		NEMO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+		*ev = e;
+	}
+	return *ev;
+}
+
+void
+Simulation::streamWait(void* stream)
+{
+	cudaEvent_t e = static_cast<cudaEvent_t>(event(&m_evOut));
+	NEMO_CUDA(cudaEventRecord(e, STREAM(m_stream)));
+	NEMO_CUDA(cudaStreamWaitEvent(STREAM(stream), e, 0));
+}
+
+void
+Simulation::shardStepAsync(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+		uint32_t* localDev, void* stream)
+{
+	if(!m_shardMode) {
+		fail(NEMO_LOGIC_ERROR, "shard step: the simulation is not a shard");
+	}
+	if(m_awaitDeliver) {
+		fail(NEMO_LOGIC_ERROR, "shard step: the previous cycle's firing has not been delivered");
+	}
+	stageStimulus(fstim, nf, inidx, icur, ni, true);
+	launchStep();
+	const uint32_t slot = uint32_t(m_cycle) & m_net.ringMask;
+	const uint32_t words = m_shard.warpHi - m_shard.warpLo;
+	NEMO_CUDA(cudaMemcpyAsync(localDev, m_net.firedRing + size_t(slot) * m_net.nWords + m_shard.warpLo,
+				size_t(words) * 4, cudaMemcpyDeviceToDevice, STREAM(m_stream)));
+	streamWait(stream);
+	m_cycle++;
+	m_stateDirty = true;
+	m_awaitDeliver = true;
+}
+
+void
+Simulation::shardDeliverAsync(const uint32_t* allDev, void* stream)
+{
+	if(!m_awaitDeliver) {
+		fail(NEMO_LOGIC_ERROR, "shard deliver: no shard step is waiting for its cycle's firing");
+	}
+	cudaEvent_t e = static_cast<cudaEvent_t>(event(&m_evIn));
+	NEMO_CUDA(cudaEventRecord(e, STREAM(stream)));
+	NEMO_CUDA(cudaStreamWaitEvent(STREAM(m_stream), e, 0));
+	const uint64_t t = m_cycle - 1;
+	if(m_net.remoteCnt) {
+		NEMO_CUDA(cudaMemsetAsync(m_net.remoteCnt + (t & 1u), 0, 4, STREAM(m_stream)));
+		launchShardInject(m_net, t, allDev, m_shard.warpLo, m_shard.warpHi, m_stream);
+		NEMO_CUDA(cudaGetLastError());
+	}
+	m_awaitDeliver = false;
+}
+
 /* One cycle as a single phase: the update of cycle m_cycle, overlapped with
  * the gathering and learning of the cycle before when that is pending (carry
  * bit 0); this cycle's own gathering waits (carry bit 1) for the next step or
@@ -1063,9 +1167,9 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 	for(size_t k0 = 0; k0 < nf && !err; k0 += CHUNK) {
 		size_t cnt = 0;
 		for(size_t k = k0; k < nf && k < k0 + CHUNK; ++k) {
-			auto it = m_g2d.find(fstim[k]);
-			if(it == m_g2d.end()) { err = 1; badIdx = fstim[k]; break; }
-			stage[cnt++] = it->second;
+			const uint32_t d = toDev(fstim[k]);
+			if(d == ~0u) { err = 1; badIdx = fstim[k]; break; }
+			stage[cnt++] = d;
 		}
 		if(cnt) NEMO_CUDA(cudaMemcpyAsync(scratch + nfOk, stage, cnt * 4, cudaMemcpyHostToDevice, stream));
 		nfOk += uint32_t(cnt);
@@ -1073,9 +1177,9 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 	for(size_t k0 = 0; k0 < ni && !err; k0 += CHUNK) {
 		size_t cnt = 0;
 		for(size_t k = k0; k < ni && k < k0 + CHUNK; ++k) {
-			auto it = m_g2d.find(inidx[k]);
-			if(it == m_g2d.end()) { err = 1; badIdx = inidx[k]; break; }
-			stage[cnt++] = it->second;
+			const uint32_t d = toDev(inidx[k]);
+			if(d == ~0u) { err = 1; badIdx = inidx[k]; break; }
+			stage[cnt++] = d;
 		}
 		if(cnt) {
 			NEMO_CUDA(cudaMemcpyAsync(scratch + NOALLOC_STIM_MAX + niOk, stage, cnt * 4,
@@ -1597,7 +1701,15 @@ Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_
 void
 Simulation::readStats(uint64_t out[4])
 {
-	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 4 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
+	uint64_t all[8];
+	readAllStats(all);
+	std::copy(all, all + 4, out);
+}
+
+void
+Simulation::readAllStats(uint64_t out[8])
+{
+	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 8 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 }
 
@@ -1647,7 +1759,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 }
 
 void
-Simulation::profile(unsigned cycles, float reward, double out[10])
+Simulation::profile(unsigned cycles, float reward, double out[12])
 {
 	notShard("profile");
 	notExternal("profile");
@@ -1657,8 +1769,8 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	NEMO_CUDA(cudaEventCreate(&e0));
 	NEMO_CUDA(cudaEventCreate(&e1));
 	NEMO_CUDA(cudaEventCreate(&e2));
-	uint64_t before[4], after[4];
-	readStats(before);
+	uint64_t before[8], after[8];
+	readAllStats(before);
 	NEMO_CUDA(cudaEventRecord(e0, stream));
 	launchBlock(m_cycle, cycles);
 	m_cycle += cycles;
@@ -1676,7 +1788,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	cudaEventDestroy(e1);
 	cudaEventDestroy(e2);
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
-	readStats(after);
+	readAllStats(after);
 	checkDeviceError();
 	m_stateDirty = true;
 	out[0] = tc;
@@ -1689,6 +1801,8 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 	out[7] = (m_stdpOn && m_nrcm) ? ta : 0.0;
 	out[8] = double(m_nrcm);
 	out[9] = double(after[3] - before[3]);
+	out[10] = double(after[4] - before[4]);
+	out[11] = double(after[5] - before[5]);
 }
 
 void

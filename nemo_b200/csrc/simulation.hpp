@@ -81,6 +81,19 @@ public:
 	void shardStep(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 			uint32_t* localWords);
 	const std::vector<unsigned>& shardDeliver(const uint32_t* allWords);
+	/* The same cycle with the fired words kept in device memory and nothing
+	 * waited for on the host: shardStepAsync queues the step and a copy of
+	 * the shard's own words into localDev (device, shard().warpHi -
+	 * warpLo words), then makes `stream` (a cudaStream_t, NULL: the legacy
+	 * default stream; e.g. the stream a collective is queued on) wait for
+	 * that copy. shardDeliverAsync makes the simulation's stream wait for
+	 * `stream`'s work queued so far and then reads allDev (device, every
+	 * warp's words). The cycle's fired neurons are read with firedAt. */
+	void shardStepAsync(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
+			uint32_t* localDev, void* stream);
+	void shardDeliverAsync(const uint32_t* allDev, void* stream);
+	/* make `stream` wait for the work queued on the simulation's stream */
+	void streamWait(void* stream);
 	const ShardSpec& shard() const { return m_shard; }
 
 	float getNeuronState(unsigned gidx, unsigned var);
@@ -128,9 +141,10 @@ public:
 	 * blocks, [2] 0, [3] synapses pushed, [4] neurons fired, [5] STDP synapse
 	 * visits, [6] neuron updates, [7] applyStdp ms, [8] plastic synapses,
 	 * [9] synaptic events generated. */
-	void profile(unsigned cycles, float reward, double out[10]);
+	void profile(unsigned cycles, float reward, double out[12]);
 
 	void readStats(uint64_t out[4]);
+	void readAllStats(uint64_t out[8]);
 	unsigned applyLaunches() const { return m_stdpOn && m_nrcm ? unsigned(m_applyGroups.size() - 1) : 0u; }
 
 	/* ---- batches of independent networks (Network::merge) ---- */
@@ -229,6 +243,23 @@ private:
 	uint64_t m_nrcm;
 	std::vector<Group> m_groups;
 	std::unordered_map<uint32_t, uint32_t> m_g2d;  /* user index -> device index */
+	/* the same as a table from user index m_g2dLo on, when the indices are
+	 * compact enough (empty otherwise) */
+	uint32_t m_g2dLo = 0;
+	std::vector<uint32_t> m_g2dDense;
+	/* device index of a user index, ~0u for none */
+	uint32_t toDev(uint32_t gidx) const
+	{
+		if(!m_g2dDense.empty()) {
+			const uint32_t k = gidx - m_g2dLo;
+			return gidx >= m_g2dLo && k < m_g2dDense.size() ? m_g2dDense[k] : ~0u;
+		}
+		auto it = m_g2d.find(gidx);
+		return it == m_g2d.end() ? ~0u : it->second;
+	}
+	/* repeated current-stimulus neurons within one call (stageStimulus) */
+	std::vector<uint32_t> m_stimEpoch, m_stimEntry;
+	uint32_t m_epoch = 0;
 	std::vector<uint32_t> m_d2g;                   /* device index -> user index (~0: padding) */
 	std::vector<int32_t> m_d2group;                /* device index -> group (-1: padding) */
 
@@ -297,6 +328,15 @@ private:
 	ShardSpec m_shard;
 	bool m_awaitDeliver = false;    /* the last cycle's remote firing has not come in */
 	uint32_t* m_dAllWords = nullptr;
+
+	/* events ordering the simulation's stream with a caller's stream, and
+	 * the end of the last staged stimulus copy (its pinned source is
+	 * rewritten only after it) */
+	void* m_evOut = nullptr;
+	void* m_evIn = nullptr;
+	void* m_evStaged = nullptr;
+	bool m_stagedPending = false;
+	void* event(void** ev);
 
 	/* graph run */
 	void destroyGraph();

@@ -5,7 +5,10 @@ the CPU tests).
   --gpus N, no data-path collective) or one network over all GPUs as shards
   (``ShardedSimulation``; bench.py --sharded): each shard owns a contiguous
   range of neuron warps and the synapses to them, and the shards' fired
-  words are all-gathered once per cycle (``exchange_fired_words``).
+  words are all-gathered once per cycle: through host memory
+  (``exchange_fired_words``; gloo and NCCL), or as CUDA tensors that never
+  leave the GPUs (``exchange_fired_words_device``; NCCL, queued without
+  waiting on the host).
 * The batched form splits its independent networks over the ranks
   (``shard_instances``): each rank advances its own batch, no collective.
 * The differentiable form is data-parallel over trials: each rank runs its
@@ -88,3 +91,37 @@ def exchange_fired_words(local_words, first_word, total_words, group=None):
         f, c = shard_warps(total_words, r, world)
         full[f:f + c] = part[:c].cpu().numpy().view(np.uint32)
     return full
+
+
+def exchange_fired_words_device(local_words, first_word, total_words, group=None):
+    """exchange_fired_words for CUDA tensors: `local_words` (int32, this
+    rank's words) -> a new int32 CUDA tensor of all total_words words, by one
+    all_gather_into_tensor of padded shares and one index gather, both queued
+    on the current stream. Without a process group the shard must own every
+    warp and the tensor is returned as it is."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        if first_word != 0 or local_words.numel() != total_words:
+            raise ValueError("without a process group the shard must own every warp")
+        return local_words
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    if (first_word, local_words.numel()) != shard_warps(total_words, rank, world):
+        raise ValueError("rank %d does not own warps [%d, %d)" % (rank, first_word, first_word + local_words.numel()))
+    width = -(-int(total_words) // world)
+    dev = local_words.device
+    send = torch.zeros(width, dtype=torch.int32, device=dev)
+    send[:local_words.numel()] = local_words
+    gathered = torch.empty(world * width, dtype=torch.int32, device=dev)
+    dist.all_gather_into_tensor(gathered, send, group=group)
+    key = (int(total_words), world, dev)
+    index = _gather_index.get(key)
+    if index is None:
+        parts = [r * width + np.arange(shard_warps(total_words, r, world)[1]) for r in range(world)]
+        index = torch.as_tensor(np.concatenate(parts), dtype=torch.int64, device=dev)
+        _gather_index[key] = index
+    return gathered.index_select(0, index)
+
+
+_gather_index = {}

@@ -440,6 +440,10 @@ def _bind_shard(lib):
                                        c_size_t, POINTER(ctypes.c_uint32)]
     d.nemo_b200_shard_deliver.argtypes = [ctypes.c_void_p, POINTER(ctypes.c_uint32), POINTER(POINTER(c_uint)),
                                           POINTER(c_size_t)]
+    d.nemo_b200_shard_step_async.argtypes = [ctypes.c_void_p, POINTER(c_uint), c_size_t, POINTER(c_uint),
+                                             POINTER(c_float), c_size_t, ctypes.c_void_p, ctypes.c_void_p]
+    d.nemo_b200_shard_deliver_async.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    d.nemo_b200_stream_wait.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     d._shard_bound = True
     return d
 
@@ -505,6 +509,42 @@ class ShardedSimulation(Simulation):
             from .dist import exchange_fired_words
             all_words = exchange_fired_words(local, self.first_word, self.total_words)
         return self.deliver(all_words)
+
+    def step_device(self, fstim=(), istim=(), exchange=None):
+        """One cycle with the fired words exchanged as CUDA tensors on the
+        current stream (nemo_b200_shard_step_async / _deliver_async):
+        nothing waits on the host and no word crosses to host memory.
+        ``exchange(local)`` maps this shard's words (int32 CUDA tensor) to
+        every warp's; by default nemo_b200.dist.exchange_fired_words_device
+        (NCCL). The cycle's fired neurons: fired_at(cycle)."""
+        import torch
+        from .dist import exchange_fired_words_device
+        f = _u32(fstim) if len(fstim) else None
+        if len(istim):
+            inidx = _u32([p[0] for p in istim])
+            icur = _f32([p[1] for p in istim])
+        else:
+            inidx = icur = None
+        stream = torch.cuda.current_stream().cuda_stream
+        local = torch.empty(self.words, dtype=torch.int32, device="cuda")
+        self.lib.call("nemo_b200_shard_step_async", self.handle,
+                      _ptr(f, c_uint) if f is not None else None, 0 if f is None else f.size,
+                      _ptr(inidx, c_uint) if inidx is not None else None,
+                      _ptr(icur, c_float) if icur is not None else None,
+                      0 if inidx is None else inidx.size, local.data_ptr(), stream)
+        if exchange is None:
+            all_words = exchange_fired_words_device(local, self.first_word, self.total_words)
+        else:
+            all_words = exchange(local)
+        self.lib.call("nemo_b200_shard_deliver_async", self.handle, all_words.data_ptr(), stream)
+        # the simulation reads both buffers later on its own stream: keep
+        # them until the next cycle's step, which that stream runs after
+        self._in_flight = (local, all_words)
+
+    def stream_wait(self):
+        """Order the current stream after the simulation's queued work."""
+        import torch
+        self.lib.call("nemo_b200_stream_wait", self.handle, torch.cuda.current_stream().cuda_stream)
 
 
 

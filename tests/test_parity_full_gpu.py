@@ -133,7 +133,7 @@ def test_batched_form_all_instances(oracle_lib):
                                       sigma_inh=float(0.4 * sig[j])) for j in range(count)]
     lib = Library()
     batch = Batch(lib, specs)
-    del batch.nets
+    batch.nets = [None] * count   # the networks' host copies are not needed after construction
     oracles = [_build(s, oracle_lib, True) for s in specs]
     del specs
     batch.run_graph(cycles, cycles)

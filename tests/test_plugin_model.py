@@ -308,8 +308,10 @@ def _failing_plugin(tmp_path, name, body):
     (tmp_path / (name + ".ini")).write_text(open(os.path.join(PLUGIN_DIR, "QIFPlugin.ini")).read())
     (tmp_path / "b200").mkdir(exist_ok=True)
     src = tmp_path / (name + ".c")
-    src.write_text(body)
-    subprocess.check_call(["gcc", "-shared", "-fPIC", "-o", str(tmp_path / "b200" / ("lib%s.so" % name)), str(src)])
+    # built against the plugin header, so that it carries its ABI version
+    src.write_text("#include <nemo_b200_plugin.h>\n" + body)
+    subprocess.check_call(["gcc", "-shared", "-fPIC", "-I", os.path.join(ROOT, "include"),
+                           "-o", str(tmp_path / "b200" / ("lib%s.so" % name)), str(src)])
 
 
 @pytest.mark.gpu
@@ -318,7 +320,7 @@ def test_plugin_update_error_is_reported(tmp_path):
     without launching anything): nemo_step fails with
     NEMO_CUDA_INVOCATION_ERROR naming the plugin's entry point."""
     _failing_plugin(tmp_path, "FailingUpdate",
-                    "int b200_update_neurons(const void* batch, void* stream) { return 1; }\n")
+                    "int b200_update_neurons(const b200_neuron_batch* batch, void* stream) { return 1; }\n")
     lib = Library()
     lib.add_plugin_path(str(tmp_path))
     net = Network(lib)
@@ -336,8 +338,8 @@ def test_plugin_init_error_is_reported(tmp_path):
     """An initialisation that returns a CUDA error code: the simulation is
     not created, with NEMO_CUDA_INVOCATION_ERROR naming b200_init_neurons."""
     _failing_plugin(tmp_path, "FailingInit",
-                    "int b200_update_neurons(const void* batch, void* stream) { return 0; }\n"
-                    "int b200_init_neurons(const void* batch, void* stream) { return 1; }\n")
+                    "int b200_update_neurons(const b200_neuron_batch* batch, void* stream) { return 0; }\n"
+                    "int b200_init_neurons(const b200_neuron_batch* batch, void* stream) { return 1; }\n")
     lib = Library()
     lib.add_plugin_path(str(tmp_path))
     net = Network(lib)

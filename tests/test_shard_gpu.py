@@ -112,3 +112,50 @@ def test_shard_protocol_errors():
         s.step_local()
     with pytest.raises(ValueError):
         s.deliver(np.zeros(s.total_words + 1, np.uint32))
+
+
+@pytest.mark.parametrize("world", [1, 3])
+def test_sharded_device_exchange(oracle_lib, world):
+    """The device-resident exchange (nemo_b200_shard_step_async /
+    _deliver_async): each shard's words go to a CUDA tensor, the cycle's
+    words of all shards are concatenated on the current stream (as the NCCL
+    all-gather does across processes), and delivery reads them there; no word
+    crosses to host memory and nothing waits on the host inside a cycle. The
+    firing of every cycle, read afterwards with fired_at, and the weights
+    after STDP equal the oracle's."""
+    import torch
+    spec = netgen.izhikevich_random(2000, 100, dmax=20, seed=4, stdp=True)
+    stdp = netgen.standard_stdp()
+    net, shards = _shards(spec, world, stdp)
+    onet, o = _oracle(spec, oracle_lib, stdp)
+    stream = torch.cuda.current_stream().cuda_stream
+    cycle = 0
+    for epoch in range(2):
+        for c in range(100):
+            locals_ = []
+            for s in shards:
+                local = torch.empty(s.words, dtype=torch.int32, device="cuda")
+                s.lib.call("nemo_b200_shard_step_async", s.handle, None, 0, None, None, 0, local.data_ptr(), stream)
+                locals_.append(local)
+            all_words = torch.cat(locals_)
+            for s in shards:
+                s.lib.call("nemo_b200_shard_deliver_async", s.handle, all_words.data_ptr(), stream)
+            for s in shards:
+                s._in_flight = (locals_, all_words)
+            cycle += 1
+        for s in shards:
+            s.stream_wait()
+        for k in range(cycle - 100, cycle):
+            want = o.step()
+            for s in shards:
+                assert np.array_equal(s.fired_at(k), want), "cycle %d" % k
+        for s in shards:
+            s.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+    for src in range(0, 2000, 13):
+        expected = {int(sid): o.get_synapse_weight(int(sid)) for sid in o.get_synapses_from(src)}
+        got = {}
+        for s in shards:
+            for sid in s.get_synapses_from(src):
+                got[int(sid)] = s.get_synapse_weight(int(sid))
+        assert got == expected, src
