@@ -289,19 +289,18 @@ def roofline(sim, lib, wl):
     """Device times of one step's two kernels — the persistent step kernel
     (100 cycles of update, spike push and STDP accumulation) and applyStdp —
     and the dominant one's algorithmic bytes / time against the measured HBM
-    copy bandwidth. Algorithmic bytes: spike push 8 B per pushed synapse
-    (packed target/delay + i32 weight); Izhikevich update 92 B per neuron per
-    cycle; STDP accumulation 4 B per visited synapse (its source/delay word)
-    plus 12 B per visit whose source fired in the last 64 cycles (the 8 B
-    source history and the 4 B accumulator; for the others the kernel's
-    recent-firing bitmap shows that the change is 0) plus 4 B per
-    accumulator written; applyStdp 20 B per plastic synapse."""
-    out = (ctypes.c_double * 12)()
-    lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 12]
+    copy bandwidth. Algorithmic bytes (per unit of work of the reference
+    algorithm): spike delivery 8 B per delivered synapse (packed
+    target/delay + i32 weight); Izhikevich update 92 B per neuron per cycle;
+    STDP accumulation 20 B per (post-spike x plastic in-synapse) visit (4 B
+    reverse synapse, 8 B source history, 4+4 B accumulator); applyStdp 20 B
+    per plastic synapse."""
+    out = (ctypes.c_double * 10)()
+    lib.dll.nemo_b200_profile.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_float, ctypes.c_double * 10]
     lib.call("nemo_b200_profile", sim.handle, CYCLES_PER_STEP, ctypes.c_float(REWARD), out)
-    tcyc, blocks, _, pushed, fired, visits, updates, tapply, nplastic, generated, hist, accw = list(out)
+    tcyc, blocks, _, pushed, fired, visits, updates, tapply, nplastic, generated = list(out)
     kernels = {
-        "k_cycles": (8.0 * pushed + 92.0 * updates + 4.0 * visits + 12.0 * hist + 4.0 * accw, tcyc, 1),
+        "k_cycles": (8.0 * pushed + 92.0 * updates + 20.0 * visits, tcyc, 1),
         "k_apply_stdp": (20.0 * nplastic, tapply, 1),
     }
     peak, peak_kind = measured_peaks()
@@ -321,8 +320,7 @@ def roofline(sim, lib, wl):
             "per_kernel": {k: {kk: (round(vv, 5) if isinstance(vv, float) else vv) for kk, vv in v.items()}
                            for k, v in table.items()},
             "work_per_step": {"cycles": CYCLES_PER_STEP, "pushed_synapses": int(pushed), "fired": int(fired),
-                              "stdp_visits": int(visits), "stdp_history_reads": int(hist),
-                              "stdp_accumulator_writes": int(accw), "neuron_updates": int(updates),
+                              "stdp_visits": int(visits), "neuron_updates": int(updates),
                               "plastic_synapses": int(nplastic), "grid_blocks": int(blocks)}}
     return roof
 
@@ -842,11 +840,13 @@ def run_sharded(args):
     1e8-synapse STDP network as N shards (ShardedSimulation), one per GPU,
     each owning a contiguous range of the neuron warps and the synapses to
     them; every cycle the shards' fired words are all-gathered (NCCL) and
-    delivered, and applyStdp runs every 100 cycles (strong scaling). Every
-    cycle is host-synchronous (the step's fired words come back before the
-    exchange), so the time is the host clock between device
-    synchronisations, max over ranks; events are the shards' device
-    counters summed over ranks."""
+    delivered, and applyStdp runs every 100 cycles (strong scaling). The
+    words stay in device memory (step_device: the step, the all-gather of
+    CUDA tensors and the delivery are queued on the GPU without waiting on
+    the host); --host-exchange takes them through host memory instead,
+    every cycle host-synchronous. Time: CUDA events on the current stream,
+    which waits for the shard's work at the end, max over ranks; events are
+    the shards' device counters summed over ranks."""
     import torch
     import torch.distributed as dist
     from nemo_b200.nemo import ShardedSimulation
@@ -874,19 +874,26 @@ def run_sharded(args):
     def steps(k):
         for _ in range(k):
             for _ in range(CYCLES_PER_STEP):
-                sim.step()
+                if args.host_exchange:
+                    sim.step()
+                else:
+                    sim.step_device()
             sim.apply_stdp(REWARD)
 
     steps(max(args.warmup, 1))
+    sim.stream_wait()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     lib.call("nemo_b200_counters", sim.handle, counters)
     ev0 = counters[3]
-    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
     steps(args.steps)
+    sim.stream_wait()
+    e1.record()
     torch.cuda.synchronize()
-    secs = time.perf_counter() - t0
+    secs = e0.elapsed_time(e1) * 1e-3
     lib.call("nemo_b200_counters", sim.handle, counters)
     events = float(counters[3] - ev0)
     if world > 1:
@@ -903,8 +910,9 @@ def run_sharded(args):
             "data": "synthetic (seeded generator, numpy PCG64 seed %d)" % wl["seed"],
             "config": {"workload": wl["name"], "neurons": wl["n"], "synapses": wl["n"] * wl["m"],
                        "parallelism": "shards%d" % world, "cycles_per_step": CYCLES_PER_STEP,
-                       "exchange": "all-gather of the fired words every cycle"},
-            "timing": "host clock around host-synchronous cycles, max over ranks",
+                       "exchange": "all-gather of the fired words every cycle, "
+                                   + ("through host memory" if args.host_exchange else "in device memory")},
+            "timing": "CUDA events on the current stream, which waits for the shard's work, max over ranks",
             "sim_ms_per_wall_s": round(CYCLES_PER_STEP * args.steps / secs, 1),
             "gpu_launches": launches}
     if rank == 0:
@@ -952,6 +960,8 @@ def main():
                     help="measure the 1000-neuron benchmark network (no STDP)")
     ap.add_argument("--sharded", action="store_true",
                     help="one network over all ranks as shards (fired words all-gathered every cycle)")
+    ap.add_argument("--host-exchange", action="store_true",
+                    help="--sharded: exchange the fired words through host memory")
     ap.add_argument("--mixed", action="store_true",
                     help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
     ap.add_argument("--mixed-cycles", type=int, default=1000)

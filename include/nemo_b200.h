@@ -286,10 +286,8 @@ nemo_status_t nemo_b200_timed_steps(nemo_simulation_t sim, unsigned steps, unsig
  * simulated). out[0] = step-kernel ms, out[1] = its grid blocks, out[2] = 0,
  * out[3] = synapses pushed, out[4] = neurons fired, out[5] = STDP synapse
  * visits, out[6] = neuron updates, out[7] = applyStdp ms, out[8] = plastic
- * synapses, out[9] = synaptic events generated, out[10] = STDP visits that
- * read the source's firing history (the others' sources fired in none of the
- * last 64 cycles), out[11] = STDP accumulators written. */
-nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[12]);
+ * synapses, out[9] = synaptic events generated. */
+nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float reward, double out[10]);
 
 /* Phase timing of the step kernel over `cycles` cycles (one traced launch;
  * the cycles are simulated). Means over cycles, in ns: out[0] whole phase,

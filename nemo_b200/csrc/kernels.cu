@@ -651,7 +651,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	__shared__ uint32_t sPreF[MAX_BLOCKS + 2];    /* + the remote list of a shard */
 	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
 	__shared__ uint32_t sNFired, sNPost, sWork;
-	__shared__ unsigned long long sEvents, sPushed, sVisits, sHist, sAccW;
+	__shared__ unsigned long long sEvents, sPushed, sVisits;
 
 	const NetDev& net = A.net;
 	const uint32_t tid = threadIdx.x;
@@ -713,8 +713,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			sEvents = 0;
 			sPushed = 0;
 			sVisits = 0;
-			sHist = 0;
-			sAccW = 0;
 			if(doUpdate && b == 0) {
 				net.firedCountRing[(t + 1) & net.ringMask] = 0;
 				net.eventsRing[(t + 1) & net.ringMask] = 0;
@@ -832,10 +830,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					if(A.hostWords) A.hostWords[dw] = word;
 				}
 				if(net.stdp) {
-					const uint32_t rec = __ballot_sync(FULL, rfNew != 0ull && valid);
-					if(lane == 0) net.recentWords[size_t((t + 1u) & 1u) * net.nWords + dw] = rec;
-				}
-				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
 					const bool post = valid && ((rfNew >> net.postShift) & 1ull);
 					const uint32_t pm = __ballot_sync(FULL, post);
@@ -862,24 +856,41 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t ev = __reduce_add_sync(FULL, fired ? deg : 0u);
 					if(lane == 0) atomicAdd(&sEvents, (unsigned long long) ev);
 					if(net.deliver) {
-						const uint32_t np = pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
-						pushed += lane == 0 ? np : 0u;   /* warp total, counted once */
 						/* every block gathers these sources next phase: their
 						 * chunk of each block group, and the bucket starts of
-						 * the chunk, into L2 now; one (source, group) pair per
-						 * lane */
+						 * the chunk, go into L2 now; one (source, group) pair
+						 * per lane. The chunk bounds are loaded before the
+						 * delay-1 push, so that the two loads' latencies
+						 * overlap */
 						const uint32_t G = net.groups;
 						const uint32_t pairs = uint32_t(__popc(word)) * G;
-						for(uint32_t q = lane; q < pairs; q += 32u) {
+						uint32_t c0 = 0u, c1 = 0u;
+						size_t k0 = 0;
+						uint32_t bg = 0u;
+						if(lane < pairs) {
+							const uint32_t f = lane / G, g = lane - f * G;
+							const uint32_t src = dw * 32u + uint32_t(__fns(word, 0u, int(f) + 1));
+							const uint32_t g0 = __ldg(&net.groupFirst[g]);
+							bg = __ldg(&net.groupFirst[g + 1]) - g0;
+							k0 = size_t(g0) * nDev + size_t(src) * bg;
+							prefetchL2(net.segOff + k0, net.segOff + k0 + bg + 1u);
+							c0 = __ldg(&net.srcChunk[size_t(src) * G + g]);
+							c1 = __ldg(&net.srcChunk[size_t(src + 1u) * G + g]);
+						}
+						const uint32_t np = pushDelayOne(net, word, fired ? d1 : make_uint2(0u, 0u), (t + 1u) & 1u, lane);
+						pushed += lane == 0 ? np : 0u;   /* warp total, counted once */
+						if(lane < pairs) prefetchL2(net.fcm + c0, net.fcm + c1);
+						/* more than 32 pairs (several sources firing in a
+						 * warp of a network with many groups): the rest */
+						for(uint32_t q = lane + 32u; q < pairs; q += 32u) {
 							const uint32_t f = q / G, g = q - f * G;
 							const uint32_t src = dw * 32u + uint32_t(__fns(word, 0u, int(f) + 1));
 							const uint32_t g0 = __ldg(&net.groupFirst[g]);
-							const uint32_t bg = __ldg(&net.groupFirst[g + 1]) - g0;
-							const size_t k0 = size_t(g0) * nDev + size_t(src) * bg;
-							prefetchL2(net.segOff + k0, net.segOff + k0 + bg + 1u);
-							const uint32_t c0 = __ldg(&net.srcChunk[size_t(src) * G + g]);
-							const uint32_t c1 = __ldg(&net.srcChunk[size_t(src + 1u) * G + g]);
-							prefetchL2(net.fcm + c0, net.fcm + c1);
+							const uint32_t b2 = __ldg(&net.groupFirst[g + 1]) - g0;
+							const size_t k2 = size_t(g0) * nDev + size_t(src) * b2;
+							prefetchL2(net.segOff + k2, net.segOff + k2 + b2 + 1u);
+							prefetchL2(net.fcm + __ldg(&net.srcChunk[size_t(src) * G + g]),
+									net.fcm + __ldg(&net.srcChunk[size_t(src + 1u) * G + g]));
 						}
 					}
 				}
@@ -917,10 +928,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const uint32_t* flist = net.firedList + par * listStride;
 			const uint2* plist = net.postList + par * listStride;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
-			const uint32_t* recent = net.recentWords + size_t(t & 1u) * net.nWords;
 			const uint32_t slotPrev = uint32_t((t64 - 1u) % net.slots);
 			uint32_t pushed = 0;
-			uint64_t visited = 0, histReads = 0, accWrites = 0;
+			uint64_t visited = 0;
 			for(;;) {
 				uint32_t u = 0;
 				if(lane == 0) u = atomicAdd(&sWork, 1u);
@@ -1000,39 +1010,29 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						const uint32_t b0 = range.x + off;
 						const uint32_t cnt = range.y - off < item ? range.y - off : item;
 						visited += cnt;
+						/* the accumulators do not depend on the sources: load
+						 * them with the source words, before the histories */
 						uint32_t sd[STDP_PER_LANE];
-#pragma unroll
-						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
-							const uint32_t jj = lane + 32u * x;
-							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
-						}
-						/* a source whose history is 0 contributes nothing
-						 * (weightChange(0) = 0): only the others' histories
-						 * and accumulators are read */
-						bool hot[STDP_PER_LANE];
-#pragma unroll
-						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
-							const uint32_t jj = lane + 32u * x;
-							const uint32_t src = sd[x] >> 6;
-							hot[x] = jj < cnt && ((recent[src >> 5] >> (src & 31u)) & 1u);
-						}
-						uint64_t pre[STDP_PER_LANE];
 						int32_t old[STDP_PER_LANE];
 #pragma unroll
 						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
-							pre[x] = hot[x] ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
-							old[x] = hot[x] ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
-							histReads += hot[x] ? 1u : 0u;
+							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
+							old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
+						}
+						uint64_t pre[STDP_PER_LANE];
+#pragma unroll
+						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+							const uint32_t jj = lane + 32u * x;
+							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
 						}
 #pragma unroll
 						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
 							const uint32_t jj = lane + 32u * x;
-							if(hot[x]) {
+							if(jj < cnt) {
 								const int32_t dw = weightChange(pre[x], A.rule);
 								if(dw != 0) {
 									__stcs(&net.rcmAcc[b0 + jj], int32_t(uint32_t(old[x]) + uint32_t(dw)));
-									accWrites++;
 								}
 							}
 						}
@@ -1047,13 +1047,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				}
 			}
 			pushed = __reduce_add_sync(FULL, pushed);
-			histReads = __reduce_add_sync(FULL, uint32_t(histReads));
-			accWrites = __reduce_add_sync(FULL, uint32_t(accWrites));
 			if(lane == 0) {
 				if(pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
 				if(visited) atomicAdd(&sVisits, (unsigned long long) visited);
-				if(histReads) atomicAdd(&sHist, (unsigned long long) histReads);
-				if(accWrites) atomicAdd(&sAccW, (unsigned long long) accWrites);
 			}
 		}
 		__syncthreads();
@@ -1071,8 +1067,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			}
 			if(sPushed) atomicAdd(&net.stats[0], sPushed);
 			if(sVisits) atomicAdd(&net.stats[1], sVisits);
-			if(sHist) atomicAdd(&net.stats[4], sHist);
-			if(sAccW) atomicAdd(&net.stats[5], sAccW);
 		}
 		if(trace && tid == 0) trace[3] = globalTimer();
 		if(k < barriers) {
@@ -1356,10 +1350,6 @@ k_shard_inject(NetDev net, uint64_t t64, const uint32_t* allWords, uint32_t ownL
 		const uint64_t rfNew = (rfIn[n] << 1) | uint64_t(fired);
 		rfOut[n] = rfNew;
 		if(lane == 0) net.firedRing[size_t(t & net.ringMask) * net.nWords + w] = word;
-		if(net.stdp) {
-			const uint32_t rec = __ballot_sync(FULL, rfNew != 0ull);
-			if(lane == 0) net.recentWords[size_t(par ^ 1u) * net.nWords + w] = rec;
-		}
 		if(word) {
 			uint32_t base = 0;
 			if(lane == 0) base = atomicAdd(&net.remoteCnt[par], uint32_t(__popc(word)));

@@ -130,11 +130,6 @@ struct NetDev {
 
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
-	/* [2][nWords] by the parity of rf: bit n % 32 of word n / 32 is set when
-	 * neuron n's firing history (rf of the same parity) is not 0. A synapse
-	 * whose source's bit is clear has no spike in its STDP window, so the
-	 * accumulation skips it without reading the history */
-	uint32_t* recentWords;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
 	uint32_t stdpChunks;           /* STDP items per target (max in-degree / (32 x STDP_PER_LANE)) */
 	uint32_t applyChunks;          /* (32 x APPLY_PER_LANE)-synapse chunks per target */
@@ -164,9 +159,7 @@ struct NetDev {
 	uint32_t* remoteCnt;
 
 	/* cumulative counters: [0] synapses pushed, [1] STDP synapse visits,
-	 * [2] neurons fired, [3] synaptic events (fired x out-degree), [4] STDP
-	 * visits that read the source's history (and the accumulator), [5]
-	 * accumulators written; [6], [7] unused */
+	 * [2] neurons fired, [3] synaptic events (fired x out-degree) */
 	unsigned long long* stats;
 
 	/* grid barrier: [0] arrivals since the simulation was created (every

@@ -459,7 +459,7 @@ nemo_b200_timed_steps(nemo_simulation_t s, unsigned steps, unsigned cycles_per_s
 }
 
 nemo_status_t
-nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out[12])
+nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out[10])
 {
 	RETURN_CALL(s->sim.profile(cycles, reward, out));
 }

@@ -548,7 +548,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
 	m_net.noise = (float*) alloc(size_t(2) * m_nDev * 4);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
-	m_net.stats = (unsigned long long*) alloc(8 * 8);
+	m_net.stats = (unsigned long long*) alloc(4 * 8);
 	m_net.barrier = (unsigned*) alloc(4 * 4);
 	m_net.firedList = (uint32_t*) alloc(size_t(2) * B * ownN * 4);
 	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
@@ -559,7 +559,6 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		m_net.remoteCnt = (uint32_t*) alloc(2 * 4);
 	}
 	m_net.stdp = m_stdpOn ? 1 : 0;
-	if(m_stdpOn) m_net.recentWords = (uint32_t*) alloc(size_t(2) * m_net.nWords * 4);
 	m_net.stdpChunks = uint32_t(stdpChunks);
 	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
 	if(m_stdpOn) {
@@ -784,13 +783,24 @@ Simulation::checkDeviceError()
 void
 Simulation::decodeFired(const uint32_t* words, std::vector<unsigned>& out) const
 {
-	out.clear();
-	for(uint32_t w = 0; w < m_net.nWords; ++w) {
+	/* two words at a time: nearly all are 0 at ordinary firing rates */
+	out.resize(0);
+	const uint32_t nw = m_net.nWords;
+	uint32_t w = 0;
+	for(; w + 1 < nw; w += 2) {
+		uint64_t bits = uint64_t(words[w]) | (uint64_t(words[w + 1]) << 32);
+		while(bits) {
+			const uint32_t b = uint32_t(__builtin_ctzll(bits));
+			bits &= bits - 1;
+			out.push_back(m_d2g[size_t(w) * 32 + b]);
+		}
+	}
+	for(; w < nw; ++w) {
 		uint32_t bits = words[w];
 		while(bits) {
-			uint32_t b = uint32_t(__builtin_ctz(bits));
+			const uint32_t b = uint32_t(__builtin_ctz(bits));
 			bits &= bits - 1;
-			out.push_back(m_d2g[w * 32 + b]);
+			out.push_back(m_d2g[size_t(w) * 32 + b]);
 		}
 	}
 }
@@ -1701,15 +1711,7 @@ Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_
 void
 Simulation::readStats(uint64_t out[4])
 {
-	uint64_t all[8];
-	readAllStats(all);
-	std::copy(all, all + 4, out);
-}
-
-void
-Simulation::readAllStats(uint64_t out[8])
-{
-	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 8 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
+	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 4 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 }
 
@@ -1759,7 +1761,7 @@ Simulation::timedSteps(unsigned steps, unsigned cyclesPerStep, bool apply, float
 }
 
 void
-Simulation::profile(unsigned cycles, float reward, double out[12])
+Simulation::profile(unsigned cycles, float reward, double out[10])
 {
 	notShard("profile");
 	notExternal("profile");
@@ -1769,8 +1771,8 @@ Simulation::profile(unsigned cycles, float reward, double out[12])
 	NEMO_CUDA(cudaEventCreate(&e0));
 	NEMO_CUDA(cudaEventCreate(&e1));
 	NEMO_CUDA(cudaEventCreate(&e2));
-	uint64_t before[8], after[8];
-	readAllStats(before);
+	uint64_t before[4], after[4];
+	readStats(before);
 	NEMO_CUDA(cudaEventRecord(e0, stream));
 	launchBlock(m_cycle, cycles);
 	m_cycle += cycles;
@@ -1788,7 +1790,7 @@ Simulation::profile(unsigned cycles, float reward, double out[12])
 	cudaEventDestroy(e1);
 	cudaEventDestroy(e2);
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
-	readAllStats(after);
+	readStats(after);
 	checkDeviceError();
 	m_stateDirty = true;
 	out[0] = tc;
@@ -1801,8 +1803,6 @@ Simulation::profile(unsigned cycles, float reward, double out[12])
 	out[7] = (m_stdpOn && m_nrcm) ? ta : 0.0;
 	out[8] = double(m_nrcm);
 	out[9] = double(after[3] - before[3]);
-	out[10] = double(after[4] - before[4]);
-	out[11] = double(after[5] - before[5]);
 }
 
 void

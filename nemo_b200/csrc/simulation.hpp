@@ -141,10 +141,9 @@ public:
 	 * blocks, [2] 0, [3] synapses pushed, [4] neurons fired, [5] STDP synapse
 	 * visits, [6] neuron updates, [7] applyStdp ms, [8] plastic synapses,
 	 * [9] synaptic events generated. */
-	void profile(unsigned cycles, float reward, double out[12]);
+	void profile(unsigned cycles, float reward, double out[10]);
 
 	void readStats(uint64_t out[4]);
-	void readAllStats(uint64_t out[8]);
 	unsigned applyLaunches() const { return m_stdpOn && m_nrcm ? unsigned(m_applyGroups.size() - 1) : 0u; }
 
 	/* ---- batches of independent networks (Network::merge) ---- */
