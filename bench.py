@@ -712,17 +712,28 @@ def run_random1k(args):
     outdeg = spec.out_degree()
 
     def step_run(sim_lib, sim):
+        """nemo_step per cycle; each cycle's fired list is copied out of the
+        call's array (memmove) in the timed loop, its events counted after"""
         fptr = P(ctypes.c_uint)()
         nf = ctypes.c_size_t()
-        counts, events = [], 0
+        counts = []
+        buf = np.zeros(cycles * spec.neuron_count, np.uint32)
+        base = buf.ctypes.data
+        fref, nref = ctypes.byref(fptr), ctypes.byref(nf)
+        step = sim_lib.dll.nemo_step
+        h = sim.handle
+        pos = 0
         t0 = time.perf_counter()
         for _ in range(cycles):
-            if sim_lib.dll.nemo_step(sim.handle, None, 0, None, None, 0, ctypes.byref(fptr), ctypes.byref(nf)) != 0:
+            if step(h, None, 0, None, None, 0, fref, nref) != 0:
                 raise RuntimeError(sim_lib.dll.nemo_strerror().decode())
-            counts.append(nf.value)
-            if nf.value:
-                events += int(outdeg[np.ctypeslib.as_array(fptr, shape=(nf.value,))].sum())
-        return time.perf_counter() - t0, counts, events
+            n = nf.value
+            if n:
+                ctypes.memmove(base + 4 * pos, fptr, 4 * n)
+            pos += n
+            counts.append(n)
+        secs = time.perf_counter() - t0
+        return secs, counts, int(outdeg[buf[:pos]].sum())
 
     net = spec.build(Network(lib))
     sim = Simulation(net, Configuration(lib))
@@ -779,23 +790,30 @@ def run_mixed(args):
     P = ctypes.POINTER
 
     def run(sim_lib, sim, count, budget_s=None):
-        """per-cycle (seconds, events), stopping early past budget_s"""
+        """per-cycle (seconds, events), stopping early past budget_s; the
+        fired lists are copied out in the timed loop and counted after"""
         fptr = P(ctypes.c_uint)()
         nf = ctypes.c_size_t()
-        per = []
+        fref, nref = ctypes.byref(fptr), ctypes.byref(nf)
+        step = sim_lib.dll.nemo_step
+        h = sim.handle
+        args = [(f.ctypes.data_as(P(ctypes.c_uint)), f.size) for f in stim[:count]]
+        times, lists = [], []
         t_start = time.perf_counter()
         for c in range(count):
-            f = stim[c]
+            fp, fn = args[c]
             t0 = time.perf_counter()
-            st = sim_lib.dll.nemo_step(sim.handle, f.ctypes.data_as(P(ctypes.c_uint)), f.size, None, None, 0,
-                                       ctypes.byref(fptr), ctypes.byref(nf))
-            if st != 0:
+            if step(h, fp, fn, None, None, 0, fref, nref) != 0:
                 raise RuntimeError(sim_lib.dll.nemo_strerror().decode())
-            ev = int(outdeg[np.ctypeslib.as_array(fptr, shape=(nf.value,))].sum()) if nf.value else 0
-            per.append((time.perf_counter() - t0, ev))
-            if budget_s is not None and time.perf_counter() - t_start > budget_s:
+            out = np.empty(nf.value, np.uint32)
+            if nf.value:
+                ctypes.memmove(out.ctypes.data, fptr, 4 * nf.value)
+            t1 = time.perf_counter()
+            times.append(t1 - t0)
+            lists.append(out)
+            if budget_s is not None and t1 - t_start > budget_s:
                 break
-        return per
+        return [(dt, int(outdeg[f].sum())) for dt, f in zip(times, lists)]
 
     net = spec.build(Network(lib))
     sim = Simulation(net, Configuration(lib))

@@ -621,6 +621,51 @@ __device__ __forceinline__ uint32_t findList(const uint32_t* pre, uint32_t n, ui
 	return lo;
 }
 
+/* Block 0 of a resident launch, after its phase for command seq: wait (thread
+ * 0, at most idleNs) for command seq + 1 in host memory and copy it into the
+ * broadcast buffer of the next phase (parity (k + 1) & 1, so that the other
+ * blocks may still read this phase's); an exit command or the idle limit
+ * copies an exit. Called by all threads of block 0. */
+__device__ __forceinline__ void residentNext(const CycleArgs& A, uint32_t seq, uint32_t k, uint32_t warp, uint32_t lane)
+{
+	__shared__ uint32_t sOp, sNf, sNi;
+	if(threadIdx.x == 0) {
+		const size_t seqAddr = __cvta_generic_to_global(&A.cmd->seq);
+		const unsigned long long start = globalTimer();
+		uint32_t op = RESIDENT_EXIT, nf = 0u, ni = 0u;
+		for(;;) {
+			uint32_t v;
+			asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(seqAddr) : "memory");
+			if(v == seq + 1u) {
+				op = *(volatile const uint32_t*) &A.cmd->op;
+				nf = min(*(volatile const uint32_t*) &A.cmd->nf, INLINE_STIM_MAX);
+				ni = min(*(volatile const uint32_t*) &A.cmd->ni, INLINE_STIM_MAX);
+				break;
+			}
+			if(globalTimer() - start > A.idleNs) break;
+		}
+		sOp = op == RESIDENT_STEP ? RESIDENT_STEP : RESIDENT_EXIT;
+		sNf = nf;
+		sNi = ni;
+	}
+	__syncthreads();
+	ResidentCmd* c = A.bcast + ((k + 1u) & 1u);
+	if(warp == 0) {
+		const bool step = sOp == RESIDENT_STEP;
+		if(step && lane < sNf) c->f[lane] = *(volatile const uint32_t*) &A.cmd->f[lane];
+		if(step && lane < sNi) {
+			c->i[lane] = *(volatile const uint32_t*) &A.cmd->i[lane];
+			c->cur[lane] = *(volatile const float*) &A.cmd->cur[lane];
+		}
+		if(lane == 0) {
+			c->nf = step ? sNf : 0u;
+			c->ni = step ? sNi : 0u;
+			c->seq = seq + 1u;
+			c->op = sOp;
+		}
+	}
+}
+
 /* Add one forward-matrix record into current slot `slot` of its target
  * (E for w >= 0, else I), in shared memory or in net.acc */
 template<bool SMEM>
@@ -696,13 +741,38 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	 * gathering waits for the next launch, and nothing follows that phase,
 	 * so it needs no grid barrier after it (a one-cycle step has none at
 	 * all and runs as an ordinary launch) */
-	const bool lastPending = (A.carry & 2u) != 0u;
-	const uint32_t phases = A.cycles + (lastPending ? 0u : 1u);
+	/* resident stepping (CycleArgs::cmd): one update phase per command until
+	 * an exit command or the idle limit; the last cycle stays pending */
+	const bool resident = A.cmd != nullptr;
+	const bool lastPending = resident || (A.carry & 2u) != 0u;
+	const uint32_t phases = resident ? 0xffffffffu : A.cycles + (lastPending ? 0u : 1u);
 	const uint32_t barriers = lastPending && A.cycles ? A.cycles - 1u : A.cycles;
-	for(uint32_t k = 0; k < phases; ++k) {
+	uint32_t passed = 0;   /* grid barriers passed */
+	uint32_t k = 0;
+	for(; k < phases; ++k) {
 		const uint64_t t64 = first + k;
 		const uint32_t t = uint32_t(t64);
-		const bool doUpdate = k < A.cycles;
+		const bool doUpdate = resident || k < A.cycles;
+		/* this phase's stimulus: the launch's own (first phase), or the
+		 * command block 0 copied before the last grid barrier */
+		uint32_t stNf = 0u, stNi = 0u;
+		const uint32_t* stF = nullptr;
+		const uint32_t* stI = nullptr;
+		const float* stC = nullptr;
+		if(k == 0) {
+			stNf = A.inlineNf;
+			stNi = A.inlineNi;
+			stF = A.inlineF;
+			stI = A.inlineI;
+			stC = A.inlineCur;
+		} else if(resident) {
+			const ResidentCmd* c = A.bcast + (k & 1u);
+			stNf = c->nf;
+			stNi = c->ni;
+			stF = c->f;
+			stI = c->i;
+			stC = c->cur;
+		}
 		const bool doPrev = k > 0 || (A.carry & 1u);     /* gather and learn for cycle t-1 */
 		const uint32_t slotT = uint32_t(t64 % net.slots);
 
@@ -758,16 +828,17 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				 * needs it); cleared after the model has issued its loads,
 				 * so that nothing orders them behind it */
 				uint32_t stimWord = net.fstim[dw];
-				if(k == 0 && (A.inlineNf | A.inlineNi)) {
-					/* a step's short stimulus, from the parameters: this warp's
-					 * firing bits, and the currents of its own neurons (read
-					 * by the model below, by every lane of an HH neuron) */
-					for(uint32_t q = 0; q < A.inlineNf; ++q) {
-						const uint32_t x = A.inlineF[q];
+				if(stNf | stNi) {
+					/* a step's short stimulus, from the parameters or the
+					 * resident command: this warp's firing bits, and the
+					 * currents of its own neurons (read by the model below,
+					 * by every lane of an HH neuron) */
+					for(uint32_t q = 0; q < stNf; ++q) {
+						const uint32_t x = stF[q];
 						if((x >> 5) == dw) stimWord |= 1u << (x & 31u);
 					}
-					for(uint32_t q = 0; q < A.inlineNi; ++q) {
-						if(A.inlineI[q] == n) net.ext[n] = A.inlineCur[q];
+					for(uint32_t q = 0; q < stNi; ++q) {
+						if(stI[q] == n) net.ext[n] = stC[q];
 					}
 					__syncwarp();
 				}
@@ -1069,11 +1140,28 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			if(sVisits) atomicAdd(&net.stats[1], sVisits);
 		}
 		if(trace && tid == 0) trace[3] = globalTimer();
-		if(k < barriers) {
+		if(resident) {
+			/* the block's fired words of this command are in host memory:
+			 * report it; block 0 then waits for the next command and hands
+			 * it to every block through the grid barrier */
+			const uint32_t seqK = A.firstSeq + k;
+			if(tid == 0) {
+				__threadfence_system();
+				*(volatile uint32_t*) &A.doneWords[b] = seqK;
+			}
+			if(b == 0) residentNext(A, seqK, k, warp, lane);
+			if(!gridSync(net.barrier, barBase + (passed + 1u) * B, A.timeoutNs)) {
+				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
+				return;
+			}
+			passed++;
+			if(*(volatile const uint32_t*) &A.bcast[(k + 1u) & 1u].op != RESIDENT_STEP) break;
+		} else if(k < barriers) {
 			if(!gridSync(net.barrier, barBase + (k + 1u) * B, A.timeoutNs)) {
 				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
 				return;
 			}
+			passed++;
 		}
 		if(trace && tid == 0) trace[4] = globalTimer();
 	}
@@ -1115,7 +1203,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		/* every block has read barBase: they all arrived at this launch's
 		 * barriers, which block 0 has passed (a launch without barriers
 		 * leaves the count as it found it) */
-		if(barriers) *(volatile unsigned*) &net.barrier[1] = barBase + barriers * B;
+		if(passed) *(volatile unsigned*) &net.barrier[1] = barBase + passed * B;
+		if(resident) {
+			/* the commands up to firstSeq + k ran; the host waits for the
+			 * stream before anything else */
+			__threadfence_system();
+			*(volatile uint32_t*) A.exitInfo = ((A.firstSeq + k) << 1) | 1u;
+		}
 	}
 }
 
@@ -1519,7 +1613,7 @@ static cudaError_t
 launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
 {
 	const NetDev& net = args.net;
-	if(args.cycles <= 1u && (args.carry & 2u)) {
+	if(args.cycles <= 1u && (args.carry & 2u) && args.cmd == nullptr) {
 		/* one update phase and no grid barrier: the blocks never wait for one
 		 * another, so they need not be co-resident */
 		switch(net.threads) {

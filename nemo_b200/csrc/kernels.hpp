@@ -197,6 +197,21 @@ struct StdpRule {
 	int32_t fnPost[64];
 };
 
+/* A resident step kernel's command (resident stepping, CycleArgs::cmd): in
+ * host memory mapped into the device, written by the host (the fields, then
+ * seq) and read by block 0; and the same layout in device memory, where block
+ * 0 copies it for the other blocks. */
+const uint32_t RESIDENT_STEP = 1;
+const uint32_t RESIDENT_EXIT = 2;
+struct ResidentCmd {
+	uint32_t seq;           /* command number, written last */
+	uint32_t op;            /* RESIDENT_STEP or RESIDENT_EXIT */
+	uint32_t nf, ni;        /* stimulus entries (<= INLINE_STIM_MAX each) */
+	uint32_t f[INLINE_STIM_MAX];    /* firing stimulus, device indices */
+	uint32_t i[INLINE_STIM_MAX];    /* current stimulus, device indices (unique) */
+	float cur[INLINE_STIM_MAX];
+};
+
 struct CycleArgs {
 	NetDev net;
 	StdpRule rule;
@@ -233,6 +248,22 @@ struct CycleArgs {
 	/* when set, the first cycle is read from here instead of firstCycle and
 	 * advanced by the launch (launches replayed from a CUDA graph) */
 	uint64_t* cycleCounter;
+	/* resident stepping: when cmd is set, the launch runs one update phase
+	 * per command instead of `cycles` phases. The first command (seq
+	 * firstSeq) is this launch's inline stimulus; after each phase every
+	 * block writes the command's seq into doneWords[block] (mapped host
+	 * memory) once its fired words are in hostWords, and block 0 waits for
+	 * command seq + 1 in *cmd (mapped host memory) for at most idleNs, copies
+	 * it to *bcast (device) and the grid barrier hands it to every block. An
+	 * exit command, or no command within idleNs, ends the launch, which
+	 * leaves its last cycle pending (as carry bit 1) and writes exitInfo =
+	 * (last seq done << 1) | 1 (mapped host memory). */
+	const ResidentCmd* cmd;
+	ResidentCmd* bcast;
+	uint32_t* doneWords;
+	uint32_t* exitInfo;
+	uint32_t firstSeq;
+	unsigned long long idleNs;
 	/* optional phase trace (%globaltimer ns), [cycles + 1][block][9]: phase
 	 * start, (unused), last update warp done (0 when the block updates
 	 * nothing), all work done, barrier passed; then the summed durations of

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -693,6 +694,13 @@ Simulation::~Simulation()
 void
 Simulation::release()
 {
+	if(m_resident && m_rcmd) {
+		/* end the resident launch without raising (destructor) */
+		m_rcmd->op = RESIDENT_EXIT;
+		std::atomic_thread_fence(std::memory_order_release);
+		reinterpret_cast<volatile uint32_t*>(m_rcmd)[0] = ++m_rseq;
+		m_resident = false;
+	}
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
 	destroyGraph();
 	for(void** ev : {&m_evOut, &m_evIn, &m_evStaged}) {
@@ -704,6 +712,11 @@ Simulation::release()
 	m_allocs.clear();
 	if(m_hWords) cudaFreeHost(m_hWords);
 	if(m_stepWords) cudaFreeHost(m_stepWords);
+	if(m_rcmd) cudaFreeHost(m_rcmd);
+	if(m_rdone) cudaFreeHost(m_rdone);
+	m_rcmd = m_dRcmd = nullptr;
+	m_rdone = m_dRdone = nullptr;
+	m_rbcast = nullptr;
 	if(m_hStim) cudaFreeHost(m_hStim);
 	if(m_hCur) cudaFreeHost(m_hCur);
 	if(m_dStim) cudaFree(m_dStim);
@@ -904,6 +917,10 @@ const std::vector<unsigned>&
 Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
 {
 	notShard("step");
+	if(m_residentOn && !m_external && stepResident(fstim, nf, inidx, icur, ni)) {
+		return m_fired;
+	}
+	stopResident();
 	stageStimulus(fstim, nf, inidx, icur, ni, false);
 	if(m_external) runPlugins();
 	cudaStream_t stream = STREAM(m_stream);
@@ -919,6 +936,155 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	m_stateDirty = true;
 	decodeFired(m_stepWords, m_fired);
 	return m_fired;
+}
+
+/* A step's stimulus mapped to device indices into m_inline, when it fits in
+ * the kernel's inline arrays and every index exists (repeated current
+ * stimulus: the last entry wins); false otherwise, with nothing applied. */
+bool
+Simulation::mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
+{
+	if(nf > INLINE_STIM_MAX || ni > INLINE_STIM_MAX) return false;
+	InlineStim st;
+	for(size_t k = 0; k < nf; ++k) {
+		const uint32_t d = toDev(fstim[k]);
+		if(d == ~0u) return false;
+		st.f[st.nf++] = d;
+	}
+	for(size_t k = 0; k < ni; ++k) {
+		const uint32_t d = toDev(inidx[k]);
+		if(d == ~0u) return false;
+		uint32_t e = 0;
+		while(e < st.ni && st.i[e] != d) ++e;
+		if(e == st.ni) st.i[st.ni++] = d;
+		st.cur[e] = icur[k];
+	}
+	m_inline = st;
+	return true;
+}
+
+/* The resident step kernel's launch for command `seq`, whose stimulus is
+ * m_inline; the pending gathering of the last cycle, if any, is its first
+ * phase's. The launch keeps the current slots in shared memory while it
+ * stays. */
+void
+Simulation::launchResident(uint32_t seq)
+{
+	if(m_rcmd == nullptr) {
+		NEMO_CUDA(cudaHostAlloc((void**) &m_rcmd, sizeof(ResidentCmd), cudaHostAllocMapped));
+		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRcmd, m_rcmd, 0));
+		NEMO_CUDA(cudaHostAlloc((void**) &m_rdone, (size_t(m_blocks) + 1) * 4, cudaHostAllocMapped));
+		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRdone, m_rdone, 0));
+		m_rbcast = (ResidentCmd*) alloc(2 * sizeof(ResidentCmd));
+		std::memset(m_rcmd, 0, sizeof(ResidentCmd));
+	}
+	/* no command of this launch has run yet */
+	for(uint32_t b = 0; b <= m_blocks; ++b) reinterpret_cast<volatile uint32_t*>(m_rdone)[b] = 0u;
+	m_stepWords[m_net.nWords] = 0u;
+	CycleArgs a = m_args;
+	a.firstCycle = m_cycle;
+	a.cycles = 1;
+	a.carry = (m_pendingGather ? 1u : 0u) | 2u;
+	a.globalAcc = 0;
+	a.hostWords = m_dStepWords;
+	a.inlineNf = m_inline.nf;
+	a.inlineNi = m_inline.ni;
+	std::copy(m_inline.f, m_inline.f + m_inline.nf, a.inlineF);
+	std::copy(m_inline.i, m_inline.i + m_inline.ni, a.inlineI);
+	std::copy(m_inline.cur, m_inline.cur + m_inline.ni, a.inlineCur);
+	for(int gi = 0; gi < a.ngroups; ++gi) a.groups[gi].timerBase = uint32_t(m_timerBase);
+	a.cmd = m_dRcmd;
+	a.bcast = m_rbcast;
+	a.doneWords = m_dRdone;
+	a.exitInfo = m_dRdone + m_blocks;
+	a.firstSeq = seq;
+	/* a caller that stops stepping releases the device after this long */
+	a.idleNs = 1000ull * 1000;
+	launchCycles(a, m_stream);
+	NEMO_CUDA(cudaGetLastError());
+	m_inline.nf = m_inline.ni = 0;
+	m_pendingGather = true;
+	m_resident = true;
+}
+
+/* One cycle through the resident kernel; false when the stimulus does not
+ * fit the command (nothing done: the caller takes the ordinary path). */
+bool
+Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
+{
+	if(!mapInline(fstim, nf, inidx, icur, ni)) return false;
+	const uint32_t seq = ++m_rseq;
+	if(!m_resident) {
+		launchResident(seq);
+	} else {
+		ResidentCmd* c = m_rcmd;
+		c->op = RESIDENT_STEP;
+		c->nf = m_inline.nf;
+		c->ni = m_inline.ni;
+		std::copy(m_inline.f, m_inline.f + m_inline.nf, c->f);
+		std::copy(m_inline.i, m_inline.i + m_inline.ni, c->i);
+		std::copy(m_inline.cur, m_inline.cur + m_inline.ni, c->cur);
+		m_inline.nf = m_inline.ni = 0;
+		std::atomic_thread_fence(std::memory_order_release);
+		reinterpret_cast<volatile uint32_t*>(c)[0] = seq;   /* seq, last */
+	}
+	volatile const uint32_t* done = m_rdone;
+	const auto start = std::chrono::steady_clock::now();
+	uint32_t b = 0;
+	for(uint64_t spin = 0;; ++spin) {
+		while(b < m_blocks && done[b] == seq) ++b;
+		if(b == m_blocks) break;
+		const uint32_t exitInfo = done[m_blocks];
+		if(exitInfo != 0u && (exitInfo >> 1) < seq) {
+			/* the launch ended (idle) before this command: run it in a new one */
+			NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+			m_resident = false;
+			if(m_stepWords[m_net.nWords] != 0) {
+				fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
+			}
+			mapInline(fstim, nf, inidx, icur, ni);
+			launchResident(seq);
+			b = 0;
+			continue;
+		}
+		if((spin & 4095u) == 4095u) {
+			const cudaError_t e = cudaStreamQuery(STREAM(m_stream));
+			if(e != cudaErrorNotReady) {
+				/* the launch is over without this command done: a fault or a
+				 * barrier timeout */
+				m_resident = false;
+				NEMO_CUDA(e);
+				fail(NEMO_CUDA_ASSERTION_FAILURE, "resident step kernel ended without completing the cycle");
+			}
+			if(std::chrono::steady_clock::now() - start > std::chrono::seconds(20)) {
+				fail(NEMO_CUDA_ASSERTION_FAILURE, "resident step kernel: no answer within 20 s");
+			}
+		}
+	}
+	std::atomic_thread_fence(std::memory_order_acquire);
+	m_cycle++;
+	m_stateDirty = true;
+	decodeFired(m_stepWords, m_fired);
+	return true;
+}
+
+/* End the resident launch, if any: an exit command, then the stream drains.
+ * The last cycle's gathering stays pending. */
+void
+Simulation::stopResident()
+{
+	if(!m_resident) return;
+	ResidentCmd* c = m_rcmd;
+	c->op = RESIDENT_EXIT;
+	c->nf = c->ni = 0;
+	std::atomic_thread_fence(std::memory_order_release);
+	reinterpret_cast<volatile uint32_t*>(c)[0] = ++m_rseq;
+	m_resident = false;
+	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+	NEMO_CUDA(cudaGetLastError());
+	if(m_stepWords[m_net.nWords] != 0) {
+		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
+	}
 }
 
 /* One applyStdp on the simulation's stream. Every plastic weight is within
@@ -1059,6 +1225,7 @@ Simulation::event(void** ev)
 void
 Simulation::streamWait(void* stream)
 {
+	stopResident();
 	cudaEvent_t e = static_cast<cudaEvent_t>(event(&m_evOut));
 	NEMO_CUDA(cudaEventRecord(e, STREAM(m_stream)));
 	NEMO_CUDA(cudaStreamWaitEvent(STREAM(stream), e, 0));
@@ -1124,6 +1291,7 @@ Simulation::launchStep()
 void
 Simulation::flushPending()
 {
+	stopResident();
 	if(m_awaitDeliver) {
 		fail(NEMO_LOGIC_ERROR, "the last shard step's firing has not been delivered");
 	}
@@ -1143,6 +1311,7 @@ size_t
 Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni,
 		unsigned* firedOut, size_t firedCapacity)
 {
+	stopResident();
 	notShard("stepNoAlloc");
 	if(nf > NOALLOC_STIM_MAX || ni > NOALLOC_STIM_MAX) {
 		fail(NEMO_INVALID_INPUT, "nemo_b200_step_noalloc: at most " + std::to_string(NOALLOC_STIM_MAX)
@@ -1422,6 +1591,7 @@ Simulation::autotune(unsigned trialCycles, double ms[3])
 void
 Simulation::synchronize()
 {
+	stopResident();
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 	NEMO_CUDA(cudaGetLastError());
 }
@@ -1429,6 +1599,7 @@ Simulation::synchronize()
 const std::vector<unsigned>&
 Simulation::firedAt(uint64_t cycle)
 {
+	stopResident();
 	if(cycle >= m_cycle || m_cycle - cycle > m_ring) {
 		fail(NEMO_INVALID_INPUT, "firing of cycle " + std::to_string(cycle) + " is no longer (or not yet) available");
 	}
@@ -1463,6 +1634,7 @@ Simulation::applyStdp(float reward)
 void
 Simulation::syncStateToHost()
 {
+	stopResident();
 	if(!m_stateDirty) return;
 	cudaStream_t stream = STREAM(m_stream);
 	for(Group& g : m_groups) {
@@ -1512,6 +1684,7 @@ Simulation::getMembranePotential(unsigned gidx)
 void
 Simulation::setNeuron(unsigned gidx, unsigned nargs, const float* args)
 {
+	stopResident();
 	uint32_t i;
 	Group& g = groupOfDev(devIndex(gidx), &i);
 	if(nargs != g.type.nParam + g.type.nState) {
@@ -1538,6 +1711,7 @@ Simulation::setNeuron(unsigned gidx, unsigned nargs, const float* args)
 void
 Simulation::setNeuronState(unsigned gidx, unsigned var, float val)
 {
+	stopResident();
 	uint32_t i;
 	Group& g = groupOfDev(devIndex(gidx), &i);
 	checkVar(var, g.type.nState, "state variable");
@@ -1551,6 +1725,7 @@ Simulation::setNeuronState(unsigned gidx, unsigned var, float val)
 void
 Simulation::setNeuronParameter(unsigned gidx, unsigned param, float val)
 {
+	stopResident();
 	uint32_t i;
 	Group& g = groupOfDev(devIndex(gidx), &i);
 	checkVar(param, g.type.nParam, "parameter");
@@ -1620,6 +1795,7 @@ unsigned char Simulation::getSynapsePlastic(synapse_id id) const { return aux(id
 float
 Simulation::getSynapseWeight(synapse_id id)
 {
+	stopResident();
 	const Aux& a = aux(id);
 	if(!m_fcmHostValid) {
 		m_fcmHost.resize(m_nsyn);
@@ -1678,6 +1854,7 @@ Simulation::elapsedWallclock() const
 void
 Simulation::resetTimer()
 {
+	stopResident();
 	m_wallStart = std::chrono::steady_clock::now();
 	m_timerBase = m_cycle;
 }
@@ -1685,6 +1862,7 @@ Simulation::resetTimer()
 void
 Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_t n)
 {
+	stopResident();
 	const LibmTables& t = libmTables();
 	cudaStream_t stream = STREAM(m_stream);
 	uint32_t *d1, *d2, *ds, *dl;
@@ -1711,6 +1889,7 @@ Simulation::nrandProbe(const uint32_t* u1, const uint32_t* u2, float* out, size_
 void
 Simulation::readStats(uint64_t out[4])
 {
+	stopResident();
 	NEMO_CUDA(cudaMemcpyAsync(out, m_net.stats, 4 * 8, cudaMemcpyDeviceToHost, STREAM(m_stream)));
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 }
@@ -1883,6 +2062,7 @@ Simulation::trace(unsigned cycles, double out[14])
 uint64_t
 Simulation::expfCheck()
 {
+	stopResident();
 	const ExpExceptions& e = expExceptions();
 	cudaStream_t stream = STREAM(m_stream);
 	NetDev net = m_net;
@@ -1930,6 +2110,7 @@ Simulation::expfCheck()
 uint64_t
 Simulation::libmCheck()
 {
+	stopResident();
 	using namespace libm;
 	const LibmTables& t = libmTables();
 	cudaStream_t stream = STREAM(m_stream);

@@ -328,6 +328,23 @@ private:
 	bool m_awaitDeliver = false;    /* the last cycle's remote firing has not come in */
 	uint32_t* m_dAllWords = nullptr;
 
+	/* resident stepping: nemo_step's cycles go to a step kernel that stays on
+	 * the device and takes them from a command in mapped host memory
+	 * (CycleArgs::cmd), instead of one launch and one synchronisation per
+	 * call. Any other call first ends the resident launch (stopResident). */
+	bool stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni);
+	bool mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni);
+	void launchResident(uint32_t seq);
+	void stopResident();
+	bool m_resident = false;            /* a resident launch is on the stream */
+	bool m_residentOn = true;           /* nemo_step may use resident stepping */
+	uint32_t m_rseq = 0;                /* the last command number */
+	ResidentCmd* m_rcmd = nullptr;      /* mapped host memory */
+	ResidentCmd* m_dRcmd = nullptr;     /* its device address */
+	ResidentCmd* m_rbcast = nullptr;    /* device, [2] */
+	uint32_t* m_rdone = nullptr;        /* mapped host memory: [blocks] done words, then the exit word */
+	uint32_t* m_dRdone = nullptr;
+
 	/* events ordering the simulation's stream with a caller's stream, and
 	 * the end of the last staged stimulus copy (its pinned source is
 	 * rewritten only after it) */
