@@ -623,9 +623,9 @@ __device__ __forceinline__ uint32_t findList(const uint32_t* pre, uint32_t n, ui
 
 /* Block 0 of a resident launch, after its phase for command seq: wait (thread
  * 0, at most idleNs) for command seq + 1 in host memory and copy it into the
- * broadcast buffer of the next phase (parity (k + 1) & 1, so that the other
- * blocks may still read this phase's); an exit command or the idle limit
- * copies an exit. Called by all threads of block 0. */
+ * broadcast buffer of the next phase (parity (k + 1) & 1: the buffer of this
+ * phase's command stays as it is), its number last; an exit command or the
+ * idle limit copies an exit. Called by all threads of block 0. */
 __device__ __forceinline__ void residentNext(const CycleArgs& A, uint32_t seq, uint32_t k, uint32_t warp, uint32_t lane)
 {
 	__shared__ uint32_t sOp, sNf, sNi;
@@ -660,10 +660,43 @@ __device__ __forceinline__ void residentNext(const CycleArgs& A, uint32_t seq, u
 		if(lane == 0) {
 			c->nf = step ? sNf : 0u;
 			c->ni = step ? sNi : 0u;
-			c->seq = seq + 1u;
 			c->op = sOp;
 		}
+		__syncwarp();
+		if(lane == 0) {
+			/* the command's fields, then its number, for the other blocks */
+			const size_t seqAddr = __cvta_generic_to_global(&c->seq);
+			asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(seqAddr), "r"(seq + 1u) : "memory");
+		}
 	}
+	__syncthreads();
+}
+
+/* The other blocks of a resident launch, after their phase for command seq:
+ * wait (thread 0) for block 0's copy of command seq + 1. Block 0 forwards a
+ * command only after the host has seen every block's phase done, so nothing
+ * else orders the phases. Returns false when the wait gives up (limit
+ * timeoutNs; the launch is then in error). */
+__device__ __forceinline__ bool residentWait(const CycleArgs& A, uint32_t seq, uint32_t k)
+{
+	__shared__ int ok;
+	if(threadIdx.x == 0) {
+		const size_t seqAddr = __cvta_generic_to_global(&A.bcast[(k + 1u) & 1u].seq);
+		const unsigned long long start = globalTimer();
+		int good = 1;
+		for(uint32_t spins = 0;; ++spins) {
+			uint32_t v;
+			asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(seqAddr) : "memory");
+			if(v == seq + 1u) break;
+			if((spins & 255u) == 255u && globalTimer() - start > A.timeoutNs) {
+				good = 0;
+				break;
+			}
+		}
+		ok = good;
+	}
+	__syncthreads();
+	return ok != 0;
 }
 
 /* Add one forward-matrix record into current slot `slot` of its target
@@ -874,8 +907,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					switch(G.kind) {
 						case 0: {
 							/* the first cycle of a launch draws its noise here;
-							 * later ones use the draw made in the phase before */
-							const float nz = k == 0 ? drawNoise(net, G, i) : net.noise[par * nDev + n];
+							 * later ones use the draw made in the phase before
+							 * (a resident launch draws every cycle's here: it
+							 * cannot know whether a next cycle comes, and a
+							 * draw advances the generator) */
+							const float nz = (k == 0 || resident) ? drawNoise(net, G, i) : net.noise[par * nDev + n];
 							fired = modelIzhikevich(net, G, i, n, E, I, stim, nz);
 							break;
 						}
@@ -1149,12 +1185,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				__threadfence_system();
 				*(volatile uint32_t*) &A.doneWords[b] = seqK;
 			}
-			if(b == 0) residentNext(A, seqK, k, warp, lane);
-			if(!gridSync(net.barrier, barBase + (passed + 1u) * B, A.timeoutNs)) {
+			if(b == 0) {
+				residentNext(A, seqK, k, warp, lane);
+			} else if(!residentWait(A, seqK, k)) {
 				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
 				return;
 			}
-			passed++;
 			if(*(volatile const uint32_t*) &A.bcast[(k + 1u) & 1u].op != RESIDENT_STEP) break;
 		} else if(k < barriers) {
 			if(!gridSync(net.barrier, barBase + (k + 1u) * B, A.timeoutNs)) {

@@ -253,11 +253,13 @@ struct CycleArgs {
 	 * firstSeq) is this launch's inline stimulus; after each phase every
 	 * block writes the command's seq into doneWords[block] (mapped host
 	 * memory) once its fired words are in hostWords, and block 0 waits for
-	 * command seq + 1 in *cmd (mapped host memory) for at most idleNs, copies
-	 * it to *bcast (device) and the grid barrier hands it to every block. An
-	 * exit command, or no command within idleNs, ends the launch, which
-	 * leaves its last cycle pending (as carry bit 1) and writes exitInfo =
-	 * (last seq done << 1) | 1 (mapped host memory). */
+	 * command seq + 1 in *cmd (mapped host memory) for at most idleNs and
+	 * copies it to bcast[(phase + 1) & 1] (device), where the other blocks
+	 * wait for it. The host issues a command only after every block's done
+	 * word has come, so no grid barrier separates the phases. An exit
+	 * command, or no command within idleNs, ends the launch, which leaves its
+	 * last cycle pending (as carry bit 1) and writes exitInfo = (last seq done
+	 * << 1) | 1 (mapped host memory). */
 	const ResidentCmd* cmd;
 	ResidentCmd* bcast;
 	uint32_t* doneWords;
