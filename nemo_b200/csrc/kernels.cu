@@ -621,46 +621,62 @@ __device__ __forceinline__ uint32_t findList(const uint32_t* pre, uint32_t n, ui
 	return lo;
 }
 
-/* Block 0 of a resident launch, after its phase for command seq: wait (thread
- * 0, at most idleNs) for command seq + 1 in host memory and copy it into the
- * broadcast buffer of the next phase (parity (k + 1) & 1: the buffer of this
- * phase's command stays as it is), its number last; an exit command or the
- * idle limit copies an exit. Called by all threads of block 0. */
+/* Block 0 of a resident launch, after its phase for command seq: wait (first
+ * warp, at most idleNs) for command seq + 1 in host memory (ResidentHostCmd:
+ * every lane reads one chunk per try, and the command is taken when each
+ * chunk its payload needs carries seq + 1) and copy it into the broadcast
+ * buffer of the next phase (parity (k + 1) & 1: the buffer of this phase's
+ * command stays as it is), its number last; an exit command or the idle limit
+ * copies an exit. Called by all threads of block 0. */
 __device__ __forceinline__ void residentNext(const CycleArgs& A, uint32_t seq, uint32_t k, uint32_t warp, uint32_t lane)
 {
-	__shared__ uint32_t sOp, sNf, sNi;
-	if(threadIdx.x == 0) {
-		const size_t seqAddr = __cvta_generic_to_global(&A.cmd->seq);
+	if(warp == 0) {
+		const size_t chunkAddr = __cvta_generic_to_global(&A.cmd->c[lane]);
 		const unsigned long long start = globalTimer();
-		uint32_t op = RESIDENT_EXIT, nf = 0u, ni = 0u;
+		uint4 ch = make_uint4(0u, 0u, 0u, 0u);
+		bool got = false;
 		for(;;) {
-			uint32_t v;
-			asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(seqAddr) : "memory");
-			if(v == seq + 1u) {
-				op = *(volatile const uint32_t*) &A.cmd->op;
-				nf = min(*(volatile const uint32_t*) &A.cmd->nf, INLINE_STIM_MAX);
-				ni = min(*(volatile const uint32_t*) &A.cmd->ni, INLINE_STIM_MAX);
+			asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+					: "=r"(ch.x), "=r"(ch.y), "=r"(ch.z), "=r"(ch.w) : "l"(chunkAddr) : "memory");
+			/* chunk 0: {seq, op, nf, ni}; the payload needs ceil((3 + nf +
+			 * 2 ni) / 3) chunks */
+			const uint32_t nf = min(__shfl_sync(FULL, ch.z, 0), INLINE_STIM_MAX);
+			const uint32_t ni = min(__shfl_sync(FULL, ch.w, 0), INLINE_STIM_MAX);
+			const uint32_t need = min((3u + nf + 2u * ni + 2u) / 3u, RESIDENT_CHUNKS);
+			const uint32_t fresh = __ballot_sync(FULL, ch.x == seq + 1u);
+			const uint32_t want = need >= 32u ? FULL : ((1u << need) - 1u);
+			if((fresh & want) == want) {
+				got = true;
 				break;
 			}
 			if(globalTimer() - start > A.idleNs) break;
 		}
-		sOp = op == RESIDENT_STEP ? RESIDENT_STEP : RESIDENT_EXIT;
-		sNf = nf;
-		sNi = ni;
-	}
-	__syncthreads();
-	ResidentCmd* c = A.bcast + ((k + 1u) & 1u);
-	if(warp == 0) {
-		const bool step = sOp == RESIDENT_STEP;
-		if(step && lane < sNf) c->f[lane] = *(volatile const uint32_t*) &A.cmd->f[lane];
-		if(step && lane < sNi) {
-			c->i[lane] = *(volatile const uint32_t*) &A.cmd->i[lane];
-			c->cur[lane] = *(volatile const float*) &A.cmd->cur[lane];
+		/* the payload words, in lane order: word 3 l + j is chunk l's w[j] */
+		ResidentCmd* c = A.bcast + ((k + 1u) & 1u);
+		const uint32_t op = got ? __shfl_sync(FULL, ch.y, 0) : RESIDENT_EXIT;
+		const bool step = op == RESIDENT_STEP;
+		const uint32_t nf = step ? min(__shfl_sync(FULL, ch.z, 0), INLINE_STIM_MAX) : 0u;
+		const uint32_t ni = step ? min(__shfl_sync(FULL, ch.w, 0), INLINE_STIM_MAX) : 0u;
+		/* payload word p (p >= 3) is chunk p / 3's word p % 3; every lane
+		 * takes part in each round's shuffles */
+		for(uint32_t base = 3u; base < 3u + nf + 2u * ni; base += 32u) {
+			const uint32_t p = base + lane;
+			const uint32_t l = min(p / 3u, 31u), j = p - 3u * (p / 3u);
+			const uint32_t y = __shfl_sync(FULL, ch.y, l);
+			const uint32_t z = __shfl_sync(FULL, ch.z, l);
+			const uint32_t w = __shfl_sync(FULL, ch.w, l);
+			const uint32_t v = j == 0u ? y : (j == 1u ? z : w);
+			const uint32_t q = p - 3u;
+			if(p < 3u + nf + 2u * ni) {
+				if(q < nf) c->f[q] = v;
+				else if(q < nf + ni) c->i[q - nf] = v;
+				else c->cur[q - nf - ni] = __uint_as_float(v);
+			}
 		}
 		if(lane == 0) {
-			c->nf = step ? sNf : 0u;
-			c->ni = step ? sNi : 0u;
-			c->op = sOp;
+			c->nf = nf;
+			c->ni = ni;
+			c->op = step ? RESIDENT_STEP : RESIDENT_EXIT;
 		}
 		__syncwarp();
 		if(lane == 0) {
@@ -728,7 +744,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	extern __shared__ int2 sAcc[];
 	__shared__ uint32_t sPreF[MAX_BLOCKS + 2];    /* + the remote list of a shard */
 	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
-	__shared__ uint32_t sNFired, sNPost, sWork;
+	__shared__ uint32_t sNFired, sNPost, sWork, sListCnt;
 	__shared__ unsigned long long sEvents, sPushed, sVisits;
 
 	const NetDev& net = A.net;
@@ -813,6 +829,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			sNFired = 0;
 			sNPost = 0;
 			sWork = 0;
+			sListCnt = 0;
 			sEvents = 0;
 			sPushed = 0;
 			sVisits = 0;
@@ -934,7 +951,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				const uint32_t word = __ballot_sync(FULL, fired);
 				if(lane == 0) {
 					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
-					if(A.hostWords) A.hostWords[dw] = word;
+					if(A.hostWords && word) {
+						const uint32_t e = atomicAdd(&sListCnt, 1u);
+						uint32_t* L = A.hostWords + 2u + size_t(b) * (2u + 2u * net.ownWarps);
+						*reinterpret_cast<uint2*>(&L[2u + 2u * e]) = make_uint2(word, dw);
+					}
 				}
 				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
@@ -1161,6 +1182,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		}
 		__syncthreads();
 		if(tid == 0) {
+			if(doUpdate && A.hostWords) A.hostWords[2u + size_t(b) * (2u + 2u * net.ownWarps)] = sListCnt;
 			if(doUpdate) {
 				const uint32_t par = t & 1u;
 				net.firedCnt[par * B + b] = sNFired;
@@ -1188,13 +1210,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			if(b == 0) {
 				residentNext(A, seqK, k, warp, lane);
 			} else if(!residentWait(A, seqK, k)) {
-				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
+				if(A.hostWords && tid == 0) A.hostWords[0] = 1u;
 				return;
 			}
 			if(*(volatile const uint32_t*) &A.bcast[(k + 1u) & 1u].op != RESIDENT_STEP) break;
 		} else if(k < barriers) {
 			if(!gridSync(net.barrier, barBase + (k + 1u) * B, A.timeoutNs)) {
-				if(A.hostWords && tid == 0) A.hostWords[net.nWords] = 1u;
+				if(A.hostWords && tid == 0) A.hostWords[0] = 1u;
 				return;
 			}
 			passed++;

@@ -197,12 +197,29 @@ struct StdpRule {
 	int32_t fnPost[64];
 };
 
-/* A resident step kernel's command (resident stepping, CycleArgs::cmd): in
- * host memory mapped into the device, written by the host (the fields, then
- * seq) and read by block 0; and the same layout in device memory, where block
- * 0 copies it for the other blocks. */
+/* A resident step kernel's command (resident stepping, CycleArgs::cmd).
+ *
+ * In host memory mapped into the device, as 16-byte chunks {seq, three
+ * payload words}: the host writes each chunk's payload, then its seq. Block
+ * 0's first warp reads all chunks at once (one read across the bus per try)
+ * and takes the command when every chunk it needs carries the command's
+ * number; a 16-byte read of one cache line sees the line at one instant, so a
+ * chunk with the new number has the new payload. Payload: op, nf, ni, then
+ * nf firing-stimulus device indices, ni current-stimulus device indices
+ * (unique) and ni currents (float bits); at most RESIDENT_CHUNKS chunks.
+ *
+ * In device memory (ResidentCmd), block 0's copy for the other blocks, its
+ * number written last. */
 const uint32_t RESIDENT_STEP = 1;
 const uint32_t RESIDENT_EXIT = 2;
+const uint32_t RESIDENT_CHUNKS = 32;
+struct ResidentChunk {
+	uint32_t seq;
+	uint32_t w[3];
+};
+struct ResidentHostCmd {
+	ResidentChunk c[RESIDENT_CHUNKS];
+};
 struct ResidentCmd {
 	uint32_t seq;           /* command number, written last */
 	uint32_t op;            /* RESIDENT_STEP or RESIDENT_EXIT */
@@ -231,9 +248,12 @@ struct CycleArgs {
 	 * array the shared copy is loaded from and spilled to): a launch of one
 	 * phase saves the copy in and out */
 	int globalAcc;
-	/* a one-cycle step's output in mapped host memory ([nWords + 1]): every
-	 * warp's fired word, and 1 in the last word when a grid barrier timed out
-	 * (the host zeroes it first); null otherwise */
+	/* a step's output in mapped host memory, null otherwise: word 0 is set to
+	 * 1 when a grid barrier timed out (the host zeroes it first); then per
+	 * block b, at 2 + b * (2 + 2 ownWarps), the count of its warps that fired
+	 * in the cycle, a pad word, and that many {fired word, device warp} pairs
+	 * (8-byte aligned, in no order; as 64-bit words they sort by warp): only
+	 * the words that are not 0 cross to the host */
 	uint32_t* hostWords;
 	/* a one-cycle step's stimulus when it is short (device indices; the
 	 * owner warp of each neuron applies it before the update), in place of
@@ -252,7 +272,7 @@ struct CycleArgs {
 	 * per command instead of `cycles` phases. The first command (seq
 	 * firstSeq) is this launch's inline stimulus; after each phase every
 	 * block writes the command's seq into doneWords[block] (mapped host
-	 * memory) once its fired words are in hostWords, and block 0 waits for
+	 * memory) once its fired words' list is in hostWords, and block 0 waits for
 	 * command seq + 1 in *cmd (mapped host memory) for at most idleNs and
 	 * copies it to bcast[(phase + 1) & 1] (device), where the other blocks
 	 * wait for it. The host issues a command only after every block's done
@@ -260,7 +280,7 @@ struct CycleArgs {
 	 * command, or no command within idleNs, ends the launch, which leaves its
 	 * last cycle pending (as carry bit 1) and writes exitInfo = (last seq done
 	 * << 1) | 1 (mapped host memory). */
-	const ResidentCmd* cmd;
+	const ResidentHostCmd* cmd;
 	ResidentCmd* bcast;
 	uint32_t* doneWords;
 	uint32_t* exitInfo;

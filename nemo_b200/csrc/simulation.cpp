@@ -662,7 +662,8 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_args.timeoutNs = 10ull * 1000 * 1000 * 1000;
 
 	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords + 1) * 4));
-	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, size_t(m_net.nWords + 1) * 4, cudaHostAllocMapped));
+	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, (2 + size_t(m_blocks) * (2 + 2 * size_t(m_net.ownWarps))) * 4,
+				cudaHostAllocMapped));
 	NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dStepWords, m_stepWords, 0));
 	/* plugin models derive their initial state (b200_init_neurons) */
 	for(const Group& g : m_groups) {
@@ -696,9 +697,7 @@ Simulation::release()
 {
 	if(m_resident && m_rcmd) {
 		/* end the resident launch without raising (destructor) */
-		m_rcmd->op = RESIDENT_EXIT;
-		std::atomic_thread_fence(std::memory_order_release);
-		reinterpret_cast<volatile uint32_t*>(m_rcmd)[0] = ++m_rseq;
+		postCommand(++m_rseq, RESIDENT_EXIT);
 		m_resident = false;
 	}
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
@@ -818,6 +817,41 @@ Simulation::decodeFired(const uint32_t* words, std::vector<unsigned>& out) const
 	}
 }
 
+/* The fired neurons of the last step from the per-block lists the kernel
+ * wrote into mapped memory (CycleArgs::hostWords): blocks own ascending warp
+ * ranges, and a block's few entries are put in warp order here. */
+template<class Emit>
+void
+Simulation::decodeStepList(Emit emit)
+{
+	uint32_t* base = m_stepWords + 2;
+	const size_t stride = 2 + 2 * size_t(m_net.ownWarps);
+	for(uint32_t b = 0; b < m_blocks; ++b) {
+		uint32_t* L = base + b * stride;
+		const uint32_t n = L[0];
+		if(n == 0) continue;
+		/* {word, warp} pairs: as 64-bit words they sort by warp */
+		uint64_t* e = reinterpret_cast<uint64_t*>(L + 2);
+		std::sort(e, e + n);
+		for(uint32_t k = 0; k < n; ++k) {
+			const size_t w = size_t(e[k] >> 32);
+			uint32_t bits = uint32_t(e[k]);
+			while(bits) {
+				const uint32_t bit = uint32_t(__builtin_ctz(bits));
+				bits &= bits - 1;
+				emit(m_d2g[w * 32 + bit]);
+			}
+		}
+	}
+}
+
+void
+Simulation::decodeStepList(std::vector<unsigned>& out)
+{
+	out.resize(0);
+	decodeStepList([&out](unsigned g) { out.push_back(g); });
+}
+
 /* src/nemo/nemo_c.cpp:439-461 and cpu/Simulation.cpp:140-163: firing
  * stimulus, then current stimulus; an invalid index raises after the entries
  * before it have been applied. */
@@ -929,12 +963,12 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	launchStep();
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	NEMO_CUDA(cudaGetLastError());
-	if(m_stepWords[m_net.nWords] != 0) {
+	if(m_stepWords[0] != 0) {
 		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
 	}
 	m_cycle++;
 	m_stateDirty = true;
-	decodeFired(m_stepWords, m_fired);
+	decodeStepList(m_fired);
 	return m_fired;
 }
 
@@ -971,16 +1005,16 @@ void
 Simulation::launchResident(uint32_t seq)
 {
 	if(m_rcmd == nullptr) {
-		NEMO_CUDA(cudaHostAlloc((void**) &m_rcmd, sizeof(ResidentCmd), cudaHostAllocMapped));
+		NEMO_CUDA(cudaHostAlloc((void**) &m_rcmd, sizeof(ResidentHostCmd), cudaHostAllocMapped));
 		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRcmd, m_rcmd, 0));
 		NEMO_CUDA(cudaHostAlloc((void**) &m_rdone, (size_t(m_blocks) + 1) * 4, cudaHostAllocMapped));
 		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRdone, m_rdone, 0));
 		m_rbcast = (ResidentCmd*) alloc(2 * sizeof(ResidentCmd));
-		std::memset(m_rcmd, 0, sizeof(ResidentCmd));
+		std::memset(m_rcmd, 0, sizeof(ResidentHostCmd));
 	}
 	/* no command of this launch has run yet */
 	for(uint32_t b = 0; b <= m_blocks; ++b) reinterpret_cast<volatile uint32_t*>(m_rdone)[b] = 0u;
-	m_stepWords[m_net.nWords] = 0u;
+	m_stepWords[0] = 0u;
 	CycleArgs a = m_args;
 	a.firstCycle = m_cycle;
 	a.cycles = 1;
@@ -1007,26 +1041,45 @@ Simulation::launchResident(uint32_t seq)
 	m_resident = true;
 }
 
+void
+Simulation::postCommand(uint32_t seq, uint32_t op)
+{
+	const bool step = op == RESIDENT_STEP;
+	const uint32_t nf = step ? m_inline.nf : 0u, ni = step ? m_inline.ni : 0u;
+	uint32_t payload[3 * RESIDENT_CHUNKS];
+	uint32_t n = 0;
+	payload[n++] = op;
+	payload[n++] = nf;
+	payload[n++] = ni;
+	for(uint32_t k = 0; k < nf; ++k) payload[n++] = m_inline.f[k];
+	for(uint32_t k = 0; k < ni; ++k) payload[n++] = m_inline.i[k];
+	for(uint32_t k = 0; k < ni; ++k) std::memcpy(&payload[n++], &m_inline.cur[k], 4);
+	const uint32_t chunks = (n + 2) / 3;
+	volatile uint32_t* c = reinterpret_cast<volatile uint32_t*>(m_rcmd->c);
+	for(uint32_t k = 0; k < chunks; ++k) {
+		/* the chunk's payload, then its number (x86 keeps the store order) */
+		for(uint32_t j = 0; j < 3; ++j) c[4 * k + 1 + j] = 3 * k + j < n ? payload[3 * k + j] : 0u;
+		std::atomic_thread_fence(std::memory_order_release);
+		c[4 * k] = seq;
+	}
+}
+
 /* One cycle through the resident kernel; false when the stimulus does not
  * fit the command (nothing done: the caller takes the ordinary path). */
 bool
 Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni)
 {
 	if(!mapInline(fstim, nf, inidx, icur, ni)) return false;
+	if(!fitsCommand()) {
+		m_inline.nf = m_inline.ni = 0;
+		return false;
+	}
 	const uint32_t seq = ++m_rseq;
 	if(!m_resident) {
 		launchResident(seq);
 	} else {
-		ResidentCmd* c = m_rcmd;
-		c->op = RESIDENT_STEP;
-		c->nf = m_inline.nf;
-		c->ni = m_inline.ni;
-		std::copy(m_inline.f, m_inline.f + m_inline.nf, c->f);
-		std::copy(m_inline.i, m_inline.i + m_inline.ni, c->i);
-		std::copy(m_inline.cur, m_inline.cur + m_inline.ni, c->cur);
+		postCommand(seq, RESIDENT_STEP);
 		m_inline.nf = m_inline.ni = 0;
-		std::atomic_thread_fence(std::memory_order_release);
-		reinterpret_cast<volatile uint32_t*>(c)[0] = seq;   /* seq, last */
 	}
 	volatile const uint32_t* done = m_rdone;
 	const auto start = std::chrono::steady_clock::now();
@@ -1039,7 +1092,7 @@ Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx
 			/* the launch ended (idle) before this command: run it in a new one */
 			NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 			m_resident = false;
-			if(m_stepWords[m_net.nWords] != 0) {
+			if(m_stepWords[0] != 0) {
 				fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
 			}
 			mapInline(fstim, nf, inidx, icur, ni);
@@ -1064,7 +1117,7 @@ Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx
 	std::atomic_thread_fence(std::memory_order_acquire);
 	m_cycle++;
 	m_stateDirty = true;
-	decodeFired(m_stepWords, m_fired);
+	decodeStepList(m_fired);
 	return true;
 }
 
@@ -1074,15 +1127,11 @@ void
 Simulation::stopResident()
 {
 	if(!m_resident) return;
-	ResidentCmd* c = m_rcmd;
-	c->op = RESIDENT_EXIT;
-	c->nf = c->ni = 0;
-	std::atomic_thread_fence(std::memory_order_release);
-	reinterpret_cast<volatile uint32_t*>(c)[0] = ++m_rseq;
+	postCommand(++m_rseq, RESIDENT_EXIT);
 	m_resident = false;
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 	NEMO_CUDA(cudaGetLastError());
-	if(m_stepWords[m_net.nWords] != 0) {
+	if(m_stepWords[0] != 0) {
 		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
 	}
 }
@@ -1279,7 +1328,7 @@ Simulation::shardDeliverAsync(const uint32_t* allDev, void* stream)
 void
 Simulation::launchStep()
 {
-	m_stepWords[m_net.nWords] = 0u;
+	m_stepWords[0] = 0u;
 	launchBlock(m_cycle, 1, (m_pendingGather ? 1u : 0u) | 2u, m_stepGlobalAcc, m_dStepWords, &m_inline);
 	m_inline.nf = m_inline.ni = 0;
 	m_pendingGather = true;
@@ -1378,20 +1427,13 @@ Simulation::stepNoAlloc(const unsigned* fstim, size_t nf, const unsigned* inidx,
 	launchStep();
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	NEMO_CUDA(cudaGetLastError());
-	if(m_stepWords[m_net.nWords] != 0) {
+	if(m_stepWords[0] != 0) {
 		fail(NEMO_CUDA_ASSERTION_FAILURE, "step kernel: a grid barrier timed out; the simulation state is invalid");
 	}
 	m_cycle++;
 	m_stateDirty = true;
 	size_t count = 0;
-	for(uint32_t w = 0; w < m_net.nWords; ++w) {
-		uint32_t bits = m_stepWords[w];
-		while(bits) {
-			uint32_t b = uint32_t(__builtin_ctz(bits));
-			bits &= bits - 1;
-			firedOut[count++] = m_d2g[w * 32 + b];
-		}
-	}
+	decodeStepList([&](unsigned g) { firedOut[count++] = g; });
 	return count;
 }
 

@@ -233,6 +233,10 @@ private:
 	void syncStateToHost();
 	void* alloc(size_t bytes);
 	void decodeFired(const uint32_t* words, std::vector<unsigned>& out) const;
+	/* the fired neurons of the last step from the kernel's per-block lists in
+	 * mapped memory (CycleArgs::hostWords), in simulation order */
+	template<class Emit> void decodeStepList(Emit emit);
+	void decodeStepList(std::vector<unsigned>& out);
 
 	unsigned m_nNeurons;
 	uint32_t m_nDev;
@@ -294,7 +298,7 @@ private:
 
 	/* pinned staging */
 	uint32_t* m_hWords;        /* one firing bitmap, then the barrier error word */
-	uint32_t* m_stepWords = nullptr;    /* mapped: a step's firing bitmap and error word */
+	uint32_t* m_stepWords = nullptr;    /* mapped: a step's error word and fired-word lists (CycleArgs::hostWords) */
 	InlineStim m_inline;
 	uint32_t* m_dStepWords = nullptr;   /* its device address */
 	uint32_t* m_hStim;         /* fstim + istim indices */
@@ -334,13 +338,17 @@ private:
 	 * call. Any other call first ends the resident launch (stopResident). */
 	bool stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni);
 	bool mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni);
+	bool fitsCommand() const { return 3u + m_inline.nf + 2u * m_inline.ni <= 3u * RESIDENT_CHUNKS; }
 	void launchResident(uint32_t seq);
 	void stopResident();
 	bool m_resident = false;            /* a resident launch is on the stream */
 	bool m_residentOn = true;           /* nemo_step may use resident stepping */
 	uint32_t m_rseq = 0;                /* the last command number */
-	ResidentCmd* m_rcmd = nullptr;      /* mapped host memory */
-	ResidentCmd* m_dRcmd = nullptr;     /* its device address */
+	ResidentHostCmd* m_rcmd = nullptr;  /* mapped host memory */
+	ResidentHostCmd* m_dRcmd = nullptr; /* its device address */
+	/* write command `seq` (op, and m_inline's stimulus for a step) into
+	 * m_rcmd: each chunk's payload, then its number */
+	void postCommand(uint32_t seq, uint32_t op);
 	ResidentCmd* m_rbcast = nullptr;    /* device, [2] */
 	uint32_t* m_rdone = nullptr;        /* mapped host memory: [blocks] done words, then the exit word */
 	uint32_t* m_dRdone = nullptr;
