@@ -944,7 +944,13 @@ def run_ncu_case(args):
     built, --warmup steps of 100 cycles + applyStdp, then --steps more, all
     through nemo_b200_timed_steps; k_cycles launches: warmup + steps, each
     followed by the applyStdp launches. Prints the device time of the last
-    steps."""
+    steps. With --batched: the 256 networks of the batched form, warmup +
+    steps launches of 100 cycles. With --bptt: the differentiable form's
+    configuration, warmup + steps forward and adjoint passes."""
+    if args.batched:
+        return _ncu_case_batched(args)
+    if args.bptt:
+        return _ncu_case_bptt(args)
     wl = workload(args.small)
     lib = Library()
     sim, _, build_s = build_sim(lib, wl)
@@ -956,6 +962,47 @@ def run_ncu_case(args):
     print(json.dumps({"case": wl["name"], "steps": max(args.steps, 1), "warmup": max(args.warmup, 1),
                       "ms_per_step": round(out[0] / max(args.steps, 1), 4), "build_s": round(build_s, 2),
                       "apply_launches_per_step": apply_launches(sim, lib)}), flush=True)
+
+
+def _ncu_case_batched(args):
+    from nemo_b200.netgen import batched_sizes
+    lib = Library()
+    d = lib.dll
+    d.nemo_b200_new_batch.restype = ctypes.c_void_p
+    d.nemo_b200_new_batch.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_size_t, ctypes.c_void_p]
+    d.nemo_b200_run.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p]
+    count = args.batch_count
+    sizes = batched_sizes(count, 500, 20000, seed=3)
+    sig = np.random.default_rng(4).uniform(3.0, 7.0, size=count)
+    nets = [netgen.izhikevich_random(int(sizes[j]), 100, dmax=20, seed=1000 + j, sigma_exc=float(sig[j]),
+                                     sigma_inh=float(0.4 * sig[j])).build(Network(lib)) for j in range(count)]
+    handles = (ctypes.c_void_p * count)(*[n.handle for n in nets])
+    batch = d.nemo_b200_new_batch(handles, count, Configuration(lib).handle)
+    if not batch:
+        raise RuntimeError(d.nemo_strerror().decode())
+    del nets
+    t0 = time.perf_counter()
+    for _ in range(max(args.warmup, 1) + max(args.steps, 1)):
+        lib.call("nemo_b200_run", batch, CYCLES_PER_STEP, None, None)
+    print(json.dumps({"case": "izhikevich-batch-%d-m100" % count, "launches": max(args.warmup, 1) + max(args.steps, 1),
+                      "seconds": round(time.perf_counter() - t0, 3)}), flush=True)
+    d.nemo_delete_simulation.argtypes = [ctypes.c_void_p]
+    d.nemo_delete_simulation(batch)
+
+
+def _ncu_case_bptt(args):
+    import torch
+    from nemo_b200.lif import LIFNetwork, lif_backward, lif_forward, poisson_bits
+    n, fan, chans, infan, steps, trials = (2000, 200, 500, 50, 100, 32) if args.small else (10000, 200, 500, 50, 500, 32)
+    net = LIFNetwork.random(n, fan, chans, infan, seed=7, checkpoint=50, bin_steps=10, kappa=10.0)
+    w = net.initial_weights(seed=7, scale_in=0.35)
+    bits, _ = poisson_bits(steps, chans, trials, rate_hz=10.0, seed=8)
+    for _ in range(max(args.warmup, 1) + max(args.steps, 1)):
+        counts, saved = lif_forward(net, w, bits, trials)
+        lif_backward(net, w, bits, trials, saved, torch.ones_like(counts))
+    torch.cuda.synchronize()
+    print(json.dumps({"case": "lif-bptt-%dk-200" % (n // 1000), "passes": max(args.warmup, 1) + max(args.steps, 1)}),
+          flush=True)
 
 
 def main():

@@ -649,7 +649,9 @@ __device__ __forceinline__ void residentNext(const CycleArgs& A, uint32_t seq, u
 				got = true;
 				break;
 			}
-			if(globalTimer() - start > A.idleNs) break;
+			/* lane 0's clock decides for the warp, so that every lane leaves
+			 * the loop on the same try */
+			if(__shfl_sync(FULL, globalTimer() - start > A.idleNs ? 1u : 0u, 0)) break;
 		}
 		/* the payload words, in lane order: word 3 l + j is chunk l's w[j] */
 		ResidentCmd* c = A.bcast + ((k + 1u) & 1u);

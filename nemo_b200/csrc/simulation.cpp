@@ -16,6 +16,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <random>
 #include <sstream>
 #include <thread>
@@ -264,6 +266,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	if(conf.cudaDevice >= 0) {
 		NEMO_CUDA(cudaSetDevice(conf.cudaDevice));
 	}
+	NEMO_CUDA(cudaGetDevice(&m_device));
 	std::vector<uint32_t> dsrc(S), dtgt(S);
 	std::vector<int32_t> wfx(S);
 	std::vector<uint32_t> outDegree(m_nDev, 0);
@@ -700,6 +703,7 @@ Simulation::release()
 		postCommand(++m_rseq, RESIDENT_EXIT);
 		m_resident = false;
 	}
+	releaseResidentDevice();
 	if(m_stream) cudaStreamSynchronize(STREAM(m_stream));
 	destroyGraph();
 	for(void** ev : {&m_evOut, &m_evIn, &m_evStaged}) {
@@ -997,6 +1001,41 @@ Simulation::mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, c
 	return true;
 }
 
+/* The simulation whose resident launch is on each device, if any. Two
+ * resident launches must not share a device: each occupies an SM with every
+ * block, and when both are partly resident, each one's blocks can wait for
+ * its first block, which cannot start while the other's hold the SMs. */
+static std::mutex g_residentLock;
+static std::map<int, Simulation*> g_residentOwner;
+
+void
+Simulation::claimResidentDevice()
+{
+	Simulation* other = nullptr;
+	{
+		std::lock_guard<std::mutex> lock(g_residentLock);
+		auto it = g_residentOwner.find(m_device);
+		if(it != g_residentOwner.end() && it->second != this) other = it->second;
+		g_residentOwner[m_device] = this;
+	}
+	if(other) {
+		/* its error, if any, is its own: that simulation reports it on its
+		 * next call */
+		try {
+			other->stopResident();
+		} catch(...) {
+		}
+	}
+}
+
+void
+Simulation::releaseResidentDevice()
+{
+	std::lock_guard<std::mutex> lock(g_residentLock);
+	auto it = g_residentOwner.find(m_device);
+	if(it != g_residentOwner.end() && it->second == this) g_residentOwner.erase(it);
+}
+
 /* The resident step kernel's launch for command `seq`, whose stimulus is
  * m_inline; the pending gathering of the last cycle, if any, is its first
  * phase's. The launch keeps the current slots in shared memory while it
@@ -1004,6 +1043,7 @@ Simulation::mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, c
 void
 Simulation::launchResident(uint32_t seq)
 {
+	claimResidentDevice();
 	if(m_rcmd == nullptr) {
 		NEMO_CUDA(cudaHostAlloc((void**) &m_rcmd, sizeof(ResidentHostCmd), cudaHostAllocMapped));
 		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRcmd, m_rcmd, 0));
@@ -1129,6 +1169,7 @@ Simulation::stopResident()
 	if(!m_resident) return;
 	postCommand(++m_rseq, RESIDENT_EXIT);
 	m_resident = false;
+	releaseResidentDevice();
 	NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
 	NEMO_CUDA(cudaGetLastError());
 	if(m_stepWords[0] != 0) {

@@ -44,6 +44,11 @@ public:
 	Simulation(const Network& net, const Configuration& conf, const ShardSpec* shard = nullptr);
 	~Simulation();
 
+	/* End this simulation's resident step launch, if any (every call but
+	 * step() does it first; a resident launch of another simulation on the
+	 * same device does it too) */
+	void stopResident();
+
 	/* One cycle with stimulus; returns the fired neurons (user indices) in
 	 * ascending simulation order (src/nemo/nemo_c.cpp:439-461). */
 	const std::vector<unsigned>& step(const unsigned* fstim, size_t nf,
@@ -310,6 +315,7 @@ private:
 	std::vector<unsigned> m_fired;
 
 	int m_noallocDevice = -1;  /* device of the simulation, found on the first stepNoAlloc */
+	int m_device = 0;          /* the device the simulation was built on */
 
 	/* batch */
 	std::vector<uint32_t> m_batchBase;
@@ -340,7 +346,8 @@ private:
 	bool mapInline(const unsigned* fstim, size_t nf, const unsigned* inidx, const float* icur, size_t ni);
 	bool fitsCommand() const { return 3u + m_inline.nf + 2u * m_inline.ni <= 3u * RESIDENT_CHUNKS; }
 	void launchResident(uint32_t seq);
-	void stopResident();
+	void claimResidentDevice();
+	void releaseResidentDevice();
 	bool m_resident = false;            /* a resident launch is on the stream */
 	bool m_residentOn = true;           /* nemo_step may use resident stepping */
 	uint32_t m_rseq = 0;                /* the last command number */
