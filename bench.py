@@ -977,7 +977,8 @@ def _ncu_case_batched(args):
     nets = [netgen.izhikevich_random(int(sizes[j]), 100, dmax=20, seed=1000 + j, sigma_exc=float(sig[j]),
                                      sigma_inh=float(0.4 * sig[j])).build(Network(lib)) for j in range(count)]
     handles = (ctypes.c_void_p * count)(*[n.handle for n in nets])
-    batch = d.nemo_b200_new_batch(handles, count, Configuration(lib).handle)
+    conf = Configuration(lib)
+    batch = d.nemo_b200_new_batch(handles, count, conf.handle)
     if not batch:
         raise RuntimeError(d.nemo_strerror().decode())
     del nets
