@@ -404,13 +404,16 @@ def run_b200(args):
 
     roof = roofline(sim, lib, wl)
     clk = clocks.summary()
-    tr = (ctypes.c_double * 14)()
-    lib.dll.nemo_b200_trace.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double * 14]
+    tr = (ctypes.c_double * 24)()
+    lib.dll.nemo_b200_trace.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_double * 24]
     lib.call("nemo_b200_trace", sim.handle, CYCLES_PER_STEP, tr)
     phase_ns = dict(zip(["phase", "update_max", "update_mean", "work_max", "work_mean",
                          "to_last_arrival", "barrier_release", "arrival_spread", "after_update_max",
                          "after_update_mean", "gather_unit", "stdp_unit", "gather_units_per_block",
-                         "stdp_units_per_block"], [round(x, 1) for x in tr]))
+                         "stdp_units_per_block", "update_warp_to_model", "update_warp",
+                         "fired_warp_after_lists", "fired_warps_per_block", "noise_unit",
+                         "noise_units_per_block", "last_unit_taken", "warp_leaves_units",
+                         "last_unit_to_end", "last_unit_end"], [round(x, 1) for x in tr]))
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -297,8 +297,16 @@ nemo_status_t nemo_b200_profile(nemo_simulation_t sim, unsigned cycles, float re
  * arrival to barrier exit, out[7] spread of the blocks' arrivals, out[8] /
  * out[9] slowest / mean block work left after its update, out[10] /
  * out[11] mean duration of one gather / STDP work unit of a warp, out[12] /
- * out[13] such units per block and cycle. */
-nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[14]);
+ * out[13] such units per block and cycle, out[14] / out[15] mean time of an
+ * update warp to its model's result / to the end of its update, out[16]
+ * mean time of a warp with fired neurons after its lists (delay-1 push,
+ * prefetches), out[17] such warps per block and cycle, out[18] / out[19]
+ * mean duration / count per block and cycle of a next-cycle noise unit,
+ * out[20] mean time from a block's phase start to its last work unit taken,
+ * out[21] mean time to a warp's leaving the work units, out[22] mean time
+ * from a block's last unit taken to its work done, out[23] mean time from a
+ * block's phase start to the end of its last unit. */
+nemo_status_t nemo_b200_trace(nemo_simulation_t sim, unsigned cycles, double out[24]);
 
 /* Diagnostics: the device noise transform of two RNG words per sample,
  * sin(2*pi*u1/2^32) * sqrt(-2 log(1 - u2/2^32)) as computed by the

@@ -23,7 +23,7 @@ namespace {
 
 const unsigned FULL = 0xffffffffu;
 /* words per block and cycle of the optional phase trace (kernels.hpp) */
-const unsigned TRACE_WORDS = 9;
+const unsigned TRACE_WORDS = 20;
 
 /* 64-bit shifts by a count that may reach 64, evaluated like the x86-64
  * shift the reference runs on (count modulo 64). */
@@ -764,7 +764,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	const uint32_t myN = myWarps * 32u;
 	const uint32_t ownBase = firstWarp * 32u;
 	const uint32_t updWarps = min(myWarps, warpsPerBlock);
-	const size_t listStride = size_t(B) * ownN;  /* one parity of the lists */
+	const size_t listStride = size_t(B) * ownN;  /* one parity of the fired lists */
+	const size_t postParity = size_t(B) * net.postStride;   /* one parity of the STDP entries */
 	int2* acc32 = reinterpret_cast<int2*>(net.acc);
 	/* this block's buckets of the forward matrix: bucket of source s =
 	 * segKey0 + s * segStride */
@@ -862,9 +863,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const uint64_t* rfIn = net.rf + (t & 1u) * nDev;
 			uint64_t* rfOut = net.rf + ((t + 1u) & 1u) * nDev;
 			uint32_t* firedOut = net.firedList + par * listStride + size_t(b) * ownN;
-			uint2* postOut = net.postList + par * listStride + size_t(b) * ownN;
+			uint2* postOut = net.postList + par * postParity + size_t(b) * net.postStride;
 			uint32_t pushed = 0;
 			for(uint32_t lw = warp; lw < myWarps; lw += warpsPerBlock) {
+				const uint32_t w0 = trace ? uint32_t(globalTimer()) : 0u;   /* low words: differences of a few µs */
 				const uint32_t dw = firstWarp + lw;
 				int gi = 0;
 				while(dw >= A.groupWarp[gi + 1]) ++gi;
@@ -951,6 +953,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					rfOut[n] = rfNew;
 				}
 				const uint32_t word = __ballot_sync(FULL, fired);
+				const uint32_t w1 = trace ? uint32_t(globalTimer()) : 0u;
 				if(lane == 0) {
 					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
 					if(A.hostWords && word) {
@@ -960,15 +963,27 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					}
 				}
 				if(net.stdp) {
-					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237) */
+					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237):
+					 * the target's plastic synapses as runs of at most
+					 * STDP_ITEM, one list entry each */
 					const bool post = valid && ((rfNew >> net.postShift) & 1ull);
-					const uint32_t pm = __ballot_sync(FULL, post);
-					if(pm) {
+					const uint32_t len = post ? rcm.y - rcm.x : 0u;
+					const uint32_t runs = (len + STDP_ITEM - 1u) / STDP_ITEM;
+					if(__ballot_sync(FULL, runs != 0u)) {
+						uint32_t incl = runs;
+#pragma unroll
+						for(int d = 1; d < 32; d <<= 1) {
+							const uint32_t x = __shfl_up_sync(FULL, incl, d);
+							if(lane >= uint32_t(d)) incl += x;
+						}
 						uint32_t base = 0;
-						if(lane == 0) base = atomicAdd(&sNPost, uint32_t(__popc(pm)));
-						base = __shfl_sync(FULL, base, 0);
-						if(post) {
-							postOut[base + __popc(pm & lt)] = make_uint2(rcm.x, rcm.y - rcm.x);
+						if(lane == 31) base = atomicAdd(&sNPost, incl);
+						base = __shfl_sync(FULL, base, 31) + incl - runs;
+						for(uint32_t r = 0; r < runs; ++r) {
+							const uint32_t off = r * STDP_ITEM;
+							postOut[base + r] = make_uint2(rcm.x + off, min(STDP_ITEM, len - off));
+						}
+						if(runs) {
 							/* the next phase's STDP accumulation walks this
 							 * target's reverse range: into L2 now */
 							prefetchL2(net.rcmSrcDelay + rcm.x, net.rcmSrcDelay + rcm.y);
@@ -976,6 +991,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						}
 					}
 				}
+				const uint32_t w2 = trace ? uint32_t(globalTimer()) : 0u;
 				if(word) {
 					uint32_t base = 0;
 					if(lane == 0) base = atomicAdd(&sNFired, uint32_t(__popc(word)));
@@ -1030,6 +1046,21 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				if(k == 0 && k + 1 < A.cycles && G.kind == 0 && valid) {
 					net.noise[(par ^ 1u) * nDev + n] = drawNoise(net, G, i);
 				}
+				if(trace) {
+					/* the warp's loads and model, its whole update, and for
+					 * a warp with fired neurons the part after its lists */
+					__syncwarp();
+					const uint32_t w3 = uint32_t(globalTimer());
+					if(lane == 0) {
+						atomicAdd(&trace[9], (unsigned long long) (w1 - w0));
+						atomicAdd(&trace[10], (unsigned long long) (w3 - w0));
+						atomicAdd(&trace[11], 1ull);
+						if(word) {
+							atomicAdd(&trace[12], (unsigned long long) (w3 - w2));
+							atomicAdd(&trace[13], 1ull);
+						}
+					}
+				}
 			}
 			pushed = __reduce_add_sync(FULL, pushed);
 			if(lane == 0 && pushed) atomicAdd(&sPushed, (unsigned long long) pushed);
@@ -1041,46 +1072,88 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		 * delay 1 went to the inbox when the sources fired) and the STDP accumulation of cycle t-1, as units
 		 * handed out by a block counter so that warps without neurons to
 		 * update start at once. Units [0, G): 32 fired
-		 * sources each; units [G, G + S): this block's share of the grid's
-		 * STDP items (item u * B + b) ---- */
+		 * sources each; units [G + NW, G + NW + S): this block's share of the
+		 * grid's STDP entries ---- */
 		if(doPrev) {
 			const uint32_t par = (t - 1u) & 1u;
 			const uint32_t nLists = B + (net.remoteList ? 1u : 0u);
 			const uint32_t F = net.deliver ? sPreF[nLists] : 0u;
 			const uint32_t G = (F + 31u) / 32u;
+			/* STDP entries of cycle t-1 over all blocks; this block takes
+			 * entries u * B + b */
 			const uint32_t P = net.stdp ? sPreP[B] : 0u;
-			const uint32_t chunks = net.stdpChunks;
-			const uint32_t items = P * chunks;
-			const uint32_t Sb = items > b ? (items - b + B - 1u) / B : 0u;
+			const uint32_t Sb = P > b ? (P - b + B - 1u) / B : 0u;
 			/* units [G, G + NW): the next cycle's noise of one owned neuron
 			 * warp each (from the second phase of a launch on) */
 			const uint32_t NW = (k + 1u < A.cycles) ? myWarps : 0u;
+			const uint32_t units = G + NW + Sb;
 			const uint32_t* flist = net.firedList + par * listStride;
-			const uint2* plist = net.postList + par * listStride;
+			const uint2* plist = net.postList + par * postParity;
 			const uint64_t* rfAfter = net.rf + (t & 1u) * nDev;   /* history after update(t-1) */
 			const uint32_t slotPrev = uint32_t((t64 - 1u) % net.slots);
 			uint32_t pushed = 0;
 			uint64_t visited = 0;
-			for(;;) {
-				uint32_t u = 0;
-				if(lane == 0) u = atomicAdd(&sWork, 1u);
-				u = __shfl_sync(FULL, u, 0);
-				if(u >= G + NW + Sb) break;
+			/* Each unit's dependent loads are issued one stage ahead, so that a
+			 * unit's chain starts from its last load: its first load (`lead`)
+			 * when the unit before it starts, its second (`second`) once the
+			 * unit before it has issued its own last loads.
+			 * lead: a gather unit's fired source of each lane {s, 1} ({0, 0}
+			 * past the end), an STDP unit's entry {first, count}.
+			 * second: a gather unit's bucket {first record, records} of each
+			 * lane, an STDP unit's source words. */
+			auto lead = [&](uint32_t u) -> uint2 {
+				uint2 v = make_uint2(0u, 0u);
+				if(u < G) {
+					const uint32_t j = u * 32u + lane;
+					if(j < F) {
+						const uint32_t bb = findList(sPreF, nLists, j);
+						v.x = bb < B ? flist[size_t(bb) * ownN + (j - sPreF[bb])]
+							: net.remoteList[size_t(par) * nDev + (j - sPreF[B])];
+						v.y = 1u;
+					}
+				} else if(u >= G + NW && u < units) {
+					const uint32_t it = (u - G - NW) * B + b;
+					const uint32_t bb = findList(sPreP, B, it);
+					v = plist[size_t(bb) * net.postStride + (it - sPreP[bb])];
+				}
+				return v;
+			};
+			auto second = [&](uint32_t u, uint2 h, uint2& row, uint32_t* sd) {
+				if(u < G) {
+					row = make_uint2(0u, 0u);
+					if(h.y) {
+						const uint32_t* r = net.segOff + segKey0 + size_t(h.x) * segStride;
+						row = make_uint2(r[0], r[1]);
+					}
+				} else if(u >= G + NW && u < units) {
+#pragma unroll
+					for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+						const uint32_t jj = lane + 32u * x;
+						sd[x] = jj < h.y ? __ldcs(&net.rcmSrcDelay[h.x + jj]) : 0u;
+					}
+				}
+			};
+			uint32_t u = 0;
+			if(lane == 0) u = atomicAdd(&sWork, 1u);
+			u = __shfl_sync(FULL, u, 0);
+			uint2 head = lead(u);
+			uint2 row = make_uint2(0u, 0u);
+			uint32_t sd[STDP_PER_LANE];
+			second(u, head, row, sd);
+			while(u < units) {
+				uint32_t un = 0;
+				if(lane == 0) un = atomicAdd(&sWork, 1u);
+				un = __shfl_sync(FULL, un, 0);
+				if(trace && lane == 0 && un < units) atomicMax(&trace[16], globalTimer());
+				const uint2 headNext = lead(un);
+				uint2 rowNext = make_uint2(0u, 0u);
+				uint32_t sdNext[STDP_PER_LANE];
 				const unsigned long long u0 = trace ? globalTimer() : 0ull;
 				if(u < G) {
 					/* 32 fired sources, one per lane; their segments of this
 					 * block's region are worked off as one concatenation so
 					 * that a warp's loads fall on few lines */
-					const uint32_t j = u * 32u + lane;
-					uint32_t beg = 0, cnt = 0;
-					if(j < F) {
-						const uint32_t bb = findList(sPreF, nLists, j);
-						const uint32_t s = bb < B ? flist[size_t(bb) * ownN + (j - sPreF[bb])]
-							: net.remoteList[size_t(par) * nDev + (j - sPreF[B])];
-						const uint32_t* row = net.segOff + segKey0 + size_t(s) * segStride;
-						beg = row[0];
-						cnt = row[1] - beg;
-					}
+					const uint32_t beg = row.x, cnt = row.y - row.x;
 					uint32_t incl = cnt;
 #pragma unroll
 					for(int d = 1; d < 32; d <<= 1) {
@@ -1090,6 +1163,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t total = __shfl_sync(FULL, incl, 31);
 					const uint32_t excl = incl - cnt;
 					pushed += lane == 0 ? total : 0u;
+					bool issued = false;   /* the next unit's second loads */
 					for(uint32_t base = 0; base < total; base += 32u * GATHER_PER_LANE) {
 						uint2 r[GATHER_PER_LANE];
 #pragma unroll
@@ -1106,6 +1180,10 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							const uint32_t bL = __shfl_sync(FULL, beg, lo);
 							r[x] = idx < total ? __ldcs(&net.fcm[bL + (idx - eL)]) : make_uint2(0u, 0u);
 						}
+						if(!issued) {
+							second(un, headNext, rowNext, sdNext);
+							issued = true;
+						}
 #pragma unroll
 						for(int x = 0; x < GATHER_PER_LANE; ++x) {
 							if(base + uint32_t(x) * 32u + lane < total) {
@@ -1115,7 +1193,9 @@ k_cycles(const __grid_constant__ CycleArgs A)
 							}
 						}
 					}
+					if(!issued) second(un, headNext, rowNext, sdNext);
 				} else if(u < G + NW) {
+					second(un, headNext, rowNext, sdNext);
 					const uint32_t lw = u - G;
 					const uint32_t dw = firstWarp + lw;
 					int gi = 0;
@@ -1127,43 +1207,32 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						net.noise[((t + 1u) & 1u) * nDev + n] = drawNoise(net, Gr, i);
 					}
 				} else {
-					/* STDP (ConnectivityMatrix.cpp:224-258): targets that
-					 * fired P cycles before cycle t-1; every accumulator has
-					 * one writer */
-					const uint32_t it = (u - G - NW) * B + b;
-					const uint32_t tg = it / chunks;
-					const uint32_t item = 32u * STDP_PER_LANE;
-					const uint32_t off = (it - tg * chunks) * item;
-					const uint32_t bb = findList(sPreP, B, tg);
-					const uint2 range = plist[size_t(bb) * ownN + (tg - sPreP[bb])];
-					if(off < range.y) {
-						const uint32_t b0 = range.x + off;
-						const uint32_t cnt = range.y - off < item ? range.y - off : item;
-						visited += cnt;
-						/* the accumulators do not depend on the sources: load
-						 * them with the source words, before the histories */
-						uint32_t sd[STDP_PER_LANE];
-						int32_t old[STDP_PER_LANE];
+					/* STDP (ConnectivityMatrix.cpp:224-258): a run of the
+					 * plastic synapses of a target that fired P cycles before
+					 * cycle t-1; every accumulator has one writer in a phase
+					 * (a plain load and store: a reduction into L2 measured
+					 * slower). The source words came with the unit before;
+					 * the accumulators and the sources' histories are loaded
+					 * together */
+					const uint32_t b0 = head.x;
+					const uint32_t cnt = head.y;
+					visited += cnt;
+					int32_t old[STDP_PER_LANE];
+					uint64_t pre[STDP_PER_LANE];
 #pragma unroll
-						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
-							const uint32_t jj = lane + 32u * x;
-							sd[x] = jj < cnt ? __ldcs(&net.rcmSrcDelay[b0 + jj]) : 0u;
-							old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
-						}
-						uint64_t pre[STDP_PER_LANE];
+					for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+						const uint32_t jj = lane + 32u * x;
+						old[x] = jj < cnt ? __ldcs(&net.rcmAcc[b0 + jj]) : 0;
+						pre[x] = jj < cnt ? rfAfter[sd[x] >> 6] : 0ull;
+					}
+					second(un, headNext, rowNext, sdNext);
 #pragma unroll
-						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
-							const uint32_t jj = lane + 32u * x;
-							pre[x] = jj < cnt ? shr64(rfAfter[sd[x] >> 6], (sd[x] & 63u) + 1u) : 0ull;
-						}
-#pragma unroll
-						for(int x = 0; x < int(STDP_PER_LANE); ++x) {
-							const uint32_t jj = lane + 32u * x;
-							if(jj < cnt) {
-								const int32_t dw = weightChange(pre[x], A.rule);
-								if(dw != 0) {
-									__stcs(&net.rcmAcc[b0 + jj], int32_t(uint32_t(old[x]) + uint32_t(dw)));
-								}
+					for(int x = 0; x < int(STDP_PER_LANE); ++x) {
+						const uint32_t jj = lane + 32u * x;
+						if(jj < cnt) {
+							const int32_t dw = weightChange(shr64(pre[x], (sd[x] & 63u) + 1u), A.rule);
+							if(dw != 0) {
+								__stcs(&net.rcmAcc[b0 + jj], int32_t(uint32_t(old[x]) + uint32_t(dw)));
 							}
 						}
 					}
@@ -1171,10 +1240,24 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				if(trace) {
 					__syncwarp();
 					if(lane == 0) {
-						atomicAdd(&trace[u < G ? 5 : 6], globalTimer() - u0);
-						atomicAdd(&trace[u < G ? 7 : 8], 1ull);
+						/* gather units [5] and [7], STDP units [6] and [8],
+						 * noise units [14] and [15] */
+						const unsigned q = u < G ? 5u : (u < G + NW ? 14u : 6u);
+						const unsigned long long u1 = globalTimer();
+						atomicAdd(&trace[q], u1 - u0);
+						atomicAdd(&trace[q == 14u ? 15u : q + 2u], 1ull);
+						atomicMax(&trace[19], u1);
 					}
 				}
+				u = un;
+				head = headNext;
+				row = rowNext;
+#pragma unroll
+				for(int x = 0; x < int(STDP_PER_LANE); ++x) sd[x] = sdNext[x];
+			}
+			if(trace && lane == 0) {
+				atomicAdd(&trace[17], globalTimer() - trace[0]);
+				atomicAdd(&trace[18], 1ull);
 			}
 			pushed = __reduce_add_sync(FULL, pushed);
 			if(lane == 0) {

@@ -27,8 +27,8 @@
  *     t-1 (all blocks' lists) and, for each, its segment of region b, adding
  *     each weight of delay d >= 2 into slot (t-1+d) mod Q of the target (E or
  *     I by sign), and the STDP accumulation of cycle t-1 over all blocks'
- *     post-spiking targets, dealt out over the grid in items of 32 x
- *     STDP_PER_LANE synapses.
+ *     post-spiking targets, dealt out over the grid as entries of at most
+ *     STDP_ITEM synapses (a target's plastic synapses in consecutive runs).
  *     Together the inbox and the gather are the reference's deliverSpikes at
  *     cycle t0+d (src/nemo/cpu/Simulation.cpp:259-308);
  *   - grid barrier.
@@ -52,12 +52,13 @@ const uint32_t MAX_BLOCKS = 256;
 const uint64_t APPLY_GROUP_SYNAPSES = uint64_t(1) << 24;
 /* plastic synapses per lane in one applyStdp work item */
 const uint32_t APPLY_PER_LANE = 4;
-/* forward records a gather lane loads per round (one round covers a unit of
- * 32 sources of about 7 records each in a block's region) */
-const int GATHER_PER_LANE = 8;
-/* plastic synapses a lane visits in one STDP accumulation item (an item is
- * 32 x STDP_PER_LANE synapses of one post-spiking target) */
+/* forward records a gather lane loads per round (a unit of 32 sources of
+ * about 7 records each in a block's region takes one or two rounds) */
+const int GATHER_PER_LANE = 4;
+/* plastic synapses a lane visits in one STDP accumulation entry (an entry is
+ * a run of at most STDP_ITEM synapses of one post-spiking target) */
 const uint32_t STDP_PER_LANE = 4;
+const uint32_t STDP_ITEM = 32 * STDP_PER_LANE;
 /* stimulus entries of each kind a one-cycle step carries in its kernel
  * parameters (CycleArgs::inlineF / inlineI) */
 const uint32_t INLINE_STIM_MAX = 32;
@@ -120,18 +121,19 @@ struct NetDev {
 	float* noise;                  /* [2][nDev] Izhikevich noise of the next cycle, by cycle parity */
 	uint32_t* fstim;               /* [nWords] firing stimulus, cleared after use */
 
-	/* per-cycle lists by cycle parity and block, [2][blocks][ownWarps * 32],
-	 * with their lengths [2][blocks]: fired sources (device indices) and the
-	 * reverse-matrix ranges {first, count} of post-spiking targets */
+	/* per-cycle lists by cycle parity and block, with their lengths
+	 * [2][blocks]: fired sources (device indices), [2][blocks][ownWarps * 32],
+	 * and the STDP entries of post-spiking targets, [2][blocks][postStride]:
+	 * reverse-matrix runs {first, count}, count in [1, STDP_ITEM] */
 	uint32_t* firedList;
 	uint32_t* firedCnt;
 	uint2* postList;
 	uint32_t* postCnt;
+	uint32_t postStride;           /* entries of a block's list: the most its neurons can make */
 
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;
 	uint32_t postShift;            /* bit of the history that triggers STDP */
-	uint32_t stdpChunks;           /* STDP items per target (max in-degree / (32 x STDP_PER_LANE)) */
 	uint32_t applyChunks;          /* (32 x APPLY_PER_LANE)-synapse chunks per target */
 	const uint32_t* rcmStart;      /* [nDev + 1] (fewer than 2^32 synapses) */
 	const uint32_t* rcmSrcDelay;   /* source << 6 | (delay - 1) */
@@ -286,10 +288,16 @@ struct CycleArgs {
 	uint32_t* exitInfo;
 	uint32_t firstSeq;
 	unsigned long long idleNs;
-	/* optional phase trace (%globaltimer ns), [cycles + 1][block][9]: phase
+	/* optional phase trace (%globaltimer ns), [cycles + 1][block][20]: phase
 	 * start, (unused), last update warp done (0 when the block updates
-	 * nothing), all work done, barrier passed; then the summed durations of
-	 * the block's gather units and STDP units, and their counts */
+	 * nothing), all work done, barrier passed; the summed durations of the
+	 * block's gather units and STDP units, and their counts; over the update
+	 * warps the summed time to their model's result, their summed update
+	 * time and their count, the summed time of the fired warps' part after
+	 * their lists (delay-1 push, prefetches) and their count; the summed
+	 * durations of the noise units and their count; the time the block's
+	 * last unit was taken, the summed times from the phase start at which its
+	 * warps left the unit loop and their count, the time its last unit ended */
 	unsigned long long* trace;
 };
 

@@ -465,7 +465,7 @@ nemo_b200_profile(nemo_simulation_t s, unsigned cycles, float reward, double out
 }
 
 nemo_status_t
-nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[14])
+nemo_b200_trace(nemo_simulation_t s, unsigned cycles, double out[24])
 {
 	RETURN_CALL(s->sim.trace(cycles, out));
 }

@@ -485,11 +485,29 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 			rcmWeight[j] = wfx[s];
 		}
 	}
-	/* STDP work items (32 x STDP_PER_LANE synapses) per post-spiking target */
-	const uint64_t stdpItem = 32u * STDP_PER_LANE;
-	const uint64_t stdpChunks = std::max<uint64_t>(1, (maxIn + stdpItem - 1) / stdpItem);
-	if(uint64_t(m_nDev) * stdpChunks >= (uint64_t(1) << 32)) {
-		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 STDP items (targets x items per target)");
+	/* STDP entries: a post-spiking target's plastic synapses in runs of at
+	 * most STDP_ITEM; a block's list of one cycle holds at most the sum of
+	 * its neurons' runs */
+	uint64_t postStride = 1;
+	if(m_stdpOn) {
+		std::vector<uint32_t> hostStart;
+		const uint32_t* rs = rcmStart.data();
+		if(onDevice) {
+			hostStart.resize(size_t(m_nDev) + 1);
+			NEMO_CUDA(cudaMemcpyAsync(hostStart.data(), dev.rcmStart, hostStart.size() * 4, cudaMemcpyDeviceToHost,
+					STREAM(m_stream)));
+			NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
+			rs = hostStart.data();
+		}
+		for(uint32_t b = 0; b < m_blocks; ++b) {
+			uint64_t runs = 0;
+			const uint32_t n0 = (warpLo + ownStart[b]) * 32u, n1 = (warpLo + ownStart[b + 1]) * 32u;
+			for(uint32_t n = n0; n < n1; ++n) runs += (uint64_t(rs[n + 1] - rs[n]) + STDP_ITEM - 1) / STDP_ITEM;
+			postStride = std::max(postStride, runs);
+		}
+	}
+	if(uint64_t(m_blocks) * postStride >= (uint64_t(1) << 32)) {
+		fail(NEMO_API_UNSUPPORTED, "The B200 backend supports at most 2^32 STDP entries in one cycle");
 	}
 
 	/* ---- synapse query data (src/nemo/ConnectivityMatrix.cpp:128-149) ---- */
@@ -556,14 +574,14 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.barrier = (unsigned*) alloc(4 * 4);
 	m_net.firedList = (uint32_t*) alloc(size_t(2) * B * ownN * 4);
 	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
-	m_net.postList = (uint2*) alloc(size_t(2) * B * ownN * 8);
+	m_net.postList = (uint2*) alloc(size_t(2) * B * postStride * 8);
+	m_net.postStride = uint32_t(postStride);
 	m_net.postCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	if(m_shard.world > 1) {
 		m_net.remoteList = (uint32_t*) alloc(size_t(2) * m_nDev * 4);
 		m_net.remoteCnt = (uint32_t*) alloc(2 * 4);
 	}
 	m_net.stdp = m_stdpOn ? 1 : 0;
-	m_net.stdpChunks = uint32_t(stdpChunks);
 	m_net.applyChunks = uint32_t(std::max<uint64_t>(1, (maxIn + 32 * APPLY_PER_LANE - 1) / (32 * APPLY_PER_LANE)));
 	if(m_stdpOn) {
 		m_net.postShift = unsigned(m_stdpFn.postfire.size()) & 63u;
@@ -2068,7 +2086,7 @@ Simulation::profile(unsigned cycles, float reward, double out[10])
 }
 
 void
-Simulation::trace(unsigned cycles, double out[14])
+Simulation::trace(unsigned cycles, double out[24])
 {
 	notShard("trace");
 	notExternal("trace");
@@ -2077,7 +2095,7 @@ Simulation::trace(unsigned cycles, double out[14])
 		fail(NEMO_INVALID_INPUT, "trace: no cycles");
 	}
 	cudaStream_t stream = STREAM(m_stream);
-	const unsigned S = 9;
+	const unsigned S = 20;
 	size_t words = size_t(cycles + 1) * m_blocks * S;
 	unsigned long long* dTrace;
 	NEMO_CUDA(cudaMalloc(&dTrace, words * 8));
@@ -2098,7 +2116,8 @@ Simulation::trace(unsigned cycles, double out[14])
 	cudaFree(dTrace);
 	checkDeviceError();
 	double acc[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-	double gNs = 0, gN = 0, sNs = 0, sN = 0;
+	double gNs = 0, gN = 0, sNs = 0, sN = 0, mNs = 0, uNs = 0, uN = 0, fNs = 0, fN = 0, nNs = 0, nN = 0;
+	double lastClaim = 0, exitMean = 0, lastToEnd = 0, lastUnitEnd = 0, blocksClaiming = 0;
 	for(unsigned k = 0; k < cycles; ++k) {
 		double minT0 = 1e300, maxT4 = 0, maxU = 0, sumU = 0, maxA = 0, sumA = 0, maxR = 0, sumR = 0,
 				maxT3 = 0, minT3 = 1e300, sumT4 = 0;
@@ -2121,6 +2140,20 @@ Simulation::trace(unsigned cycles, double out[14])
 			sNs += double(r[6]);
 			gN += double(r[7]);
 			sN += double(r[8]);
+			mNs += double(r[9]);
+			uNs += double(r[10]);
+			uN += double(r[11]);
+			fNs += double(r[12]);
+			fN += double(r[13]);
+			nNs += double(r[14]);
+			nN += double(r[15]);
+			if(r[16] != 0 && r[18] != 0) {
+				lastClaim += double(r[16]) - t0;
+				exitMean += double(r[17]) / double(r[18]);
+				lastUnitEnd += double(r[19]) - t0;
+				lastToEnd += t3 - double(r[16]);
+				blocksClaiming += 1;
+			}
 		}
 		acc[0] += maxT4 - minT0;
 		acc[1] += maxU;
@@ -2138,6 +2171,16 @@ Simulation::trace(unsigned cycles, double out[14])
 	out[11] = sN ? sNs / sN : 0.0;
 	out[12] = gN / (double(cycles) * m_blocks);
 	out[13] = sN / (double(cycles) * m_blocks);
+	out[14] = uN ? mNs / uN : 0.0;
+	out[15] = uN ? uNs / uN : 0.0;
+	out[16] = fN ? fNs / fN : 0.0;
+	out[17] = fN / (double(cycles) * m_blocks);
+	out[18] = nN ? nNs / nN : 0.0;
+	out[19] = nN / (double(cycles) * m_blocks);
+	out[20] = blocksClaiming ? lastClaim / blocksClaiming : 0.0;
+	out[21] = blocksClaiming ? exitMean / blocksClaiming : 0.0;
+	out[22] = blocksClaiming ? lastToEnd / blocksClaiming : 0.0;
+	out[23] = blocksClaiming ? lastUnitEnd / blocksClaiming : 0.0;
 }
 
 /* Every float in [-104, 89] through the device expf, compared with host

@@ -180,7 +180,7 @@ public:
 	 * arrivals, [8] max / [9] mean block work after its update, [10] / [11]
 	 * mean duration of a gather / STDP unit, [12] / [13] such units per block
 	 * and cycle. */
-	void trace(unsigned cycles, double out[14]);
+	void trace(unsigned cycles, double out[24]);
 
 private:
 	struct Group {
