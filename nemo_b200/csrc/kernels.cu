@@ -733,20 +733,73 @@ __device__ __forceinline__ void gatherAdd(const NetDev& net, int2* sAcc, uint32_
 	}
 }
 
-/* k_cycles: see kernels.hpp for the phase structure. The forward regions and
+/* The fired words of cycle t (its row of the firing ring) of the
+ * simulation's warps into host memory as CycleArgs::hostWords describes: the
+ * words that are not 0 with their warps, in warp order. Called by every
+ * thread of one block, after every block has written its words and fenced;
+ * the words are read from L2. Four words per thread are loaded at once. */
+__device__ __forceinline__ void writeStepList(const NetDev& net, uint32_t* hostWords, uint32_t t, uint32_t warp, uint32_t lane)
+{
+	__shared__ uint32_t sCnt[33];
+	const uint32_t T = blockDim.x;
+	const uint32_t warps = T >> 5;
+	const uint32_t lt = (1u << lane) - 1u;
+	const uint32_t w0 = net.warpBase;
+	const uint32_t nw = net.ownStart[gridDim.x];
+	const uint32_t* row = net.firedRing + size_t(t & net.ringMask) * net.nWords + w0;
+	uint2* out = reinterpret_cast<uint2*>(hostWords + 2);
+	uint32_t done = 0;
+	for(uint32_t r0 = 0; r0 < nw; r0 += 4u * T) {
+		uint32_t word[4];
+#pragma unroll
+		for(int q = 0; q < 4; ++q) {
+			const uint32_t w = r0 + uint32_t(q) * T + threadIdx.x;
+			word[q] = w < nw ? __ldcg(&row[w]) : 0u;
+		}
+#pragma unroll
+		for(int q = 0; q < 4; ++q) {
+			if(r0 + uint32_t(q) * T >= nw) break;   /* the same for the whole block */
+			const uint32_t w = r0 + uint32_t(q) * T + threadIdx.x;
+			const uint32_t m = __ballot_sync(0xffffffffu, word[q] != 0u);
+			if(lane == 0) sCnt[warp] = uint32_t(__popc(m));
+			__syncthreads();
+			if(warp == 0) {
+				const uint32_t v = lane < warps ? sCnt[lane] : 0u;
+				uint32_t incl = v;
+#pragma unroll
+				for(int d = 1; d < 32; d <<= 1) {
+					const uint32_t x = __shfl_up_sync(0xffffffffu, incl, d);
+					if(lane >= uint32_t(d)) incl += x;
+				}
+				sCnt[lane] = incl - v;
+				if(lane == 31) sCnt[32] = incl;
+			}
+			__syncthreads();
+			if(word[q]) out[done + sCnt[warp] + uint32_t(__popc(m & lt))] = make_uint2(word[q], w0 + w);
+			done += sCnt[32];
+			__syncthreads();
+		}
+	}
+	if(threadIdx.x == 0) hostWords[1] = done;
+}
+
+/* k_cycles: see kernels.hpp for the phase structure. HOST: the launch may
+ * write a step list to host memory or stay resident (CycleArgs::hostWords,
+ * cmd); launches that do neither use the instantiation without that code,
+ * which leaves the rest more registers. The forward regions and
  * the reverse-matrix arrays are streamed with evict-first loads and stores
  * (__ldcs / __stcs), so that they do not push the randomly read firing
  * history, segment offsets and noise tables out of L2. SMEM: the owned current
  * slots live in dynamic shared memory as int32 E/I pairs,
  * sAcc[slot * ownN + local]; otherwise every access goes to net.acc. */
-template<bool SMEM, unsigned T>
+template<bool SMEM, unsigned T, bool HOST>
 __global__ void __launch_bounds__(T, 1)
 k_cycles(const __grid_constant__ CycleArgs A)
 {
 	extern __shared__ int2 sAcc[];
 	__shared__ uint32_t sPreF[MAX_BLOCKS + 2];    /* + the remote list of a shard */
 	__shared__ uint32_t sPreP[MAX_BLOCKS + 1];
-	__shared__ uint32_t sNFired, sNPost, sWork, sListCnt;
+	__shared__ uint32_t sNFired, sNPost, sWork, sLast;
 	__shared__ unsigned long long sEvents, sPushed, sVisits;
 
 	const NetDev& net = A.net;
@@ -795,7 +848,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 	 * all and runs as an ordinary launch) */
 	/* resident stepping (CycleArgs::cmd): one update phase per command until
 	 * an exit command or the idle limit; the last cycle stays pending */
-	const bool resident = A.cmd != nullptr;
+	const bool resident = HOST && A.cmd != nullptr;
 	const bool lastPending = resident || (A.carry & 2u) != 0u;
 	const uint32_t phases = resident ? 0xffffffffu : A.cycles + (lastPending ? 0u : 1u);
 	const uint32_t barriers = lastPending && A.cycles ? A.cycles - 1u : A.cycles;
@@ -832,7 +885,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			sNFired = 0;
 			sNPost = 0;
 			sWork = 0;
-			sListCnt = 0;
 			sEvents = 0;
 			sPushed = 0;
 			sVisits = 0;
@@ -954,14 +1006,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				}
 				const uint32_t word = __ballot_sync(FULL, fired);
 				const uint32_t w1 = trace ? uint32_t(globalTimer()) : 0u;
-				if(lane == 0) {
-					net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
-					if(A.hostWords && word) {
-						const uint32_t e = atomicAdd(&sListCnt, 1u);
-						uint32_t* L = A.hostWords + 2u + size_t(b) * (2u + 2u * net.ownWarps);
-						*reinterpret_cast<uint2*>(&L[2u + 2u * e]) = make_uint2(word, dw);
-					}
-				}
+				if(lane == 0) net.firedRing[size_t(t & net.ringMask) * net.nWords + dw] = word;
 				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237):
 					 * the target's plastic synapses as runs of at most
@@ -1267,7 +1312,6 @@ k_cycles(const __grid_constant__ CycleArgs A)
 		}
 		__syncthreads();
 		if(tid == 0) {
-			if(doUpdate && A.hostWords) A.hostWords[2u + size_t(b) * (2u + 2u * net.ownWarps)] = sListCnt;
 			if(doUpdate) {
 				const uint32_t par = t & 1u;
 				net.firedCnt[par * B + b] = sNFired;
@@ -1283,25 +1327,42 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			if(sVisits) atomicAdd(&net.stats[1], sVisits);
 		}
 		if(trace && tid == 0) trace[3] = globalTimer();
-		if(resident) {
-			/* the block's fired words of this command are in host memory:
-			 * report it; block 0 then waits for the next command and hands
-			 * it to every block through the grid barrier */
-			const uint32_t seqK = A.firstSeq + k;
+		if(HOST && A.hostWords && doUpdate) {
+			/* the step's list, by the block whose update arrives last */
 			if(tid == 0) {
-				__threadfence_system();
-				*(volatile uint32_t*) &A.doneWords[b] = seqK;
+				__threadfence();
+				sLast = atomicAdd(&net.barrier[3], 1u) == B - 1u;
+				if(sLast) {
+					/* every block has arrived: the count starts again for
+					 * the next step, which the host starts after this one's
+					 * list */
+					*(volatile unsigned*) &net.barrier[3] = 0u;
+					__threadfence();
+				}
 			}
+			__syncthreads();
+			if(sLast) {
+				writeStepList(net, A.hostWords, t, warp, lane);
+				if(resident && tid == 0) {
+					__threadfence_system();
+					*(volatile uint32_t*) &A.doneWords[0] = A.firstSeq + k;
+				}
+			}
+		}
+		if(resident) {
+			/* block 0 waits for the next command and hands it to every
+			 * block */
+			const uint32_t seqK = A.firstSeq + k;
 			if(b == 0) {
 				residentNext(A, seqK, k, warp, lane);
 			} else if(!residentWait(A, seqK, k)) {
-				if(A.hostWords && tid == 0) A.hostWords[0] = 1u;
+				if(HOST && A.hostWords && tid == 0) A.hostWords[0] = 1u;
 				return;
 			}
 			if(*(volatile const uint32_t*) &A.bcast[(k + 1u) & 1u].op != RESIDENT_STEP) break;
 		} else if(k < barriers) {
 			if(!gridSync(net.barrier, barBase + (k + 1u) * B, A.timeoutNs)) {
-				if(A.hostWords && tid == 0) A.hostWords[0] = 1u;
+				if(HOST && A.hostWords && tid == 0) A.hostWords[0] = 1u;
 				return;
 			}
 			passed++;
@@ -1737,23 +1798,29 @@ cyclesPlan(const std::vector<uint32_t>& warpCost, uint32_t slots, bool acc32, ui
 	const bool smem = acc32 && bytes <= SMEM_ACC_LIMIT;
 	/* the attribute is per device and shared by all simulations: set it to
 	 * the largest size any of them uses */
-	cudaFuncSetAttribute(k_cycles<true, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
-	cudaFuncSetAttribute(k_cycles<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
-	cudaFuncSetAttribute(k_cycles<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
-	int perSm = 0;
+	cudaFuncSetAttribute(k_cycles<true, 1024, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	cudaFuncSetAttribute(k_cycles<true, 256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SMEM_ACC_LIMIT));
+	int perSm = 0, perSmHost = 0;
 	if(smem) {
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<true, 1024>, 1024, size_t(bytes));
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<true, 1024, false>, 1024, size_t(bytes));
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmHost, k_cycles<true, 1024, true>, 1024, size_t(bytes));
 	} else {
-		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false, 1024>, 1024, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_cycles<false, 1024, false>, 1024, 0);
+		cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmHost, k_cycles<false, 1024, true>, 1024, 0);
 	}
+	perSm = std::min(perSm, perSmHost);
 	*blocks = perSm >= 1 ? B : 0u;
 	*ownWarps = most;
 	*smemAcc = smem;
 }
 
-template<bool SMEM>
+template<bool SMEM, bool HOST>
 static cudaError_t
-launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
+launchCyclesH(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
 {
 	const NetDev& net = args.net;
 	if(args.cycles <= 1u && (args.carry & 2u) && args.cmd == nullptr) {
@@ -1761,27 +1828,35 @@ launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t s
 		 * another, so they need not be co-resident */
 		switch(net.threads) {
 			case 256:
-				return cudaLaunchKernel((const void*) k_cycles<SMEM, 256>, dim3(net.blocks), dim3(256), params, bytes,
-						stream);
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 256, HOST>, dim3(net.blocks), dim3(256), params,
+						bytes, stream);
 			case 512:
-				return cudaLaunchKernel((const void*) k_cycles<SMEM, 512>, dim3(net.blocks), dim3(512), params, bytes,
-						stream);
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 512, HOST>, dim3(net.blocks), dim3(512), params,
+						bytes, stream);
 			default:
-				return cudaLaunchKernel((const void*) k_cycles<SMEM, 1024>, dim3(net.blocks), dim3(1024), params,
+				return cudaLaunchKernel((const void*) k_cycles<SMEM, 1024, HOST>, dim3(net.blocks), dim3(1024), params,
 						bytes, stream);
 		}
 	}
 	switch(net.threads) {
 		case 256:
-			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 256>, dim3(net.blocks), dim3(256), params,
-					bytes, stream);
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 256, HOST>, dim3(net.blocks), dim3(256),
+					params, bytes, stream);
 		case 512:
-			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 512>, dim3(net.blocks), dim3(512), params,
-					bytes, stream);
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 512, HOST>, dim3(net.blocks), dim3(512),
+					params, bytes, stream);
 		default:
-			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 1024>, dim3(net.blocks), dim3(1024), params,
-					bytes, stream);
+			return cudaLaunchCooperativeKernel((const void*) k_cycles<SMEM, 1024, HOST>, dim3(net.blocks), dim3(1024),
+					params, bytes, stream);
 	}
+}
+
+template<bool SMEM>
+static cudaError_t
+launchCyclesT(const CycleArgs& args, void** params, size_t bytes, cudaStream_t stream)
+{
+	if(args.hostWords || args.cmd) return launchCyclesH<SMEM, true>(args, params, bytes, stream);
+	return launchCyclesH<SMEM, false>(args, params, bytes, stream);
 }
 
 void

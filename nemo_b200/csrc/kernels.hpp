@@ -251,11 +251,12 @@ struct CycleArgs {
 	 * phase saves the copy in and out */
 	int globalAcc;
 	/* a step's output in mapped host memory, null otherwise: word 0 is set to
-	 * 1 when a grid barrier timed out (the host zeroes it first); then per
-	 * block b, at 2 + b * (2 + 2 ownWarps), the count of its warps that fired
-	 * in the cycle, a pad word, and that many {fired word, device warp} pairs
-	 * (8-byte aligned, in no order; as 64-bit words they sort by warp): only
-	 * the words that are not 0 cross to the host */
+	 * 1 when a grid barrier timed out (the host zeroes it first); word 1 the
+	 * count of the simulation's warps that fired in the cycle, then that many
+	 * {fired word, device warp} pairs in warp order (only the words that are
+	 * not 0 cross to the host). The block that finishes the cycle's update
+	 * last (arrivals counted in NetDev::barrier[3]) writes the list from the
+	 * cycle's row of the firing ring */
 	uint32_t* hostWords;
 	/* a one-cycle step's stimulus when it is short (device indices; the
 	 * owner warp of each neuron applies it before the update), in place of
@@ -272,13 +273,13 @@ struct CycleArgs {
 	uint64_t* cycleCounter;
 	/* resident stepping: when cmd is set, the launch runs one update phase
 	 * per command instead of `cycles` phases. The first command (seq
-	 * firstSeq) is this launch's inline stimulus; after each phase every
-	 * block writes the command's seq into doneWords[block] (mapped host
-	 * memory) once its fired words' list is in hostWords, and block 0 waits for
-	 * command seq + 1 in *cmd (mapped host memory) for at most idleNs and
-	 * copies it to bcast[(phase + 1) & 1] (device), where the other blocks
-	 * wait for it. The host issues a command only after every block's done
-	 * word has come, so no grid barrier separates the phases. An exit
+	 * firstSeq) is this launch's inline stimulus; after each phase the block
+	 * that writes the step list writes the command's seq into doneWords[0]
+	 * (mapped host memory) after it, and block 0 waits for command seq + 1 in
+	 * *cmd (mapped host memory) for at most idleNs and copies it to
+	 * bcast[(phase + 1) & 1] (device), where the other blocks wait for it.
+	 * The host issues a command only after the done word has come, which
+	 * follows every block's phase, so no grid barrier separates the phases. An exit
 	 * command, or no command within idleNs, ends the launch, which leaves its
 	 * last cycle pending (as carry bit 1) and writes exitInfo = (last seq done
 	 * << 1) | 1 (mapped host memory). */

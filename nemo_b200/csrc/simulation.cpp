@@ -683,8 +683,8 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_args.timeoutNs = 10ull * 1000 * 1000 * 1000;
 
 	NEMO_CUDA(cudaMallocHost((void**) &m_hWords, size_t(m_net.nWords + 1) * 4));
-	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, (2 + size_t(m_blocks) * (2 + 2 * size_t(m_net.ownWarps))) * 4,
-				cudaHostAllocMapped));
+	/* error word, count, at most one {word, warp} pair per warp */
+	NEMO_CUDA(cudaHostAlloc((void**) &m_stepWords, (2 + 2 * size_t(m_net.nWords)) * 4, cudaHostAllocMapped));
 	NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dStepWords, m_stepWords, 0));
 	/* plugin models derive their initial state (b200_init_neurons) */
 	for(const Group& g : m_groups) {
@@ -839,30 +839,22 @@ Simulation::decodeFired(const uint32_t* words, std::vector<unsigned>& out) const
 	}
 }
 
-/* The fired neurons of the last step from the per-block lists the kernel
- * wrote into mapped memory (CycleArgs::hostWords): blocks own ascending warp
- * ranges, and a block's few entries are put in warp order here. */
+/* The fired neurons of the last step from the list the kernel wrote into
+ * mapped memory (CycleArgs::hostWords): {fired word, warp} pairs in warp
+ * order, one contiguous run for the host to read. */
 template<class Emit>
 void
 Simulation::decodeStepList(Emit emit)
 {
-	uint32_t* base = m_stepWords + 2;
-	const size_t stride = 2 + 2 * size_t(m_net.ownWarps);
-	for(uint32_t b = 0; b < m_blocks; ++b) {
-		uint32_t* L = base + b * stride;
-		const uint32_t n = L[0];
-		if(n == 0) continue;
-		/* {word, warp} pairs: as 64-bit words they sort by warp */
-		uint64_t* e = reinterpret_cast<uint64_t*>(L + 2);
-		std::sort(e, e + n);
-		for(uint32_t k = 0; k < n; ++k) {
-			const size_t w = size_t(e[k] >> 32);
-			uint32_t bits = uint32_t(e[k]);
-			while(bits) {
-				const uint32_t bit = uint32_t(__builtin_ctz(bits));
-				bits &= bits - 1;
-				emit(m_d2g[w * 32 + bit]);
-			}
+	const uint32_t n = m_stepWords[1];
+	const uint32_t* e = m_stepWords + 2;
+	for(uint32_t k = 0; k < n; ++k) {
+		const size_t w = e[2 * k + 1];
+		uint32_t bits = e[2 * k];
+		while(bits) {
+			const uint32_t bit = uint32_t(__builtin_ctz(bits));
+			bits &= bits - 1;
+			emit(m_d2g[w * 32 + bit]);
 		}
 	}
 }
@@ -1065,13 +1057,15 @@ Simulation::launchResident(uint32_t seq)
 	if(m_rcmd == nullptr) {
 		NEMO_CUDA(cudaHostAlloc((void**) &m_rcmd, sizeof(ResidentHostCmd), cudaHostAllocMapped));
 		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRcmd, m_rcmd, 0));
-		NEMO_CUDA(cudaHostAlloc((void**) &m_rdone, (size_t(m_blocks) + 1) * 4, cudaHostAllocMapped));
+		/* the done word and the exit word */
+		NEMO_CUDA(cudaHostAlloc((void**) &m_rdone, 64, cudaHostAllocMapped));
 		NEMO_CUDA(cudaHostGetDevicePointer((void**) &m_dRdone, m_rdone, 0));
 		m_rbcast = (ResidentCmd*) alloc(2 * sizeof(ResidentCmd));
 		std::memset(m_rcmd, 0, sizeof(ResidentHostCmd));
 	}
-	/* no command of this launch has run yet */
-	for(uint32_t b = 0; b <= m_blocks; ++b) reinterpret_cast<volatile uint32_t*>(m_rdone)[b] = 0u;
+	/* no command of this launch has run yet: done word, exit word */
+	reinterpret_cast<volatile uint32_t*>(m_rdone)[0] = 0u;
+	reinterpret_cast<volatile uint32_t*>(m_rdone)[1] = 0u;
 	m_stepWords[0] = 0u;
 	CycleArgs a = m_args;
 	a.firstCycle = m_cycle;
@@ -1088,7 +1082,7 @@ Simulation::launchResident(uint32_t seq)
 	a.cmd = m_dRcmd;
 	a.bcast = m_rbcast;
 	a.doneWords = m_dRdone;
-	a.exitInfo = m_dRdone + m_blocks;
+	a.exitInfo = m_dRdone + 1;
 	a.firstSeq = seq;
 	/* a caller that stops stepping releases the device after this long */
 	a.idleNs = 1000ull * 1000;
@@ -1141,11 +1135,9 @@ Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx
 	}
 	volatile const uint32_t* done = m_rdone;
 	const auto start = std::chrono::steady_clock::now();
-	uint32_t b = 0;
 	for(uint64_t spin = 0;; ++spin) {
-		while(b < m_blocks && done[b] == seq) ++b;
-		if(b == m_blocks) break;
-		const uint32_t exitInfo = done[m_blocks];
+		if(done[0] == seq) break;
+		const uint32_t exitInfo = done[1];
 		if(exitInfo != 0u && (exitInfo >> 1) < seq) {
 			/* the launch ended (idle) before this command: run it in a new one */
 			NEMO_CUDA(cudaStreamSynchronize(STREAM(m_stream)));
@@ -1155,7 +1147,6 @@ Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx
 			}
 			mapInline(fstim, nf, inidx, icur, ni);
 			launchResident(seq);
-			b = 0;
 			continue;
 		}
 		if((spin & 4095u) == 4095u) {
