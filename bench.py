@@ -365,14 +365,16 @@ def run_b200(args):
     lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_double * 4]
     out = (ctypes.c_double * 4)()
-    # threads per partition of the step kernel, chosen by timing 100-cycle
-    # trials (simulated like any other cycles) after a first warm-up step
-    lib.dll.nemo_b200_autotune.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),
-                                           ctypes.c_double * 3]
+    # the step kernel's work shape (threads per partition, synapses of an
+    # STDP work entry), chosen by timing 100-cycle trials (simulated like any
+    # other cycles) after a first warm-up step
+    lib.dll.nemo_b200_autotune_shape.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),
+                                                 ctypes.POINTER(ctypes.c_uint), ctypes.c_double * 6]
     lib.call("nemo_b200_timed_steps", sim.handle, 1, CYCLES_PER_STEP, 1, ctypes.c_float(REWARD), out)
-    tuned = ctypes.c_uint()
-    tune_ms = (ctypes.c_double * 3)()
-    lib.call("nemo_b200_autotune", sim.handle, CYCLES_PER_STEP, ctypes.byref(tuned), tune_ms)
+    tuned, tuned_run = ctypes.c_uint(), ctypes.c_uint()
+    tune_ms = (ctypes.c_double * 6)()
+    lib.call("nemo_b200_autotune_shape", sim.handle, CYCLES_PER_STEP, ctypes.byref(tuned), ctypes.byref(tuned_run),
+             tune_ms)
     # the clock sampler runs through warm-up and the timed region, so that the
     # GPU is under the same load for every sample
     with ClockSampler(local) as clocks:
@@ -398,9 +400,13 @@ def run_b200(args):
     # end to end through the C ABI (host buffers, per-cycle copies), the
     # same number of steps as the device-timed loop
     e2e_steps_n = max(1, args.steps)
+    lib.dll.nemo_b200_host_bytes.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong * 2]
+    bytes0 = (ctypes.c_ulonglong * 2)()
+    bytes1 = (ctypes.c_ulonglong * 2)()
+    lib.call("nemo_b200_host_bytes", sim.handle, bytes0)
     e2e_s, e2e_fired = e2e_steps(sim, n, e2e_steps_n, seed=11)
+    lib.call("nemo_b200_host_bytes", sim.handle, bytes1)
     e2e_value = e2e_fired * m / e2e_s
-    nwords = (n + 31) // 32
 
     roof = roofline(sim, lib, wl)
     clk = clocks.summary()
@@ -425,14 +431,17 @@ def run_b200(args):
         "fired_per_cycle": round(fired / (CYCLES_PER_STEP * args.steps), 1),
         "delivered_synapses": int(delivered), "build_s": round(t_build, 2),
         "e2e": {"value": round(e2e_value, 1), "unit": UNIT,
-                "h2d_bytes_per_step": 4 * CYCLES_PER_STEP,
-                "d2h_bytes_per_step": 4 * nwords * CYCLES_PER_STEP,
+                # counted by the library: the stimulus commands in, the
+                # fired lists (pairs of fired word and warp) out
+                "h2d_bytes_per_step": round((bytes1[0] - bytes0[0]) / e2e_steps_n),
+                "d2h_bytes_per_step": round((bytes1[1] - bytes0[1]) / e2e_steps_n),
                 "steps": e2e_steps_n, "s_per_step": round(e2e_s / e2e_steps_n, 4)},
         "roofline": roof,
         "phase_ns": phase_ns,
         "gpu_launches": args.steps * (1 + apply_launches(sim, lib)),
-        "autotune": {"threads": tuned.value, "ms_per_cycle": {"1024": round(tune_ms[0], 5), "512": round(tune_ms[1], 5),
-                                                             "256": round(tune_ms[2], 5)}},
+        "autotune": {"threads": tuned.value, "stdp_run": tuned_run.value,
+                     "ms_per_cycle": {"%d/%d" % (t, r): round(tune_ms[3 * i + k], 5)
+                                      for i, r in enumerate((128, 64)) for k, t in enumerate((1024, 512, 256))}},
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -740,7 +749,10 @@ def run_random1k(args):
 
     net = spec.build(Network(lib))
     sim = Simulation(net, Configuration(lib))
+    lib.dll.nemo_b200_host_bytes.argtypes = [ctypes.c_void_p, ctypes.c_ulonglong * 2]
+    bus = (ctypes.c_ulonglong * 2)()
     e2e_s, e2e_counts, e2e_events = step_run(lib, sim)
+    lib.call("nemo_b200_host_bytes", sim.handle, bus)
     # device-resident: fresh simulations, K timed launches of 1000 cycles after W
     lib.dll.nemo_b200_timed_steps.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
                                               ctypes.c_float, ctypes.c_double * 4]
@@ -758,7 +770,8 @@ def run_random1k(args):
                        "cycles_per_step": cycles, "noise": "sigma 5 / 2"},
             "sim_ms_per_wall_s": round(cycles * k / (ms * 1e-3), 1),
             "e2e": {"value": round(e2e_events / e2e_s, 1), "unit": UNIT, "sim_ms_per_wall_s": round(cycles / e2e_s, 1),
-                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 4 * sum(e2e_counts)}}
+                    # counted by the library over the 1000 calls (the step)
+                    "h2d_bytes_per_step": int(bus[0]), "d2h_bytes_per_step": int(bus[1])}}
     if not args.no_cpu_baseline:
         ol = Library(oracle_library())
         oconf = Configuration(ol)
@@ -1033,7 +1046,7 @@ def main():
                     help="--sharded: exchange the fired words through host memory")
     ap.add_argument("--mixed", action="store_true",
                     help="measure the mixed-plugin network (nemo_step with Poisson stimulus)")
-    ap.add_argument("--mixed-cycles", type=int, default=1000)
+    ap.add_argument("--mixed-cycles", type=int, default=5000)
     ap.add_argument("--ncu-case", action="store_true",
                     help="a bounded run of the headline (or --small) workload for ncu captures")
     args = ap.parse_args()

@@ -216,11 +216,26 @@ nemo_status_t nemo_b200_batch_fired_at(nemo_simulation_t sim, uint64_t cycle,
 nemo_status_t nemo_b200_run_graph(nemo_simulation_t sim, unsigned cycles, unsigned cycles_per_launch,
 		int* used_graph);
 
-/* Choose the step kernel's threads per partition (1024, 512 or 256; the
- * partitions stay) by timing `trial_cycles` cycles with each, twice, keeping
- * the fastest. The 6 x trial_cycles cycles are simulated like any others.
- * ms[k] (may be NULL): the better device ms per cycle of each size. */
+/* Choose the step kernel's work shape by timing `trial_cycles` cycles with
+ * each candidate, twice, interleaved, keeping the fastest: threads per
+ * partition (1024, 512 or 256; the partitions stay) and, for a network with
+ * STDP, the synapses of a full STDP work entry (128 or 64: a post-spiking
+ * target's plastic synapses are dealt to the warps in runs of that length).
+ * The results do not depend on the shape; the trial cycles are simulated
+ * like any others (2 x candidates x trial_cycles). nemo_b200_autotune:
+ * ms[k] (may be NULL) the best device ms per cycle with thread size k.
+ * nemo_b200_autotune_shape: ms[3 r + k] (may be NULL) with thread size k
+ * and run length r (0 for r = 1 without STDP). */
 nemo_status_t nemo_b200_autotune(nemo_simulation_t sim, unsigned trial_cycles, unsigned* threads, double ms[3]);
+nemo_status_t nemo_b200_autotune_shape(nemo_simulation_t sim, unsigned trial_cycles, unsigned* threads,
+		unsigned* stdp_run, double ms[6]);
+
+/* Bytes that crossed the bus for nemo_step calls since the simulation was
+ * made: out[0] host to device (stimulus: a resident step's command chunks,
+ * else the staged stimulus), out[1] device to host (each step's fired
+ * list: its count and error words, its {fired word, warp} pairs, and a
+ * resident step's done word). */
+nemo_status_t nemo_b200_host_bytes(nemo_simulation_t sim, unsigned long long out[2]);
 
 /* ---- the differentiable form: discrete LIF network and its BPTT adjoint ----
  *

@@ -1010,10 +1010,11 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				if(net.stdp) {
 					/* post-synaptic firing P cycles ago (ConnectivityMatrix.cpp:237):
 					 * the target's plastic synapses as runs of at most
-					 * STDP_ITEM, one list entry each */
+					 * stdpRun, one list entry each */
 					const bool post = valid && ((rfNew >> net.postShift) & 1ull);
 					const uint32_t len = post ? rcm.y - rcm.x : 0u;
-					const uint32_t runs = (len + STDP_ITEM - 1u) / STDP_ITEM;
+					const uint32_t run = net.stdpRun;
+					const uint32_t runs = (len + run - 1u) / run;
 					if(__ballot_sync(FULL, runs != 0u)) {
 						uint32_t incl = runs;
 #pragma unroll
@@ -1025,8 +1026,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 						if(lane == 31) base = atomicAdd(&sNPost, incl);
 						base = __shfl_sync(FULL, base, 31) + incl - runs;
 						for(uint32_t r = 0; r < runs; ++r) {
-							const uint32_t off = r * STDP_ITEM;
-							postOut[base + r] = make_uint2(rcm.x + off, min(STDP_ITEM, len - off));
+							const uint32_t off = r * run;
+							postOut[base + r] = make_uint2(rcm.x + off, min(run, len - off));
 						}
 						if(runs) {
 							/* the next phase's STDP accumulation walks this

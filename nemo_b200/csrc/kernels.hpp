@@ -59,6 +59,9 @@ const int GATHER_PER_LANE = 4;
  * a run of at most STDP_ITEM synapses of one post-spiking target) */
 const uint32_t STDP_PER_LANE = 4;
 const uint32_t STDP_ITEM = 32 * STDP_PER_LANE;
+/* the shortest run an STDP entry may be given (NetDev::stdpRun, chosen by
+ * the autotuner from STDP_ITEM and this); the lists are sized for it */
+const uint32_t STDP_RUN_MIN = 64;
 /* stimulus entries of each kind a one-cycle step carries in its kernel
  * parameters (CycleArgs::inlineF / inlineI) */
 const uint32_t INLINE_STIM_MAX = 32;
@@ -124,12 +127,13 @@ struct NetDev {
 	/* per-cycle lists by cycle parity and block, with their lengths
 	 * [2][blocks]: fired sources (device indices), [2][blocks][ownWarps * 32],
 	 * and the STDP entries of post-spiking targets, [2][blocks][postStride]:
-	 * reverse-matrix runs {first, count}, count in [1, STDP_ITEM] */
+	 * reverse-matrix runs {first, count}, count in [1, stdpRun] */
 	uint32_t* firedList;
 	uint32_t* firedCnt;
 	uint2* postList;
 	uint32_t* postCnt;
 	uint32_t postStride;           /* entries of a block's list: the most its neurons can make */
+	uint32_t stdpRun;              /* synapses of a full STDP entry: STDP_RUN_MIN .. STDP_ITEM, multiple of 32 */
 
 	/* STDP (reverse connectivity of plastic synapses, grouped by target) */
 	int stdp;

@@ -518,6 +518,25 @@ nemo_b200_autotune(nemo_simulation_t s, unsigned trial_cycles, unsigned* threads
 }
 
 nemo_status_t
+nemo_b200_host_bytes(nemo_simulation_t s, unsigned long long out[2])
+{
+	RETURN_CALL(s->sim.hostBytes(out));
+}
+
+nemo_status_t
+nemo_b200_autotune_shape(nemo_simulation_t s, unsigned trial_cycles, unsigned* threads, unsigned* stdp_run,
+		double ms[6])
+{
+	RETURN_CALL({
+		double t[6];
+		const nemo_b200::AutotuneShape best = s->sim.autotuneShape(trial_cycles, t);
+		if(threads) *threads = best.threads;
+		if(stdp_run) *stdp_run = best.stdpRun;
+		if(ms) for(int k = 0; k < 6; ++k) ms[k] = t[k];
+	});
+}
+
+nemo_status_t
 nemo_b200_expf_check(nemo_simulation_t s, uint64_t* mismatches)
 {
 	RETURN_CALL(*mismatches = s->sim.expfCheck());

@@ -486,8 +486,8 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		}
 	}
 	/* STDP entries: a post-spiking target's plastic synapses in runs of at
-	 * most STDP_ITEM; a block's list of one cycle holds at most the sum of
-	 * its neurons' runs */
+	 * most stdpRun; a block's list of one cycle holds at most the sum of its
+	 * neurons' runs at the shortest run length */
 	uint64_t postStride = 1;
 	if(m_stdpOn) {
 		std::vector<uint32_t> hostStart;
@@ -502,7 +502,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 		for(uint32_t b = 0; b < m_blocks; ++b) {
 			uint64_t runs = 0;
 			const uint32_t n0 = (warpLo + ownStart[b]) * 32u, n1 = (warpLo + ownStart[b + 1]) * 32u;
-			for(uint32_t n = n0; n < n1; ++n) runs += (uint64_t(rs[n + 1] - rs[n]) + STDP_ITEM - 1) / STDP_ITEM;
+			for(uint32_t n = n0; n < n1; ++n) runs += (uint64_t(rs[n + 1] - rs[n]) + STDP_RUN_MIN - 1) / STDP_RUN_MIN;
 			postStride = std::max(postStride, runs);
 		}
 	}
@@ -576,6 +576,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.firedCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	m_net.postList = (uint2*) alloc(size_t(2) * B * postStride * 8);
 	m_net.postStride = uint32_t(postStride);
+	m_net.stdpRun = STDP_ITEM;
 	m_net.postCnt = (uint32_t*) alloc(size_t(2) * B * 4);
 	if(m_shard.world > 1) {
 		m_net.remoteList = (uint32_t*) alloc(size_t(2) * m_nDev * 4);
@@ -983,6 +984,8 @@ Simulation::step(const unsigned* fstim, size_t nf, const unsigned* inidx, const 
 	m_cycle++;
 	m_stateDirty = true;
 	decodeStepList(m_fired);
+	m_bytesIn += 4 * uint64_t(nf) + 8 * uint64_t(ni);
+	m_bytesOut += 8 + 8 * uint64_t(m_stepWords[1]);
 	return m_fired;
 }
 
@@ -1107,6 +1110,7 @@ Simulation::postCommand(uint32_t seq, uint32_t op)
 	for(uint32_t k = 0; k < ni; ++k) payload[n++] = m_inline.i[k];
 	for(uint32_t k = 0; k < ni; ++k) std::memcpy(&payload[n++], &m_inline.cur[k], 4);
 	const uint32_t chunks = (n + 2) / 3;
+	m_bytesIn += 16u * chunks;
 	volatile uint32_t* c = reinterpret_cast<volatile uint32_t*>(m_rcmd->c);
 	for(uint32_t k = 0; k < chunks; ++k) {
 		/* the chunk's payload, then its number (x86 keeps the store order) */
@@ -1167,6 +1171,8 @@ Simulation::stepResident(const unsigned* fstim, size_t nf, const unsigned* inidx
 	m_cycle++;
 	m_stateDirty = true;
 	decodeStepList(m_fired);
+	/* the done word, the error and count words, the pairs */
+	m_bytesOut += 4 + 8 + 8 * uint64_t(m_stepWords[1]);
 	return true;
 }
 
@@ -1630,8 +1636,16 @@ Simulation::runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph)
 	checkDeviceError();
 }
 
-unsigned
-Simulation::autotune(unsigned trialCycles, double ms[3])
+/* The step kernel's shape by trial: threads per block (1024, 512, 256) and,
+ * for a network with STDP, the synapses of a full STDP work entry (128, 64),
+ * each candidate timed over trialCycles ordinary cycles (simulated: the
+ * network advances), twice, interleaved, the better trial kept (the
+ * network's activity drifts between trials); the fastest is kept for the
+ * following launches. Results do not depend on the shape. ms[3 * r + k]:
+ * ms per cycle with thread size k and run length r (r = 1 only with STDP,
+ * else 0). */
+AutotuneShape
+Simulation::autotuneShape(unsigned trialCycles, double ms[6])
 {
 	notShard("autotune");
 	notExternal("autotune");
@@ -1641,43 +1655,61 @@ Simulation::autotune(unsigned trialCycles, double ms[3])
 	}
 	cudaStream_t stream = STREAM(m_stream);
 	const unsigned sizes[3] = {1024, 512, 256};
-	unsigned best = sizes[0];
+	const unsigned runs[2] = {STDP_ITEM, STDP_RUN_MIN};
+	const int nRuns = m_stdpOn ? 2 : 1;
+	AutotuneShape best{sizes[0], runs[0]};
 	double bestMs = 1e300;
 	cudaEvent_t e0, e1;
 	NEMO_CUDA(cudaEventCreate(&e0));
 	NEMO_CUDA(cudaEventCreate(&e1));
-	/* two rounds, sizes interleaved, the better trial of each size: the
-	 * network's activity drifts between trials */
-	for(int k = 0; k < 3; ++k) ms[k] = 1e300;
+	for(int k = 0; k < 6; ++k) ms[k] = k < 3 * nRuns ? 1e300 : 0.0;
 	for(int round = 0; round < 2; ++round) {
-		for(int k = 0; k < 3; ++k) {
-			m_net.threads = sizes[k];
-			m_args.net.threads = sizes[k];
-			NEMO_CUDA(cudaEventRecord(e0, stream));
-			launchBlock(m_cycle, trialCycles);
-			NEMO_CUDA(cudaEventRecord(e1, stream));
-			NEMO_CUDA(cudaEventSynchronize(e1));
-			m_cycle += trialCycles;
-			float t = 0;
-			NEMO_CUDA(cudaEventElapsedTime(&t, e0, e1));
-			ms[k] = std::min(ms[k], double(t) / trialCycles);
+		for(int r = 0; r < nRuns; ++r) {
+			for(int k = 0; k < 3; ++k) {
+				m_net.threads = sizes[k];
+				m_net.stdpRun = runs[r];
+				m_args.net.threads = sizes[k];
+				m_args.net.stdpRun = runs[r];
+				NEMO_CUDA(cudaEventRecord(e0, stream));
+				launchBlock(m_cycle, trialCycles);
+				NEMO_CUDA(cudaEventRecord(e1, stream));
+				NEMO_CUDA(cudaEventSynchronize(e1));
+				m_cycle += trialCycles;
+				float t = 0;
+				NEMO_CUDA(cudaEventElapsedTime(&t, e0, e1));
+				ms[3 * r + k] = std::min(ms[3 * r + k], double(t) / trialCycles);
+			}
 		}
 	}
-	for(int k = 0; k < 3; ++k) {
-		if(ms[k] < bestMs) {
-			bestMs = ms[k];
-			best = sizes[k];
+	for(int r = 0; r < nRuns; ++r) {
+		for(int k = 0; k < 3; ++k) {
+			if(ms[3 * r + k] < bestMs) {
+				bestMs = ms[3 * r + k];
+				best = AutotuneShape{sizes[k], runs[r]};
+			}
 		}
 	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
-	m_net.threads = best;
-	m_args.net.threads = best;
+	m_net.threads = best.threads;
+	m_net.stdpRun = best.stdpRun;
+	m_args.net.threads = best.threads;
+	m_args.net.stdpRun = best.stdpRun;
 	m_stateDirty = true;
 	NEMO_CUDA(cudaMemcpyAsync(m_hWords + m_net.nWords, m_net.barrier + 2, 4, cudaMemcpyDeviceToHost, stream));
 	NEMO_CUDA(cudaStreamSynchronize(stream));
 	checkDeviceError();
 	return best;
+}
+
+/* autotuneShape, reported by thread size: ms[k] the best over run lengths */
+unsigned
+Simulation::autotune(unsigned trialCycles, double ms[3])
+{
+	double all[6];
+	const AutotuneShape best = autotuneShape(trialCycles, all);
+	for(int k = 0; k < 3; ++k) ms[k] = m_stdpOn ? std::min(all[k], all[3 + k]) : all[k];
+	return best.threads;
 }
 
 void

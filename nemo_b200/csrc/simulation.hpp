@@ -20,6 +20,12 @@ namespace nemo_b200 {
 /* One shard of a sharded simulation: shard `rank` of `world` owns the
  * device warps [warpLo, warpHi) (contiguous, equal counts of warps) and
  * holds the synapses whose target it owns; maxDelay is the whole network's. */
+/* the step kernel's shape chosen by the autotuner */
+struct AutotuneShape {
+	unsigned threads;     /* threads per block */
+	unsigned stdpRun;     /* synapses of a full STDP work entry */
+};
+
 struct ShardSpec {
 	unsigned rank = 0;
 	unsigned world = 1;
@@ -166,12 +172,25 @@ public:
 	 * when the device refused the capture and the launches ran directly. */
 	void runGraph(unsigned cycles, unsigned cyclesPerLaunch, int* usedGraph);
 
-	/* Time `trialCycles` cycles with each block size of the step kernel
-	 * (1024, 512, 256 threads over the same partitions; the results are the
-	 * same), twice each, and keep the fastest. The cycles are simulated
-	 * (6 x trialCycles in all). ms[k]: the better device ms per cycle of
-	 * each size. Returns the size. */
+	/* Time `trialCycles` cycles with each shape of the step kernel's work:
+	 * block size (1024, 512, 256 threads over the same partitions) and, with
+	 * STDP, the synapses of a full STDP work entry (128, 64); the results
+	 * are the same. Twice each, interleaved, and keep the fastest. The
+	 * cycles are simulated (2 x candidates x trialCycles in all).
+	 * autotuneShape: ms[3 r + k] the better device ms per cycle of size k
+	 * and run length r. autotune: ms[k] the best of size k; returns the
+	 * size. */
 	unsigned autotune(unsigned trialCycles, double ms[3]);
+	AutotuneShape autotuneShape(unsigned trialCycles, double ms[6]);
+
+	/* bytes that crossed between host and device for nemo_step calls since
+	 * the simulation was made: [0] to the device (stimulus), [1] to the
+	 * host (the fired lists and their counts and flags) */
+	void hostBytes(unsigned long long out[2]) const
+	{
+		out[0] = m_bytesIn;
+		out[1] = m_bytesOut;
+	}
 
 	/* Phase timing of one traced persistent launch of `cycles` cycles, means
 	 * over cycles in ns: [0] phase, [1] max / [2] mean block update with the
@@ -351,6 +370,11 @@ private:
 	bool m_resident = false;            /* a resident launch is on the stream */
 	bool m_residentOn = true;           /* nemo_step may use resident stepping */
 	uint32_t m_rseq = 0;                /* the last command number */
+	/* bytes of the per-cycle steps' inputs and outputs across the bus:
+	 * stimulus (resident command chunks, or the staged copies and kernel
+	 * parameters) and the step lists read back (hostBytes) */
+	uint64_t m_bytesIn = 0;
+	uint64_t m_bytesOut = 0;
 	ResidentHostCmd* m_rcmd = nullptr;  /* mapped host memory */
 	ResidentHostCmd* m_dRcmd = nullptr; /* its device address */
 	/* write command `seq` (op, and m_inline's stimulus for a step) into

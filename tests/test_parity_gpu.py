@@ -110,6 +110,39 @@ def test_stdp_network_weights(oracle_lib):
             assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid)
 
 
+def test_autotuned_shape_keeps_results(oracle_lib):
+    """The autotuner's trials (block sizes x STDP run lengths) are ordinary
+    cycles and the shape it keeps changes no result: firing every cycle and
+    every weight after applyStdp equal the oracle's, which runs the same
+    cycles."""
+    spec = netgen.izhikevich_random(2000, 100, dmax=20, seed=8, stdp=True)
+    pre, post = netgen.standard_stdp()
+    (gn, g), (on, o) = _pair(spec, oracle_lib, stdp=(pre, post, (0.0, 1.0, 0.0, -1.0)))
+    lib = g.lib
+    lib.dll.nemo_b200_autotune_shape.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.POINTER(ctypes.c_uint),
+                                                 ctypes.POINTER(ctypes.c_uint), ctypes.c_double * 6]
+    for c in range(50):
+        assert np.array_equal(g.step(), o.step()), c
+    threads, run = ctypes.c_uint(), ctypes.c_uint()
+    ms = (ctypes.c_double * 6)()
+    trial = 10
+    lib.call("nemo_b200_autotune_shape", g.handle, trial, ctypes.byref(threads), ctypes.byref(run), ms)
+    assert threads.value in (256, 512, 1024) and run.value in (64, 128)
+    assert all(x > 0 for x in ms)
+    # two rounds over 3 block sizes x 2 run lengths
+    first = 50
+    for c in range(first, first + 12 * trial):
+        assert np.array_equal(g.fired_at(c), o.step()), c
+    for epoch in range(2):
+        for c in range(100):
+            assert np.array_equal(g.step(), o.step()), (epoch, c)
+        g.apply_stdp(1.0)
+        o.apply_stdp(1.0)
+    for src in range(0, 2000, 7):
+        for sid in g.get_synapses_from(src):
+            assert g.get_synapse_weight(sid) == o.get_synapse_weight(sid)
+
+
 def test_stdp_clamps_out_of_bound_weights(oracle_lib):
     """Excitatory weights up to 0.5 with an STDP bound of 0.3: the first
     applyStdp clamps every plastic weight, those with a zero accumulator
