@@ -1145,8 +1145,8 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			 * unit before it has issued its own last loads.
 			 * lead: a gather unit's fired source of each lane {s, 1} ({0, 0}
 			 * past the end), an STDP unit's entry {first, count}.
-			 * second: a gather unit's bucket {first record, records} of each
-			 * lane, an STDP unit's source words. */
+			 * second: a gather unit's bucket {first record, end} of each lane,
+			 * an STDP unit's source words. */
 			auto lead = [&](uint32_t u) -> uint2 {
 				uint2 v = make_uint2(0u, 0u);
 				if(u < G) {
