@@ -406,6 +406,28 @@ class Simulation:
             return np.zeros(0, dtype=np.uint32)
         return np.ctypeslib.as_array(ptr, shape=(n.value,)).astype(np.uint32)
 
+    def autotune(self, trial_cycles=100):
+        """Choose the step kernel's work shape by timing (nemo_b200_autotune_shape):
+        returns (threads per block, synapses of a full STDP entry, {(threads,
+        run): ms per cycle}). The trial cycles are simulated like any others."""
+        threads, run = c_uint(), c_uint()
+        ms = (ctypes.c_double * 6)()
+        fn = self.lib.dll.nemo_b200_autotune_shape
+        fn.argtypes = [c_void_p, c_uint, POINTER(c_uint), POINTER(c_uint), ctypes.c_double * 6]
+        self.lib.call("nemo_b200_autotune_shape", self.handle, trial_cycles, byref(threads), byref(run), ms)
+        table = {(t, r): ms[3 * i + k] for i, r in enumerate((128, 64)) for k, t in enumerate((1024, 512, 256))
+                 if ms[3 * i + k] > 0}
+        return threads.value, run.value, table
+
+    def host_bytes(self):
+        """Bytes that nemo_step calls moved to and from the device since the
+        simulation was made (nemo_b200_host_bytes): (to device, to host)."""
+        out = (ctypes.c_ulonglong * 2)()
+        fn = self.lib.dll.nemo_b200_host_bytes
+        fn.argtypes = [c_void_p, ctypes.c_ulonglong * 2]
+        self.lib.call("nemo_b200_host_bytes", self.handle, out)
+        return int(out[0]), int(out[1])
+
     def get_weights(self, ids):
         """Weights of many synapses at once (nemo_b200_get_weights)."""
         ids = np.ascontiguousarray(np.asarray(ids, dtype=np.uint64))
