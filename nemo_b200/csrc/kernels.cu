@@ -287,6 +287,20 @@ __device__ __forceinline__ float drawNoise(const NetDev& net, const GroupDev& g,
 	return nz;
 }
 
+/* drawNoise for the next cycle of resident stepping, without advancing the
+ * neuron's generator: from state `from`, the deviate into noise[pNext] and
+ * the state after it into rngAhead[pNext] (the state unchanged when sigma is
+ * 0), where the next cycle's update takes both. */
+__device__ __forceinline__ void drawNoiseAhead(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n, uint4 from,
+		uint32_t pNext)
+{
+	const float sigma = __ldg(&g.param[4 * size_t(g.count) + i]);
+	float nz = 0.0f;
+	if(sigma != 0.0f) nz = nrand(from, net.sinTab, net.logTab);
+	net.rngAhead[size_t(pNext) * net.nDev + n] = from;
+	net.noise[size_t(pNext) * net.nDev + n] = nz;
+}
+
 /* IF_curr_exp (src/nemo/cpu/plugins/IF_curr_exp.cpp:74-121). Parameters in
  * IF_curr_exp.h order; state v, ie, ii, lastfire. Fires on v > v_thresh. */
 __device__ __forceinline__ bool modelIfCurrExp(const NetDev& net, const GroupDev& g, uint32_t i, uint32_t n,
@@ -980,12 +994,22 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					switch(G.kind) {
 						case 0: {
 							/* the first cycle of a launch draws its noise here;
-							 * later ones use the draw made in the phase before
-							 * (a resident launch draws every cycle's here: it
-							 * cannot know whether a next cycle comes, and a
-							 * draw advances the generator) */
-							const float nz = (k == 0 || resident) ? drawNoise(net, G, i) : net.noise[par * nDev + n];
+							 * later ones use the draw made in the phase before.
+							 * A resident launch cannot know whether a next cycle
+							 * comes, and a draw advances the generator: there the
+							 * draw ahead leaves the generator alone, and the
+							 * cycle that uses it advances it here */
+							float nz;
+							uint4 ahead = make_uint4(0u, 0u, 0u, 0u);
+							if(k == 0) {
+								nz = drawNoise(net, G, i);
+							} else {
+								nz = net.noise[par * nDev + n];
+								if(resident) ahead = net.rngAhead[size_t(par) * nDev + n];
+							}
 							fired = modelIzhikevich(net, G, i, n, E, I, stim, nz);
+							/* stored after the model has issued its loads */
+							if(k > 0 && resident) G.rng[i] = ahead;
 							break;
 						}
 						case 1: fired = modelIfCurrExp(net, G, i, n, E, I, stim); break;
@@ -1089,8 +1113,12 @@ k_cycles(const __grid_constant__ CycleArgs A)
 				/* in the first phase the noise of the next cycle is drawn by
 				 * the warp that just advanced the generator (later phases
 				 * draw it in work units below) */
-				if(k == 0 && k + 1 < A.cycles && G.kind == 0 && valid) {
-					net.noise[(par ^ 1u) * nDev + n] = drawNoise(net, G, i);
+				if(k == 0 && G.kind == 0 && valid) {
+					if(k + 1 < A.cycles) {
+						net.noise[(par ^ 1u) * nDev + n] = drawNoise(net, G, i);
+					} else if(resident) {
+						drawNoiseAhead(net, G, i, n, G.rng[i], par ^ 1u);
+					}
 				}
 				if(trace) {
 					/* the warp's loads and model, its whole update, and for
@@ -1131,7 +1159,7 @@ k_cycles(const __grid_constant__ CycleArgs A)
 			const uint32_t Sb = P > b ? (P - b + B - 1u) / B : 0u;
 			/* units [G, G + NW): the next cycle's noise of one owned neuron
 			 * warp each (from the second phase of a launch on) */
-			const uint32_t NW = (k + 1u < A.cycles) ? myWarps : 0u;
+			const uint32_t NW = (k + 1u < A.cycles || (resident && k > 0u)) ? myWarps : 0u;
 			const uint32_t units = G + NW + Sb;
 			const uint32_t* flist = net.firedList + par * listStride;
 			const uint2* plist = net.postList + par * postParity;
@@ -1250,7 +1278,13 @@ k_cycles(const __grid_constant__ CycleArgs A)
 					const uint32_t n = dw * 32u + lane;
 					const uint32_t i = n - Gr.devBase;
 					if(Gr.kind == 0 && i < Gr.count) {
-						net.noise[((t + 1u) & 1u) * nDev + n] = drawNoise(net, Gr, i);
+						if(resident) {
+							/* from the state this cycle's update advances the
+							 * generator to */
+							drawNoiseAhead(net, Gr, i, n, net.rngAhead[size_t(t & 1u) * nDev + n], (t + 1u) & 1u);
+						} else {
+							net.noise[((t + 1u) & 1u) * nDev + n] = drawNoise(net, Gr, i);
+						}
 					}
 				} else {
 					/* STDP (ConnectivityMatrix.cpp:224-258): a run of the

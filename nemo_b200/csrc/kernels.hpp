@@ -122,6 +122,10 @@ struct NetDev {
 	uint32_t* firedCountRing;      /* [ring] */
 	float* ext;                    /* [nDev] external current, cleared after use */
 	float* noise;                  /* [2][nDev] Izhikevich noise of the next cycle, by cycle parity */
+	/* resident stepping: [2][nDev] the generator state after the next cycle's draw, by cycle
+	 * parity, drawn ahead without advancing the neuron's generator (which the next cycle's
+	 * update advances to it, if that cycle comes) */
+	uint4* rngAhead;
 	uint32_t* fstim;               /* [nWords] firing stimulus, cleared after use */
 
 	/* per-cycle lists by cycle parity and block, with their lengths

@@ -569,6 +569,7 @@ Simulation::construct(const Network& net, const Configuration& conf, const Shard
 	m_net.firedCountRing = (uint32_t*) alloc(size_t(m_ring) * 4);
 	m_net.ext = (float*) alloc(size_t(m_nDev) * 4);
 	m_net.noise = (float*) alloc(size_t(2) * m_nDev * 4);
+	m_net.rngAhead = (uint4*) alloc(size_t(2) * m_nDev * 16);
 	m_net.fstim = (uint32_t*) alloc(size_t(m_net.nWords) * 4);
 	m_net.stats = (unsigned long long*) alloc(4 * 8);
 	m_net.barrier = (unsigned*) alloc(4 * 4);
